@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark of the in-place Esoteric-Pull step on B200.
+
+Workload (N = 1): D3Q19, 512^3, TRT (magic 3/16) + Smagorinsky Cs = 0.1,
+lid-driven cavity (half-way bounce-back on five walls, moving lid u = (0.1, 0, 0)),
+tau = 0.51, FP32 populations, started at rest with rho = 1.  One bench step is
+one fused stream+collide launch over the whole lattice.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  ``value`` is whole-job GLUPS (lattice cells x
+steps / device time, max over ranks); with N > 1 every rank runs its own
+independent 512^3 lattice (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "D3Q19/27 GLUPS + % of HBM roofline, FP16-store vs FP32; adjoint/forward time"
+L2_BYTES = 126 * 1024 * 1024
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+STEP_KERNEL_PROFILE = ROOT / "profiles" / "k_step_d3q19_fp32_cavity512.md"
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser(description=__doc__)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=500)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n", type=int, default=512, help="cavity edge (cells)")
+    p.add_argument("--lattice", choices=["d3q19", "d3q27"], default="d3q19")
+    p.add_argument("--storage", choices=["fp32", "fp16s"], default="fp32")
+    p.add_argument("--no-variants", action="store_true", help="skip the FP16S / D3Q27 side measurements")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args(argv)
+
+
+# ------------------------------------------------------------------ helpers
+def bytes_per_update(q: int, storage: str) -> int:
+    s = {"fp32": 4, "fp16s": 2, "fp64": 8}[storage]
+    return 2 * q * s
+
+
+def cavity_fluid_cells(n: int) -> int:
+    # walls on x = 0, x = n-1, y = 0, z = 0, z = n-1; lid on y = n-1
+    return (n - 2) * (n - 2) * (n - 2)
+
+
+def algorithmic_bytes_per_launch(n: int, q: int, storage: str) -> int:
+    """Populations read + written once per fluid cell, plus the 1-byte flag of every cell."""
+    return cavity_fluid_cells(n) * bytes_per_update(q, storage) + n ** 3
+
+
+def hbm_peak():
+    try:
+        peaks = json.loads(PEAKS_FILE.read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per launch of the step kernel from the committed ncu summary, if any."""
+    try:
+        for line in STEP_KERNEL_PROFILE.read_text().splitlines():
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- our engine
+def make_cavity(cs, n, lattice="d3q19", storage="fp32", device=0):
+    s = cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(
+        nx=n, ny=n, nz=n, tau=0.51, lattice=lattice, collision="trt", trt_magic=3.0 / 16.0, smagorinsky_les=True,
+        smagorinsky_cs=0.1, storage=storage, device=device))
+    return s
+
+
+def setup_cavity(s, cs, n, flags=None):
+    s.set_flags(cs.cavity_flags(n, n, n) if flags is None else flags)
+    s.set_wall_velocity(2, 0.1, 0.0, 0.0)
+    s.initialize_uniform()
+
+
+def time_steps(torch, s, steps):
+    """Device time (ms) of `steps` step launches, CUDA events on the solver's own stream."""
+    stream = torch.cuda.ExternalStream(s.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    s.wait()
+    e0.record(stream)
+    s.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def e2e_job(torch, cs, n, steps, device):
+    """The whole job through the public API with host buffers, timed end to end.
+
+    Upload the cavity flags from pinned host memory, initialise, run `steps`
+    steps, download rho/u (4 floats per cell) into pinned host memory and the
+    FP64 reductions.  Returns (GLUPS, h2d bytes, d2h bytes).
+    """
+    cells = n ** 3
+    flags_host = torch.from_numpy(cs.cavity_flags(n, n, n)).pin_memory()
+    out = [torch.empty(cells, dtype=torch.float32).pin_memory() for _ in range(4)]
+    s = make_cavity(cs, n, device=device)
+    lib = s.library.raw
+    import ctypes
+
+    try:
+        s.wait()
+        t0 = time.perf_counter()
+        lib.cfdx_lbm_set_flags(s.handle, ctypes.c_void_p(flags_host.data_ptr()), cs.bindings.HOST)
+        s.set_wall_velocity(2, 0.1, 0.0, 0.0)
+        s.initialize_uniform()
+        s.step(steps)
+        s.library.check(lib.cfdx_lbm_macroscopic(s.handle, *[ctypes.c_void_p(o.data_ptr()) for o in out],
+                                                 cs.bindings.HOST))
+        red = s.reduce()
+        t1 = time.perf_counter()
+        stats = s.transfer_stats()
+    finally:
+        s.close()
+    if red["nonfinite"]:
+        raise RuntimeError("e2e job produced non-finite populations")
+    return cells * steps / (t1 - t0) / 1e9, stats.host_to_device_bytes, stats.device_to_host_bytes
+
+
+def measure_variant(torch, cs, n, lattice, storage, steps, device):
+    s = make_cavity(cs, n, lattice=lattice, storage=storage, device=device)
+    try:
+        setup_cavity(s, cs, n)
+        time_steps(torch, s, 3)
+        ms = time_steps(torch, s, steps)
+        red = s.reduce()
+    finally:
+        s.close()
+    q = 19 if lattice == "d3q19" else 27
+    glups = n ** 3 * steps / (ms / 1e3) / 1e9
+    gbs = algorithmic_bytes_per_launch(n, q, storage) / (ms / steps / 1e3) / 1e9
+    return {"glups": glups, "ms_per_step": ms / steps, "achieved_gbs": gbs, "nonfinite": red["nonfinite"]}
+
+
+# ----------------------------------------------------------- reference (CPU)
+def cpu_reference_sample(n, warmup, steps, threads=0):
+    """The reference's CPU path on the closest feature set: EsotericPullSolver<D3Q19>
+    BGK + Smagorinsky with the cavity's walls and lid as a static solid mask
+    (its 3-pass solid step; it has no in-place TRT or moving wall)."""
+    from oracle import oracle as O
+
+    mask = (O.cavity_flags(n, n, n) != 0).astype(np.uint8)
+    mlups, seconds, _ = O.ref_bench(19, n, n, n, 0.51, warmup, steps, threads=threads, les=True, mask=mask)
+    return mlups, seconds, O.ref_threads()
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    # Calibrate a per-step sample so that warmup + steps end within ~2 minutes.
+    probe_n = 96
+    mlups, secs, cores = cpu_reference_sample(probe_n, 1, 2)
+    rate = mlups * 1e6
+    budget = 110.0
+    edge = int((rate * budget / max(1, args.steps + args.warmup)) ** (1.0 / 3.0))
+    edge = max(48, min(args.n, edge))
+    mlups, secs, cores = cpu_reference_sample(edge, args.warmup, args.steps)
+    glups = mlups / 1e3
+    sample = (f"reference EsotericPullSolver<D3Q19> BGK+Smagorinsky, cavity as static solid mask, "
+              f"{edge}^3 cells per step, {args.warmup} warmup + {args.steps} timed steps (3-pass solid path)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"D3Q19 lid-driven cavity {args.n}^3 (reference CPU sample {edge}^3)",
+                   "lattice": "d3q19", "n": args.n, "sample_n": edge},
+        "cpu_baseline": {"value": glups, "unit": "GLUPS", "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": glups, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------- main
+def main(argv=None):
+    args = parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+
+    import torch
+
+    import cfd_solvers_b200 as cs
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (no CPU fallback)")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    n = args.n
+    q = 19 if args.lattice == "d3q19" else 27
+    s = make_cavity(cs, n, lattice=args.lattice, storage=args.storage, device=local_rank)
+    setup_cavity(s, cs, n)
+    time_steps(torch, s, args.warmup)
+
+    sampler = ClockSampler(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    ms = time_steps(torch, s, args.steps)
+    clocks = sampler.stop()
+    barrier()
+    red = s.reduce()
+    s.close()
+
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    cells = n ** 3
+    value = cells * args.steps * world / (ms_max / 1e3) / 1e9
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        per_launch_s = ms / args.steps / 1e3
+        alg = algorithmic_bytes_per_launch(n, q, args.storage)
+        achieved = alg / per_launch_s / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.storage == "fp32" else "f16 storage / f32 arithmetic", "data": "synthetic",
+            "config": {
+                "workload": f"{args.lattice.upper()} lid-driven cavity {n}^3, TRT magic 3/16 + Smagorinsky Cs 0.1, "
+                            f"tau 0.51, lid u=(0.1,0,0), {args.storage.upper()} populations, from rest",
+                "lattice": args.lattice, "n": n, "storage": args.storage, "collision": "trt+les",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "l2": f"populations {cells * q * (4 if args.storage == 'fp32' else 2) / 1e9:.1f} GB > 126 MB L2 "
+                      "(no flush needed)",
+                "fluid_cells": cavity_fluid_cells(n),
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic": profiled_traffic(), "algorithmic_bytes_per_launch": alg,
+                         "kernel": "cfdx::k_step (one launch per step)"},
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+            "checks": {"nonfinite_cells": red["nonfinite"], "mass": red["mass"]},
+        }
+
+    # ---- end to end through the public API with host buffers (each rank its own job)
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        glups_e2e, h2d, d2h = e2e_job(torch, cs, n, args.steps, local_rank)
+        t = torch.tensor([glups_e2e], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        e2e = {"value": float(t.item()) * world, "unit": "GLUPS",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "job": f"host flags upload (pinned) + init + {args.steps} steps + rho/u download (pinned) + "
+                      "FP64 reductions, host wall clock; bytes per step = job bytes / steps"}
+
+    # ---- side measurements on rank 0 (FP16 storage, D3Q27)
+    variants = {}
+    if rank == 0 and not args.no_variants and world == 1:
+        vs = max(20, args.steps // 2)
+        if args.storage == "fp32" and args.lattice == "d3q19":
+            f16 = measure_variant(torch, cs, n, "d3q19", "fp16s", vs, local_rank)
+            f16["speedup_vs_fp32"] = f16["glups"] / value
+            f16["roofline_frac"] = f16["achieved_gbs"] / hbm_peak()[0]
+            variants["d3q19_fp16s"] = f16
+            d27 = measure_variant(torch, cs, n, "d3q27", "fp32", vs, local_rank)
+            d27["roofline_frac"] = d27["achieved_gbs"] / hbm_peak()[0]
+            variants["d3q27_fp32"] = d27
+
+    if rank == 0:
+        line["e2e"] = e2e
+        if variants:
+            line["variants"] = variants
+        if not args.no_cpu_baseline and world == 1:
+            edge = min(n, 256)
+            mlups, secs, cores = cpu_reference_sample(edge, 1, 5)
+            line["cpu_baseline"] = {
+                "value": mlups / 1e3, "unit": "GLUPS", "cores": cores, "kind": "reference",
+                "sample": f"reference EsotericPullSolver<D3Q19> BGK+Smagorinsky, cavity as static solid mask, "
+                          f"{edge}^3, 1 warmup + 5 timed steps ({secs:.1f} s), all host threads",
+            }
+        print(json.dumps(line), flush=True)
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

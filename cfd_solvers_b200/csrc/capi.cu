@@ -1,0 +1,756 @@
+// C ABI of the B200 in-place Esoteric-Pull engine (declared in include/cfdx_lbm.h).
+//
+// The handle owns the single population lattice, the optional flag /
+// acceleration / solid-fraction fields, the reduction scratch and one CUDA
+// stream.  Every entry point converts C++ and CUDA failures into a status
+// code and a thread-local message; nothing here throws across the ABI or
+// aborts.  There is no CPU fallback: without a CUDA device every call that
+// needs one returns CFDX_ERR_CUDA.
+#include "cfdx_lbm.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "lbm_launch.h"
+
+namespace {
+
+using namespace cfdx;
+
+thread_local std::string g_error;
+thread_local int g_error_status = CFDX_OK;
+std::atomic<int> g_fail_allocations{0};
+
+struct CfdxError : std::runtime_error {
+    int status;
+    CfdxError(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] void fail(int status, const std::string& message) { throw CfdxError(status, message); }
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    if (e == cudaErrorMemoryAllocation) fail(CFDX_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+    fail(CFDX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Allocation wrapper with the test hook of cfdx_debug_fail_allocations().
+void* device_alloc(std::size_t bytes, const char* what) {
+    if (g_fail_allocations.load() > 0) {
+        g_fail_allocations.fetch_sub(1);
+        fail(CFDX_ERR_OOM, std::string(what) + ": injected allocation failure (cudaErrorMemoryAllocation)");
+    }
+    void* p = nullptr;
+    check_cuda(cudaMalloc(&p, bytes), what);
+    return p;
+}
+
+void device_free(void* p) {
+    if (p) cudaFree(p);
+}
+
+template <class F> int guarded(F&& body) {
+    try {
+        body();
+        return CFDX_OK;
+    } catch (const CfdxError& e) {
+        g_error = e.what();
+        g_error_status = e.status;
+        return e.status;
+    } catch (const std::invalid_argument& e) {
+        g_error = e.what();
+        g_error_status = CFDX_ERR_INVALID;
+        return CFDX_ERR_INVALID;
+    } catch (const std::out_of_range& e) {
+        g_error = e.what();
+        g_error_status = CFDX_ERR_RANGE;
+        return CFDX_ERR_RANGE;
+    } catch (const std::bad_alloc& e) {
+        g_error = e.what();
+        g_error_status = CFDX_ERR_OOM;
+        return CFDX_ERR_OOM;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        g_error_status = CFDX_ERR_UNKNOWN;
+        return CFDX_ERR_UNKNOWN;
+    } catch (...) {
+        g_error = "unknown C++ exception";
+        g_error_status = CFDX_ERR_UNKNOWN;
+        return CFDX_ERR_UNKNOWN;
+    }
+}
+
+void copy_error(char* out, std::size_t cap, const std::string& text) {
+    if (!out || cap == 0U) return;
+    const std::size_t n = std::min(cap - 1U, text.size());
+    std::memcpy(out, text.data(), n);
+    out[n] = '\0';
+}
+
+int storage_bytes(int storage) { return storage == kStoreF64 ? 8 : (storage == kStoreF16S ? 2 : 4); }
+
+// Reference Smagorinsky coefficient 16 sqrt(2) / (3 pi^2), evaluated in float
+// as include/cfd/solvers/lbm/esoteric_pull.hpp:94-95 does.
+float reference_les_k() {
+    const float pi = 3.14159265358979323846F;
+    return 16.0F * 1.4142135623730950488F / (3.0F * pi * pi);
+}
+
+double lattice_weight(int q, int d) {
+    static const int cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
+    static const int cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1};
+    static const int cz[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1};
+    const int len2 = cx[d] * cx[d] + cy[d] * cy[d] + cz[d] * cz[d];
+    if (q == 19) return len2 == 0 ? 1.0 / 3.0 : (len2 == 1 ? 1.0 / 18.0 : 1.0 / 36.0);
+    return len2 == 0 ? 8.0 / 27.0 : (len2 == 1 ? 2.0 / 27.0 : (len2 == 2 ? 1.0 / 54.0 : 1.0 / 216.0));
+}
+
+} // namespace
+
+struct cfdx_lbm {
+    cfdx_lbm_config cfg{};
+    KernelKey key{};
+    std::size_t N = 0;
+    void* f = nullptr;
+    std::size_t f_bytes = 0;
+    std::uint8_t* flags = nullptr; // internal flag bytes
+    float* local_a = nullptr;
+    float* ns = nullptr;
+    float* macro_scratch = nullptr; // 4*N floats, lazily allocated
+    double* reduce_partials = nullptr;
+    double* reduce_out = nullptr;
+    double* host_reduce = nullptr; // pinned
+    int reduce_blocks = 0;
+    cudaStream_t stream = nullptr;
+    std::uint64_t t = 0;
+    float wall_u[kMaxWallIds][3]{};
+    float scale[27]{};
+    LaunchShape shape{};
+    double les_k = 0.0;
+    std::uint64_t h2d = 0, d2h = 0, syncs = 0;
+
+    LbmArgs args() const {
+        LbmArgs a{};
+        a.f = f;
+        a.flags = key.flags ? flags : nullptr;
+        a.local_a = local_a;
+        a.ns = ns;
+        a.nx = static_cast<long long>(cfg.nx);
+        a.ny = static_cast<long long>(cfg.ny);
+        a.nz = static_cast<long long>(cfg.nz);
+        a.N = N;
+        a.odd = static_cast<int>(t & 1U);
+        a.tau = cfg.tau;
+        a.omega_minus = cfg.trt_tau_minus > 0.0F ? 1.0 / static_cast<double>(cfg.trt_tau_minus) : 0.0;
+        a.trt_magic = cfg.trt_magic;
+        a.les_k = les_k;
+        a.ax = cfg.acceleration_x;
+        a.ay = cfg.acceleration_y;
+        a.az = cfg.acceleration_z;
+        std::memcpy(a.wall_u, wall_u, sizeof wall_u);
+        for (int d = 0; d < 27; ++d) {
+            a.scale[d] = scale[d] == 0.0F ? 1.0F : scale[d];
+            a.inv_scale[d] = 1.0F / a.scale[d];
+        }
+        return a;
+    }
+    dim3 block() const { return cell_block(static_cast<long long>(cfg.nx), static_cast<long long>(cfg.ny), shape); }
+    dim3 grid() const {
+        return cell_grid(static_cast<long long>(cfg.nx), static_cast<long long>(cfg.ny),
+                         static_cast<long long>(cfg.nz), block());
+    }
+    void set_device() const { check_cuda(cudaSetDevice(cfg.device), "cudaSetDevice"); }
+    void sync() {
+        check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+        ++syncs;
+    }
+};
+
+namespace {
+
+void require(bool ok, const char* message) {
+    if (!ok) throw std::invalid_argument(message);
+}
+
+cfdx_lbm* checked(cfdx_lbm* h) {
+    if (!h) throw std::invalid_argument("null cfdx_lbm handle");
+    h->set_device();
+    return h;
+}
+
+void default_scales(cfdx_lbm* h) {
+    // Power of two nearest 1/w_d: (f - w_d) * s_d is then the relative
+    // deviation from the rest weight, which keeps small deviations out of the
+    // FP16 subnormal range; powers of two make the scaling exact.
+    for (int d = 0; d < 27; ++d) {
+        if (d >= h->key.q) {
+            h->scale[d] = 1.0F;
+            continue;
+        }
+        const double w = lattice_weight(h->key.q, d);
+        h->scale[d] = static_cast<float>(std::ldexp(1.0, static_cast<int>(std::lround(std::log2(1.0 / w)))));
+    }
+}
+
+// Copies a caller buffer (host or device) into device memory `dst`.
+void upload(cfdx_lbm* h, void* dst, const void* src, std::size_t bytes, int where) {
+    require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+    const cudaMemcpyKind kind = where == CFDX_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    check_cuda(cudaMemcpyAsync(dst, src, bytes, kind, h->stream), "cudaMemcpyAsync (upload)");
+    if (where == CFDX_HOST) {
+        h->h2d += bytes;
+        h->sync(); // the caller may release its host buffer on return
+    }
+}
+
+void download(cfdx_lbm* h, void* dst, const void* src, std::size_t bytes, int where) {
+    require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+    const cudaMemcpyKind kind = where == CFDX_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    check_cuda(cudaMemcpyAsync(dst, src, bytes, kind, h->stream), "cudaMemcpyAsync (download)");
+    if (where == CFDX_HOST) h->d2h += bytes;
+    h->sync();
+}
+
+void init_state(cfdx_lbm* h, const InitSpec& spec) {
+    // Zero first: wall cells and wall-only slots are never written by the init
+    // kernel and must not hold stale or non-finite data.
+    check_cuda(cudaMemsetAsync(h->f, 0, h->f_bytes, h->stream), "cudaMemsetAsync");
+    check_cuda(launch_init(h->key, h->args(), spec, h->grid(), h->block(), h->stream), "init kernel");
+    h->t = 0;
+}
+
+void ensure_reduce(cfdx_lbm* h) {
+    if (h->reduce_partials) return;
+    int sms = 0;
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->cfg.device), "device attribute");
+    const long long rows = static_cast<long long>(h->cfg.ny * h->cfg.nz);
+    h->reduce_blocks = static_cast<int>(std::max(1LL, std::min<long long>(4LL * sms, rows)));
+    h->reduce_partials = static_cast<double*>(
+        device_alloc(sizeof(double) * kReduceFields * static_cast<std::size_t>(h->reduce_blocks), "reduction scratch"));
+    h->reduce_out = static_cast<double*>(device_alloc(sizeof(double) * kReduceFields, "reduction output"));
+    check_cuda(cudaMallocHost(&h->host_reduce, sizeof(double) * kReduceFields), "cudaMallocHost");
+}
+
+void release(cfdx_lbm* h) {
+    if (!h) return;
+    cudaSetDevice(h->cfg.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    device_free(h->f);
+    device_free(h->flags);
+    device_free(h->local_a);
+    device_free(h->ns);
+    device_free(h->macro_scratch);
+    device_free(h->reduce_partials);
+    device_free(h->reduce_out);
+    if (h->host_reduce) cudaFreeHost(h->host_reduce);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+} // namespace
+
+namespace cfdx {
+
+dim3 cell_block(long long nx, long long ny, const LaunchShape& s) {
+    int bx = s.block_x, by = s.block_y;
+    if (bx <= 0 || by <= 0) {
+        bx = static_cast<int>(std::min<long long>(128, ((nx + 31) / 32) * 32));
+        by = std::max(1, 128 / bx);
+        by = static_cast<int>(std::min<long long>(by, ny));
+    }
+    return dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by), 1U);
+}
+
+dim3 cell_grid(long long nx, long long ny, long long nz, dim3 block) {
+    return dim3(static_cast<unsigned>((nx + block.x - 1) / block.x), static_cast<unsigned>((ny + block.y - 1) / block.y),
+                static_cast<unsigned>(nz));
+}
+
+cudaError_t launch_step(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::step(k, a, g, b, s);
+    case kStoreF64: return Launcher<kStoreF64>::step(k, a, g, b, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::step(k, a, g, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_init(const KernelKey& k, const LbmArgs& a, const InitSpec& spec, dim3 g, dim3 b, cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::init(k, a, spec, g, b, s);
+    case kStoreF64: return Launcher<kStoreF64>::init(k, a, spec, g, b, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::init(k, a, spec, g, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_macro(const KernelKey& k, const LbmArgs& a, void* rho, void* ux, void* uy, void* uz, bool f64,
+                         dim3 g, dim3 b, cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::macro(k, a, rho, ux, uy, uz, f64, g, b, s);
+    case kStoreF64: return Launcher<kStoreF64>::macro(k, a, rho, ux, uy, uz, f64, g, b, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::macro(k, a, rho, ux, uy, uz, f64, g, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_logical(const KernelKey& k, const LbmArgs& a, float* out, dim3 g, dim3 b, cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::logical(k, a, out, g, b, s);
+    case kStoreF64: return Launcher<kStoreF64>::logical(k, a, out, g, b, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::logical(k, a, out, g, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_reduce(const KernelKey& k, const LbmArgs& a, double* partials, int blocks, double* out,
+                          cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::reduce(k, a, partials, blocks, out, s);
+    case kStoreF64: return Launcher<kStoreF64>::reduce(k, a, partials, blocks, out, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::reduce(k, a, partials, blocks, out, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+} // namespace cfdx
+
+extern "C" {
+
+CFDX_API const char* cfdx_version(void) { return "cfd_solvers_b200 0.1.0 (sm_100a)"; }
+
+CFDX_API int cfdx_last_error(char* buffer, std::size_t capacity) {
+    copy_error(buffer, capacity, g_error);
+    return g_error_status;
+}
+
+CFDX_API int cfdx_lbm_config_default(cfdx_lbm_config* c) {
+    return guarded([&] {
+        require(c != nullptr, "null config");
+        *c = cfdx_lbm_config{};
+        c->nx = c->ny = c->nz = 128;
+        c->tau = 0.6F;
+        c->lattice = CFDX_D3Q19;
+        c->collision = CFDX_BGK;
+        c->storage = CFDX_STORE_F32;
+        c->smagorinsky_cs = 0.0F;
+        c->trt_magic = 3.0F / 16.0F;
+        c->trt_tau_minus = 0.0F;
+        c->device = 0;
+    });
+}
+
+CFDX_API int cfdx_lbm_create(const cfdx_lbm_config* config, cfdx_lbm** out, char* error, std::size_t cap) {
+    cfdx_lbm* h = nullptr;
+    const int rc = guarded([&] {
+        require(config != nullptr && out != nullptr, "null config or output handle");
+        *out = nullptr;
+        const cfdx_lbm_config& c = *config;
+        // reference esoteric_pull.hpp:111-113,292-301
+        require(c.nx >= 2 && c.ny >= 2, "LBM grid requires nx, ny >= 2");
+        require(c.nz >= 2, "3-D LBM grid requires nz >= 2");
+        require(c.tau > 0.5F && std::isfinite(c.tau), "LBM tau must be > 0.5 for positive viscosity");
+        require(c.lattice == CFDX_D3Q19 || c.lattice == CFDX_D3Q27, "lattice must be CFDX_D3Q19 or CFDX_D3Q27");
+        require(c.collision == CFDX_BGK || c.collision == CFDX_TRT, "collision must be CFDX_BGK or CFDX_TRT");
+        require(c.storage == CFDX_STORE_F32 || c.storage == CFDX_STORE_F64 || c.storage == CFDX_STORE_F16S,
+                "unknown storage");
+        require(std::isfinite(c.acceleration_x) && std::isfinite(c.acceleration_y) && std::isfinite(c.acceleration_z),
+                "acceleration must be finite");
+        if (c.collision == CFDX_TRT)
+            require(c.trt_tau_minus > 0.5F || (c.trt_tau_minus <= 0.0F && c.trt_magic > 0.0F),
+                    "TRT needs trt_tau_minus > 0.5 or trt_magic > 0");
+        require(c.nx <= (1U << 30) && c.ny <= 65535U && c.nz <= 65535U, "grid extent exceeds launch limits");
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+            fail(CFDX_ERR_CUDA, "no CUDA device is available (the B200 engine has no CPU fallback)");
+        require(c.device >= 0 && c.device < count, "device ordinal out of range");
+        h = new cfdx_lbm();
+        h->cfg = c;
+        h->set_device();
+        h->N = c.nx * c.ny * c.nz;
+        h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false};
+        h->les_k = c.smagorinsky_les ? (c.smagorinsky_cs > 0.0F
+                                            ? 18.0 * std::sqrt(2.0) * double(c.smagorinsky_cs) * double(c.smagorinsky_cs)
+                                            : double(reference_les_k()))
+                                     : 0.0;
+        default_scales(h);
+        check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        h->f_bytes = static_cast<std::size_t>(c.lattice) * h->N * static_cast<std::size_t>(storage_bytes(c.storage));
+        h->f = device_alloc(h->f_bytes, "population lattice");
+        InitSpec spec{};
+        spec.kind = 0;
+        spec.rho = 1.0F;
+        init_state(h, spec); // reference constructor calls initialize_uniform()
+        h->sync();
+        *out = h;
+    });
+    if (rc != CFDX_OK) {
+        release(h);
+        copy_error(error, cap, g_error);
+    }
+    return rc;
+}
+
+CFDX_API int cfdx_lbm_destroy(cfdx_lbm* h) {
+    return guarded([&] { release(h); });
+}
+
+CFDX_API int cfdx_lbm_init_uniform(cfdx_lbm* h, float rho, float ux, float uy, float uz) {
+    return guarded([&] {
+        checked(h);
+        // reference esoteric_pull_sycl.hpp:53-56
+        require(rho > 0.0F && std::isfinite(rho) && std::isfinite(ux) && std::isfinite(uy) && std::isfinite(uz),
+                "LBM uniform state must be finite with positive density");
+        InitSpec s{};
+        s.kind = 0;
+        s.rho = rho;
+        s.ux = ux;
+        s.uy = uy;
+        s.uz = uz;
+        init_state(h, s);
+    });
+}
+
+CFDX_API int cfdx_lbm_init_taylor_green(cfdx_lbm* h, float amplitude) {
+    return guarded([&] {
+        checked(h);
+        require(std::isfinite(amplitude), "Taylor-Green amplitude must be finite");
+        InitSpec s{};
+        s.kind = 1;
+        s.amplitude = amplitude;
+        init_state(h, s);
+    });
+}
+
+CFDX_API int cfdx_lbm_init_fields(cfdx_lbm* h, const float* fields, int where) {
+    return guarded([&] {
+        checked(h);
+        require(fields != nullptr, "null fields");
+        float* tmp = static_cast<float*>(device_alloc(4U * h->N * sizeof(float), "init staging"));
+        try {
+            upload(h, tmp, fields, 4U * h->N * sizeof(float), where);
+            InitSpec s{};
+            s.kind = 2;
+            s.fields = tmp;
+            init_state(h, s);
+            h->sync();
+        } catch (...) {
+            device_free(tmp);
+            throw;
+        }
+        device_free(tmp);
+    });
+}
+
+CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
+    return guarded([&] {
+        checked(h);
+        if (!flags) {
+            h->key.flags = false;
+            return;
+        }
+        if (!h->flags) h->flags = static_cast<std::uint8_t*>(device_alloc(h->N, "flag field"));
+        std::uint8_t* user = static_cast<std::uint8_t*>(device_alloc(h->N, "flag staging"));
+        try {
+            upload(h, user, flags, h->N, where);
+            check_cuda(launch_prepare_flags(h->key.q, h->args(), user, h->flags, h->grid(), h->block(), h->stream),
+                       "flag preparation kernel");
+            h->sync();
+        } catch (...) {
+            device_free(user);
+            throw;
+        }
+        device_free(user);
+        h->key.flags = true;
+    });
+}
+
+CFDX_API int cfdx_lbm_set_wall_velocity(cfdx_lbm* h, int id, float ux, float uy, float uz) {
+    return guarded([&] {
+        checked(h);
+        if (id < CFDX_MOVING_WALL_MIN || id >= CFDX_MAX_WALL_IDS)
+            throw std::out_of_range("moving-wall id must be in [2, 15]");
+        require(std::isfinite(ux) && std::isfinite(uy) && std::isfinite(uz), "wall velocity must be finite");
+        h->wall_u[id][0] = ux;
+        h->wall_u[id][1] = uy;
+        h->wall_u[id][2] = uz;
+    });
+}
+
+CFDX_API int cfdx_lbm_set_local_acceleration(cfdx_lbm* h, const float* accel, int where) {
+    return guarded([&] {
+        checked(h);
+        if (!accel) {
+            device_free(h->local_a);
+            h->local_a = nullptr;
+            return;
+        }
+        if (!h->local_a) h->local_a = static_cast<float*>(device_alloc(3U * h->N * sizeof(float), "acceleration field"));
+        upload(h, h->local_a, accel, 3U * h->N * sizeof(float), where);
+    });
+}
+
+CFDX_API int cfdx_lbm_device_local_acceleration(cfdx_lbm* h, float** accel) {
+    return guarded([&] {
+        checked(h);
+        require(accel != nullptr, "null output pointer");
+        if (!h->local_a) {
+            h->local_a = static_cast<float*>(device_alloc(3U * h->N * sizeof(float), "acceleration field"));
+            check_cuda(cudaMemsetAsync(h->local_a, 0, 3U * h->N * sizeof(float), h->stream), "cudaMemsetAsync");
+            h->sync();
+        }
+        *accel = h->local_a;
+    });
+}
+
+CFDX_API int cfdx_lbm_set_solid_fraction(cfdx_lbm* h, const float* ns, int where) {
+    return guarded([&] {
+        checked(h);
+        if (!ns) {
+            device_free(h->ns);
+            h->ns = nullptr;
+            h->key.gray = false;
+            return;
+        }
+        if (!h->ns) h->ns = static_cast<float*>(device_alloc(h->N * sizeof(float), "solid fraction field"));
+        upload(h, h->ns, ns, h->N * sizeof(float), where);
+        h->key.gray = true;
+    });
+}
+
+CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* h, const float* scale) {
+    return guarded([&] {
+        checked(h);
+        require(h->key.storage == kStoreF16S, "storage scales apply to CFDX_STORE_F16S only");
+        if (!scale) {
+            default_scales(h);
+            return;
+        }
+        for (int d = 0; d < h->key.q; ++d)
+            require(std::isfinite(scale[d]) && scale[d] > 0.0F, "storage scales must be finite and positive");
+        for (int d = 1; d < h->key.q; d += 2)
+            require(scale[d] == scale[d + 1], "opposite directions must share a storage scale");
+        for (int d = 0; d < h->key.q; ++d) h->scale[d] = scale[d];
+    });
+}
+
+CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
+    return guarded([&] {
+        checked(h);
+        const dim3 g = h->grid(), b = h->block();
+        LbmArgs a = h->args();
+        for (std::uint64_t i = 0; i < count; ++i) {
+            a.odd = static_cast<int>(h->t & 1U);
+            check_cuda(launch_step(h->key, a, g, b, h->stream), "step kernel");
+            ++h->t;
+        }
+    });
+}
+
+CFDX_API int cfdx_lbm_synchronize(cfdx_lbm* h) {
+    return guarded([&] {
+        checked(h);
+        h->sync();
+    });
+}
+
+CFDX_API int cfdx_lbm_macroscopic(cfdx_lbm* h, float* rho, float* ux, float* uy, float* uz, int where) {
+    return guarded([&] {
+        checked(h);
+        require(rho && ux && uy && uz, "null output buffer");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        const std::size_t bytes = h->N * sizeof(float);
+        if (where == CFDX_DEVICE) {
+            check_cuda(launch_macro(h->key, h->args(), rho, ux, uy, uz, false, h->grid(), h->block(), h->stream),
+                       "macroscopic kernel");
+            h->sync();
+            return;
+        }
+        if (!h->macro_scratch)
+            h->macro_scratch = static_cast<float*>(device_alloc(4U * bytes, "macroscopic scratch"));
+        float* s = h->macro_scratch;
+        check_cuda(launch_macro(h->key, h->args(), s, s + h->N, s + 2 * h->N, s + 3 * h->N, false, h->grid(),
+                                h->block(), h->stream),
+                   "macroscopic kernel");
+        float* outs[4] = {rho, ux, uy, uz};
+        for (int k = 0; k < 4; ++k)
+            check_cuda(cudaMemcpyAsync(outs[k], s + k * h->N, bytes, cudaMemcpyDeviceToHost, h->stream),
+                       "cudaMemcpyAsync (macroscopic)");
+        h->d2h += 4U * bytes;
+        h->sync();
+    });
+}
+
+CFDX_API int cfdx_lbm_macroscopic_f64(cfdx_lbm* h, double* rho, double* ux, double* uy, double* uz, int where) {
+    return guarded([&] {
+        checked(h);
+        require(rho && ux && uy && uz, "null output buffer");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        const std::size_t bytes = h->N * sizeof(double);
+        if (where == CFDX_DEVICE) {
+            check_cuda(launch_macro(h->key, h->args(), rho, ux, uy, uz, true, h->grid(), h->block(), h->stream),
+                       "macroscopic kernel");
+            h->sync();
+            return;
+        }
+        double* s = static_cast<double*>(device_alloc(4U * bytes, "macroscopic staging"));
+        try {
+            check_cuda(launch_macro(h->key, h->args(), s, s + h->N, s + 2 * h->N, s + 3 * h->N, true, h->grid(),
+                                    h->block(), h->stream),
+                       "macroscopic kernel");
+            double* outs[4] = {rho, ux, uy, uz};
+            for (int k = 0; k < 4; ++k)
+                check_cuda(cudaMemcpyAsync(outs[k], s + k * h->N, bytes, cudaMemcpyDeviceToHost, h->stream),
+                           "cudaMemcpyAsync (macroscopic)");
+            h->d2h += 4U * bytes;
+            h->sync();
+        } catch (...) {
+            device_free(s);
+            throw;
+        }
+        device_free(s);
+    });
+}
+
+CFDX_API int cfdx_lbm_refresh_device_macroscopic(cfdx_lbm* h, float** rho, float** ux, float** uy, float** uz) {
+    return guarded([&] {
+        checked(h);
+        require(rho && ux && uy && uz, "null output pointer");
+        if (!h->macro_scratch)
+            h->macro_scratch = static_cast<float*>(device_alloc(4U * h->N * sizeof(float), "macroscopic scratch"));
+        float* s = h->macro_scratch;
+        check_cuda(launch_macro(h->key, h->args(), s, s + h->N, s + 2 * h->N, s + 3 * h->N, false, h->grid(),
+                                h->block(), h->stream),
+                   "macroscopic kernel");
+        *rho = s;
+        *ux = s + h->N;
+        *uy = s + 2 * h->N;
+        *uz = s + 3 * h->N;
+    });
+}
+
+CFDX_API int cfdx_lbm_reduce(cfdx_lbm* h, double* out) {
+    int nonfinite = 0;
+    const int rc = guarded([&] {
+        checked(h);
+        require(out != nullptr, "null output");
+        ensure_reduce(h);
+        check_cuda(launch_reduce(h->key, h->args(), h->reduce_partials, h->reduce_blocks, h->reduce_out, h->stream),
+                   "reduction kernel");
+        check_cuda(cudaMemcpyAsync(h->host_reduce, h->reduce_out, sizeof(double) * kReduceFields,
+                                   cudaMemcpyDeviceToHost, h->stream),
+                   "cudaMemcpyAsync (reduction)");
+        h->d2h += sizeof(double) * kReduceFields;
+        h->sync();
+        for (int k = 0; k < kReduceFields; ++k) out[k] = h->host_reduce[k];
+        out[CFDX_REDUCE_KINETIC_ENERGY] *= 0.5;
+        nonfinite = out[CFDX_REDUCE_NONFINITE] > 0.0;
+    });
+    if (rc == CFDX_OK && nonfinite) {
+        g_error = "non-finite populations in " + std::to_string(static_cast<long long>(out[CFDX_REDUCE_NONFINITE])) +
+                  " fluid cells";
+        g_error_status = CFDX_ERR_NONFINITE;
+        return CFDX_ERR_NONFINITE;
+    }
+    return rc;
+}
+
+CFDX_API int cfdx_lbm_checksum(cfdx_lbm* h, double* checksum) {
+    double r[kReduceFields];
+    if (!checksum) {
+        g_error = "null output";
+        g_error_status = CFDX_ERR_INVALID;
+        return CFDX_ERR_INVALID;
+    }
+    const int rc = cfdx_lbm_reduce(h, r);
+    if (rc == CFDX_OK || rc == CFDX_ERR_NONFINITE) *checksum = r[CFDX_REDUCE_MASS] + r[CFDX_REDUCE_KINETIC_ENERGY];
+    return rc;
+}
+
+CFDX_API int cfdx_lbm_logical_populations(cfdx_lbm* h, float* out, int where) {
+    return guarded([&] {
+        checked(h);
+        require(out != nullptr, "null output buffer");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        const std::size_t bytes = static_cast<std::size_t>(h->key.q) * h->N * sizeof(float);
+        if (where == CFDX_DEVICE) {
+            check_cuda(launch_logical(h->key, h->args(), out, h->grid(), h->block(), h->stream), "logical kernel");
+            h->sync();
+            return;
+        }
+        float* tmp = static_cast<float*>(device_alloc(bytes, "logical staging"));
+        try {
+            check_cuda(launch_logical(h->key, h->args(), tmp, h->grid(), h->block(), h->stream), "logical kernel");
+            download(h, out, tmp, bytes, CFDX_HOST);
+        } catch (...) {
+            device_free(tmp);
+            throw;
+        }
+        device_free(tmp);
+    });
+}
+
+CFDX_API int cfdx_lbm_get_info(cfdx_lbm* h, cfdx_lbm_info* info) {
+    return guarded([&] {
+        require(h != nullptr && info != nullptr, "null handle or info");
+        info->cells = h->N;
+        info->q = h->key.q;
+        info->storage = h->key.storage;
+        info->time_step = h->t;
+        info->population_bytes = h->f_bytes;
+        std::size_t r = h->f_bytes;
+        if (h->flags) r += h->N;
+        if (h->local_a) r += 3U * h->N * sizeof(float);
+        if (h->ns) r += h->N * sizeof(float);
+        if (h->macro_scratch) r += 4U * h->N * sizeof(float);
+        if (h->reduce_partials) r += sizeof(double) * kReduceFields * (static_cast<std::size_t>(h->reduce_blocks) + 1U);
+        info->resident_bytes = r;
+        info->host_to_device_bytes = h->h2d;
+        info->device_to_host_bytes = h->d2h;
+        info->synchronizations = h->syncs;
+        info->fluid_flags = h->key.flags ? 1 : 0;
+    });
+}
+
+CFDX_API int cfdx_lbm_stream(cfdx_lbm* h, void** stream) {
+    return guarded([&] {
+        require(h != nullptr && stream != nullptr, "null handle or output");
+        *stream = h->stream;
+    });
+}
+
+CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* h, void** ptr, std::size_t* bytes) {
+    return guarded([&] {
+        require(h != nullptr && ptr != nullptr && bytes != nullptr, "null handle or output");
+        *ptr = h->f;
+        *bytes = h->f_bytes;
+    });
+}
+
+CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by) {
+    return guarded([&] {
+        require(h != nullptr, "null handle");
+        if (bx == 0 && by == 0) {
+            h->shape = LaunchShape{};
+            return;
+        }
+        require(bx > 0 && by > 0 && bx * by <= 256 && (bx * by) % 32 == 0,
+                "block shape must have bx*by a multiple of 32 and at most 256");
+        h->shape = LaunchShape{bx, by};
+    });
+}
+
+CFDX_API int cfdx_debug_fail_allocations(int count) {
+    g_fail_allocations.store(count > 0 ? count : 0);
+    return CFDX_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,53 @@
+// Launch arguments shared by the host dispatcher and the device kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace cfdx {
+
+constexpr int kMaxWallIds = 16;
+
+// Internal per-cell flag byte, derived on the device from the caller's flags
+// (0 fluid, 1 stationary wall, 2..15 moving wall id):
+//   bits 0-3  wall id (0 = fluid)
+//   bit 6     fluid cell with a moving-wall neighbour
+//   bit 7     fluid cell with at least one wall neighbour
+constexpr std::uint8_t kFlagTypeMask = 0x0f;
+constexpr std::uint8_t kFlagNearMoving = 0x40;
+constexpr std::uint8_t kFlagNearWall = 0x80;
+
+enum Storage : int { kStoreF32 = 0, kStoreF64 = 1, kStoreF16S = 2 };
+enum Collision : int { kBGK = 0, kTRT = 1 };
+
+struct LbmArgs {
+    void* f;                   // populations, [q][N] structure of arrays
+    const std::uint8_t* flags; // internal flags or nullptr
+    const float* local_a;      // 3*N per-cell acceleration (ax|ay|az) or nullptr
+    const float* ns;           // N gray-LBM solid fractions or nullptr
+    long long nx, ny, nz;
+    std::size_t N;
+    int odd;                   // parity of the time step being executed / read
+    double tau;                // base symmetric relaxation time
+    double omega_minus;        // TRT antisymmetric rate when fixed (> 0), else from magic
+    double trt_magic;
+    double les_k;              // Smagorinsky K (0 = off)
+    double ax, ay, az;         // uniform acceleration
+    float wall_u[kMaxWallIds][3];
+    float scale[27];           // FP16S per-direction scale
+    float inv_scale[27];
+};
+
+// Initial state for k_init.
+struct InitSpec {
+    int kind; // 0 uniform, 1 Taylor-Green, 2 per-cell fields
+    float rho, ux, uy, uz, amplitude;
+    const float* fields; // 4*N (rho|ux|uy|uz), device
+};
+
+// Output of the fluid-cell reduction, accumulated in FP64.
+constexpr int kReduceFields = 7; // mass, mx, my, mz, 2*KE, max|u|, non-finite cells
+
+} // namespace cfdx

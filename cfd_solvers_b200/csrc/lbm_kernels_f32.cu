@@ -1,0 +1,23 @@
+// Kernel instantiations for one population storage type (compiled separately
+// to keep build times parallel).
+#include "lbm_launch_impl.cuh"
+
+namespace cfdx {
+template struct Launcher<kStoreF32>;
+} // namespace cfdx
+
+namespace cfdx {
+
+// Flag preparation does not depend on the storage type; it lives here once.
+cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out, dim3 g, dim3 b,
+                                 cudaStream_t s) {
+    if (q == 19)
+        k_prepare_flags<D3Q19><<<g, b, 0, s>>>(a, user, out);
+    else if (q == 27)
+        k_prepare_flags<D3Q27><<<g, b, 0, s>>>(a, user, out);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+} // namespace cfdx

@@ -1,0 +1,54 @@
+// Host-side launch interface of the lattice kernels (one implementation per
+// storage type, compiled in separate translation units).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "lbm_args.h"
+
+namespace cfdx {
+
+struct LaunchShape {
+    int block_x = 0; // 0 = choose from nx
+    int block_y = 0;
+};
+
+// Kernel selection that is fixed per handle.
+struct KernelKey {
+    int storage;   // Storage
+    int q;         // 19 / 27
+    int collision; // Collision
+    bool les;
+    bool flags;
+    bool gray;
+};
+
+dim3 cell_block(long long nx, long long ny, const LaunchShape& s);
+dim3 cell_grid(long long nx, long long ny, long long nz, dim3 block);
+
+template <int STORAGE> struct Launcher {
+    static cudaError_t step(const KernelKey& k, const LbmArgs& a, dim3 grid, dim3 block, cudaStream_t s);
+    static cudaError_t init(const KernelKey& k, const LbmArgs& a, const InitSpec& spec, dim3 grid, dim3 block,
+                            cudaStream_t s);
+    static cudaError_t macro(const KernelKey& k, const LbmArgs& a, void* rho, void* ux, void* uy, void* uz,
+                             bool out_f64, dim3 grid, dim3 block, cudaStream_t s);
+    static cudaError_t logical(const KernelKey& k, const LbmArgs& a, float* out, dim3 grid, dim3 block,
+                               cudaStream_t s);
+    static cudaError_t reduce(const KernelKey& k, const LbmArgs& a, double* partials, int blocks, double* out,
+                              cudaStream_t s);
+};
+
+cudaError_t launch_step(const KernelKey& k, const LbmArgs& a, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t launch_init(const KernelKey& k, const LbmArgs& a, const InitSpec& spec, dim3 grid, dim3 block,
+                        cudaStream_t s);
+cudaError_t launch_macro(const KernelKey& k, const LbmArgs& a, void* rho, void* ux, void* uy, void* uz,
+                         bool out_f64, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t launch_logical(const KernelKey& k, const LbmArgs& a, float* out, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t launch_reduce(const KernelKey& k, const LbmArgs& a, double* partials, int blocks, double* out,
+                          cudaStream_t s);
+cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out, dim3 grid,
+                                 dim3 block, cudaStream_t s);
+
+} // namespace cfdx

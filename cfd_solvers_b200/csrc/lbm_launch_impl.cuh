@@ -1,0 +1,125 @@
+// Template dispatch from a runtime KernelKey to the kernel instantiations of
+// one storage type.  Included by lbm_kernels_{f32,f16s,f64}.cu only.
+#pragma once
+
+#include "lbm_device.cuh"
+#include "lbm_launch.h"
+
+namespace cfdx {
+
+template <int STORAGE> struct StorageOf;
+template <> struct StorageOf<kStoreF32> {
+    using type = StF32;
+};
+template <> struct StorageOf<kStoreF64> {
+    using type = StF64;
+};
+template <> struct StorageOf<kStoreF16S> {
+    using type = StF16;
+};
+
+template <class F> cudaError_t with_lattice(int q, F&& f) {
+    if (q == 19) return f(D3Q19{});
+    if (q == 27) return f(D3Q27{});
+    return cudaErrorInvalidValue;
+}
+
+template <class L, class S, int C, bool LES, bool FL>
+cudaError_t step_gray(bool gray, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    if (gray)
+        k_step<L, S, C, LES, FL, true><<<g, b, 0, s>>>(a);
+    else
+        k_step<L, S, C, LES, FL, false><<<g, b, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class L, class S, int C, bool LES>
+cudaError_t step_flags(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    return k.flags ? step_gray<L, S, C, LES, true>(k.gray, a, g, b, s) : step_gray<L, S, C, LES, false>(k.gray, a, g, b, s);
+}
+
+template <class L, class S, int C>
+cudaError_t step_les(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    return k.les ? step_flags<L, S, C, true>(k, a, g, b, s) : step_flags<L, S, C, false>(k, a, g, b, s);
+}
+
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::step(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        return k.collision == kTRT ? step_les<L, S, kTRT>(k, a, g, b, s) : step_les<L, S, kBGK>(k, a, g, b, s);
+    });
+}
+
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::init(const KernelKey& k, const LbmArgs& a, const InitSpec& spec, dim3 g, dim3 b,
+                                    cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        if (k.flags)
+            k_init<L, S, true><<<g, b, 0, s>>>(a, spec);
+        else
+            k_init<L, S, false><<<g, b, 0, s>>>(a, spec);
+        return cudaGetLastError();
+    });
+}
+
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::macro(const KernelKey& k, const LbmArgs& a, void* rho, void* ux, void* uy, void* uz,
+                                     bool out_f64, dim3 g, dim3 b, cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        if (out_f64) {
+            auto r = static_cast<double*>(rho), x = static_cast<double*>(ux), y = static_cast<double*>(uy),
+                 z = static_cast<double*>(uz);
+            if (k.flags)
+                k_macro<L, S, true, double><<<g, b, 0, s>>>(a, r, x, y, z);
+            else
+                k_macro<L, S, false, double><<<g, b, 0, s>>>(a, r, x, y, z);
+        } else {
+            auto r = static_cast<float*>(rho), x = static_cast<float*>(ux), y = static_cast<float*>(uy),
+                 z = static_cast<float*>(uz);
+            if (k.flags)
+                k_macro<L, S, true, float><<<g, b, 0, s>>>(a, r, x, y, z);
+            else
+                k_macro<L, S, false, float><<<g, b, 0, s>>>(a, r, x, y, z);
+        }
+        return cudaGetLastError();
+    });
+}
+
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::logical(const KernelKey& k, const LbmArgs& a, float* out, dim3 g, dim3 b,
+                                       cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        if (k.flags)
+            k_logical<L, S, true, float><<<g, b, 0, s>>>(a, out);
+        else
+            k_logical<L, S, false, float><<<g, b, 0, s>>>(a, out);
+        return cudaGetLastError();
+    });
+}
+
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::reduce(const KernelKey& k, const LbmArgs& a, double* partials, int blocks, double* out,
+                                      cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        if (k.flags)
+            k_reduce<L, S, true><<<blocks, kReduceThreads, 0, s>>>(a, partials);
+        else
+            k_reduce<L, S, false><<<blocks, kReduceThreads, 0, s>>>(a, partials);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        k_reduce_final<<<1, kReduceThreads, 0, s>>>(partials, blocks, out);
+        return cudaGetLastError();
+    });
+}
+
+} // namespace cfdx

@@ -1,0 +1,232 @@
+/*
+ * cfdx_lbm.h -- C ABI of the B200 in-place Esoteric-Pull lattice-Boltzmann engine.
+ *
+ * Plain C types only (pointers, sizes, ints, floats); no CUDA or torch types
+ * appear in any signature.  Every entry point returns an int status
+ * (CFDX_OK = 0) and never throws or aborts; the message of the last failure on
+ * the calling thread is available through cfdx_last_error().  The status and
+ * error-copy convention follows the reference C ABI
+ * (include/cfd/python/c_api.h:3-12, src/python/c_api.cpp:8-16: 0 ok,
+ * 1 std::exception, 2 unknown), extended with CUDA-specific codes.
+ *
+ * Each entry point replaces one member of the reference solver classes
+ *   cfd::lbm::EsotericPullSolver<D>      include/cfd/solvers/lbm/esoteric_pull.hpp:104-515
+ *   cfd::lbm::EsotericPullSyclSolver<D>  include/cfd/solvers/lbm/esoteric_pull_sycl.hpp:18-475
+ * as cited beside it.  The reference has no C ABI for this path; the C++
+ * class cfd::lbm::EsotericPullCudaSolver<D> (include/cfd/solvers/lbm/
+ * esoteric_pull_cuda.hpp) and the Python package cfd_solvers_b200 are thin
+ * layers over these functions.
+ *
+ * Threading: a handle is not thread-safe; use one handle per thread or
+ * serialise calls.  Each handle owns one CUDA stream; cfdx_lbm_step() is
+ * asynchronous on it, every call that returns data to the caller
+ * synchronises it.
+ */
+#ifndef CFDX_LBM_H
+#define CFDX_LBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define CFDX_API __declspec(dllexport)
+#else
+#define CFDX_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define CFDX_OK 0
+#define CFDX_ERR_INVALID 1   /* invalid argument / configuration (std::invalid_argument in the reference) */
+#define CFDX_ERR_UNKNOWN 2   /* unknown failure */
+#define CFDX_ERR_CUDA 3      /* CUDA runtime error, including "no CUDA device" */
+#define CFDX_ERR_OOM 4       /* device allocation failed (std::bad_alloc in the reference) */
+#define CFDX_ERR_NONFINITE 5 /* a reduction met NaN/Inf populations */
+#define CFDX_ERR_IO 6        /* checkpoint file could not be written or read / is corrupt */
+#define CFDX_ERR_RANGE 7     /* index out of range (std::out_of_range in the reference) */
+
+/* Lattices (value = q). */
+#define CFDX_D3Q19 19
+#define CFDX_D3Q27 27
+
+/* Population storage. */
+#define CFDX_STORE_F32 0  /* FP32 populations, FP32 arithmetic (the reference's layout) */
+#define CFDX_STORE_F64 1  /* FP64 populations, FP64 arithmetic (at-scale FP64 oracle) */
+#define CFDX_STORE_F16S 2 /* FP16 shifted populations h = half((f - w_d) * s_d), FP32 arithmetic */
+
+/* Collision operators. */
+#define CFDX_BGK 0 /* single relaxation time (esoteric_pull.hpp:408-432) */
+#define CFDX_TRT 1 /* two relaxation times (one_step_pull.hpp:187-204) */
+
+/* Where a caller buffer lives. */
+#define CFDX_HOST 0
+#define CFDX_DEVICE 1
+
+/* Cell flags passed to cfdx_lbm_set_flags(). */
+#define CFDX_FLUID 0
+#define CFDX_WALL 1       /* stationary half-way bounce-back wall */
+#define CFDX_MOVING_WALL_MIN 2
+#define CFDX_MAX_WALL_IDS 16 /* ids 2..15 are moving walls with a velocity from cfdx_lbm_set_wall_velocity() */
+
+/* Reduction slots of cfdx_lbm_reduce(). */
+#define CFDX_REDUCE_MASS 0
+#define CFDX_REDUCE_MOMENTUM_X 1
+#define CFDX_REDUCE_MOMENTUM_Y 2
+#define CFDX_REDUCE_MOMENTUM_Z 3
+#define CFDX_REDUCE_KINETIC_ENERGY 4
+#define CFDX_REDUCE_MAX_SPEED 5
+#define CFDX_REDUCE_NONFINITE 6
+#define CFDX_REDUCE_COUNT 7
+
+typedef struct cfdx_lbm cfdx_lbm; /* opaque handle */
+
+/* Solver configuration.  The first eight fields are the reference's
+ * InPlaceLbmConfig (esoteric_pull.hpp:20-29); the rest extend it. */
+typedef struct cfdx_lbm_config {
+    size_t nx, ny, nz;
+    float tau;               /* > 0.5 */
+    float acceleration_x;    /* uniform body acceleration (Guo forcing) */
+    float acceleration_y;
+    float acceleration_z;
+    int smagorinsky_les;     /* 0/1 */
+    int lattice;             /* CFDX_D3Q19 / CFDX_D3Q27 */
+    int collision;           /* CFDX_BGK / CFDX_TRT */
+    int storage;             /* CFDX_STORE_* */
+    float smagorinsky_cs;    /* <= 0: the reference's fixed coefficient (Cs = sqrt(8/27)/pi) */
+    float trt_magic;         /* TRT magic parameter Lambda (default 3/16) */
+    float trt_tau_minus;     /* > 0: fixed antisymmetric relaxation time instead of Lambda */
+    int device;              /* CUDA device ordinal */
+} cfdx_lbm_config;
+
+/* Handle information. */
+typedef struct cfdx_lbm_info {
+    size_t cells;
+    int q;
+    int storage;
+    uint64_t time_step;          /* reference time_step(), esoteric_pull.hpp:271 */
+    size_t population_bytes;     /* reference population_bytes(), esoteric_pull.hpp:272-274 */
+    size_t resident_bytes;       /* reference SYCL resident_bytes(), esoteric_pull_sycl.hpp:387-391 */
+    uint64_t host_to_device_bytes; /* reference DeviceTransferStats, core/device_residency.hpp:11-42 */
+    uint64_t device_to_host_bytes;
+    uint64_t synchronizations;
+    int fluid_flags;             /* 1 when a flag field is active */
+} cfdx_lbm_info;
+
+/* Library version string. Replaces cfd_solvers_version (c_api.h:11). */
+CFDX_API const char* cfdx_version(void);
+
+/* Copies the calling thread's last error message (error-copy convention of
+ * src/python/c_api.cpp:8).  Returns the status of that failure. */
+CFDX_API int cfdx_last_error(char* buffer, size_t capacity);
+
+/* Fills *config with defaults (128^3 D3Q19 BGK FP32, tau 0.6, Lambda 3/16).
+ * Reference: InPlaceLbmConfig defaults, esoteric_pull.hpp:20-29. */
+CFDX_API int cfdx_lbm_config_default(cfdx_lbm_config* config);
+
+/* Allocates the single population lattice on the device and initialises it
+ * to rest (rho = 1).  Reference: EsotericPullSolver(InPlaceLbmConfig),
+ * esoteric_pull.hpp:109-115; EsotericPullSyclSolver ctor, esoteric_pull_sycl.hpp:23-33.
+ * error/error_capacity may be NULL/0. */
+CFDX_API int cfdx_lbm_create(const cfdx_lbm_config* config, cfdx_lbm** out, char* error, size_t error_capacity);
+
+/* Frees every device buffer of the handle.  Reference: ~EsotericPullSyclSolver, esoteric_pull_sycl.hpp:35-45. */
+CFDX_API int cfdx_lbm_destroy(cfdx_lbm* lbm);
+
+/* Reference: initialize_uniform, esoteric_pull.hpp:117-119 / esoteric_pull_sycl.hpp:52-60. */
+CFDX_API int cfdx_lbm_init_uniform(cfdx_lbm* lbm, float rho, float ux, float uy, float uz);
+
+/* Reference: initialize_taylor_green, esoteric_pull.hpp:121-137 / esoteric_pull_sycl.hpp:62-85. */
+CFDX_API int cfdx_lbm_init_taylor_green(cfdx_lbm* lbm, float amplitude);
+
+/* Equilibrium from per-cell fields rho|ux|uy|uz (4*N floats, host or device).
+ * Reference: the initializer callback of initialize, esoteric_pull.hpp:312-333. */
+CFDX_API int cfdx_lbm_init_fields(cfdx_lbm* lbm, const float* fields, int where);
+
+/* Cell flags (N bytes, host or device): 0 fluid, 1 wall, 2..15 moving wall.
+ * NULL clears.  Half-way bounce-back is applied in place.  Set flags before
+ * initialising.  Reference: set_solid_mask / clear_solid_mask,
+ * esoteric_pull.hpp:161-177 (mask != 0 => wall). */
+CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* lbm, const uint8_t* flags, int where);
+
+/* Velocity of moving-wall id (2..15).  Formula: reference src/lbm/d2q9.cpp:109-115,220-223. */
+CFDX_API int cfdx_lbm_set_wall_velocity(cfdx_lbm* lbm, int wall_id, float ux, float uy, float uz);
+
+/* Per-cell acceleration ax|ay|az (3*N floats, host or device); NULL clears.
+ * Reference: set_local_body_acceleration / clear_local_body_acceleration,
+ * esoteric_pull.hpp:144-157; esoteric_pull_sycl.hpp:355-372. */
+CFDX_API int cfdx_lbm_set_local_acceleration(cfdx_lbm* lbm, const float* accel, int where);
+
+/* Device pointer to the per-cell acceleration buffer (3*N floats), allocated
+ * and zeroed on first use.  Reference: device_local_acceleration, esoteric_pull_sycl.hpp:349-353. */
+CFDX_API int cfdx_lbm_device_local_acceleration(cfdx_lbm* lbm, float** accel);
+
+/* Gray-LBM solid fraction n_s per cell (N floats in [0,1), host or device);
+ * NULL clears.  Partial bounce-back f_i <- (1-n_s) f_i* + n_s f_opp(i).
+ * No reference counterpart (Walsh, Burwinkle & Saar 2009). */
+CFDX_API int cfdx_lbm_set_solid_fraction(cfdx_lbm* lbm, const float* ns, int where);
+
+/* FP16S only: q per-direction scales s_d (opposite directions must share a
+ * scale); NULL restores the default power-of-two scales near 1/w_d.
+ * Reference codec: ShiftedHalfCodec (s_d = 1), compressed_pull.hpp:71-79. */
+CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* lbm, const float* scale);
+
+/* Enqueues count fused stream+collide steps.  Reference: step(count),
+ * esoteric_pull.hpp:139-142 / esoteric_pull_sycl.hpp:87-211. */
+CFDX_API int cfdx_lbm_step(cfdx_lbm* lbm, uint64_t count);
+
+/* Waits for all work of the handle.  Reference: wait(), esoteric_pull_sycl.hpp:213-216. */
+CFDX_API int cfdx_lbm_synchronize(cfdx_lbm* lbm);
+
+/* rho and u + a/2 per cell into caller buffers (N floats each; host or
+ * device); wall cells report 0.  Reference: compute_macroscopic,
+ * esoteric_pull.hpp:180-209; download_macroscopic, esoteric_pull_sycl.hpp:309-325. */
+CFDX_API int cfdx_lbm_macroscopic(cfdx_lbm* lbm, float* rho, float* ux, float* uy, float* uz, int where);
+
+/* Same in double precision (N doubles each); exact for CFDX_STORE_F64. */
+CFDX_API int cfdx_lbm_macroscopic_f64(cfdx_lbm* lbm, double* rho, double* ux, double* uy, double* uz, int where);
+
+/* Device pointers to a handle-owned rho|ux|uy|uz scratch (4*N floats)
+ * refreshed from the current state.  Reference: refresh_device_macroscopic,
+ * esoteric_pull_sycl.hpp:226-307. */
+CFDX_API int cfdx_lbm_refresh_device_macroscopic(cfdx_lbm* lbm, float** rho, float** ux, float** uy, float** uz);
+
+/* FP64-accumulated reductions over fluid cells into out[CFDX_REDUCE_COUNT]
+ * (mass, momentum xyz, kinetic energy 0.5*sum rho|u|^2, max |u|, non-finite
+ * cell count).  Returns CFDX_ERR_NONFINITE (with out filled) when any fluid
+ * cell is NaN/Inf.  Reference: mass, kinetic_energy, max_speed,
+ * esoteric_pull.hpp:211-255; total_mass, esoteric_pull_sycl.hpp:327-339. */
+CFDX_API int cfdx_lbm_reduce(cfdx_lbm* lbm, double* out);
+
+/* mass + kinetic energy (the checksum of examples/phase02_lbm_taylor_green.cpp:3). */
+CFDX_API int cfdx_lbm_checksum(cfdx_lbm* lbm, double* checksum);
+
+/* Parity-independent populations [d][n] (q*N floats, host or device).
+ * Reference: logical_populations, esoteric_pull.hpp:257-267. */
+CFDX_API int cfdx_lbm_logical_populations(cfdx_lbm* lbm, float* out, int where);
+
+/* Reference: time_step, population_bytes, cells, resident_bytes, transfer_stats. */
+CFDX_API int cfdx_lbm_get_info(cfdx_lbm* lbm, cfdx_lbm_info* info);
+
+/* The handle's CUDA stream (a cudaStream_t) for callers that time or order
+ * work around the step. */
+CFDX_API int cfdx_lbm_stream(cfdx_lbm* lbm, void** stream);
+
+/* Device pointer and size of the raw population storage (esoteric layout).
+ * Reference: raw_storage, esoteric_pull.hpp:276-278. */
+CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* lbm, void** device_ptr, size_t* bytes);
+
+/* Threads per block of the cell kernels (x, y); 0,0 restores the default. */
+CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y);
+
+/* Test hook: the next `count` device allocations of this process fail with
+ * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
+ * without exhausting the device. */
+CFDX_API int cfdx_debug_fail_allocations(int count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFDX_LBM_H */

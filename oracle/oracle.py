@@ -1,0 +1,346 @@
+"""ctypes access to the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, the smoke check in __graft_entry__.py and the CPU-baseline leg
+of bench.py import this module.  It wraps
+
+* ``liblbm_oracle.so`` -- the C restatement of the reference's in-place
+  Esoteric-Pull step (lbm_oracle.h), and
+* ``_ref/libcfdref.so`` / ``_ref/libcfdref_fast.so`` -- the reference's own
+  CPU solvers compiled from its sources by oracle/Makefile
+  (include/cfd/solvers/lbm/esoteric_pull.hpp, one_step_pull.hpp,
+  precision_pull.hpp, compressed_pull.hpp).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liblbm_oracle.so"
+REF_SO = HERE / "_ref" / "libcfdref.so"
+REF_FAST_SO = HERE / "_ref" / "libcfdref_fast.so"
+REF_CLI = HERE / "_ref" / "cfd-bench"
+
+STORE = {"f32": 0, "f64": 1, "f16s": 2}
+COLLISION = {"bgk": 0, "trt": 1}
+MAX_WALL_IDS = 16
+
+_f = ctypes.POINTER(ctypes.c_float)
+_d = ctypes.POINTER(ctypes.c_double)
+_u8 = ctypes.POINTER(ctypes.c_uint8)
+
+
+class _OraCfg(ctypes.Structure):
+    _fields_ = [
+        ("q", ctypes.c_int),
+        ("nx", ctypes.c_size_t),
+        ("ny", ctypes.c_size_t),
+        ("nz", ctypes.c_size_t),
+        ("storage", ctypes.c_int),
+        ("collision", ctypes.c_int),
+        ("tau", ctypes.c_double),
+        ("tau_minus", ctypes.c_double),
+        ("trt_magic", ctypes.c_double),
+        ("les_k", ctypes.c_double),
+        ("ax", ctypes.c_double),
+        ("ay", ctypes.c_double),
+        ("az", ctypes.c_double),
+        ("local_a", _f),
+        ("flags", _u8),
+        ("wall_u", _f),
+        ("solid_fraction", _f),
+        ("scale", _f),
+    ]
+
+
+_lib = None
+_ref = {}
+
+
+def oracle_lib():
+    global _lib
+    if _lib is None:
+        if not ORACLE_SO.exists():
+            raise RuntimeError(f"{ORACLE_SO} is not built; run `make -C oracle oracle`")
+        lib = ctypes.CDLL(str(ORACLE_SO))
+        P = ctypes.POINTER(_OraCfg)
+        lib.ora_init.argtypes = [P, ctypes.c_void_p, ctypes.c_int, _f, _f]
+        lib.ora_step.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64]
+        lib.ora_macroscopic.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64] + [ctypes.c_void_p] * 4
+        lib.ora_reduce.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64, _d]
+        lib.ora_logical.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+        lib.ora_f32_to_f16.argtypes = [ctypes.c_float]
+        lib.ora_f32_to_f16.restype = ctypes.c_uint16
+        lib.ora_f16_to_f32.argtypes = [ctypes.c_uint16]
+        lib.ora_f16_to_f32.restype = ctypes.c_float
+        lib.ora_reference_les_k.restype = ctypes.c_float
+        for name in ("ora_init", "ora_step", "ora_macroscopic", "ora_reduce", "ora_logical"):
+            getattr(lib, name).restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def reference_les_k() -> float:
+    """The reference's fixed Smagorinsky coefficient 16*sqrt(2)/(3*pi^2) in float."""
+    return float(oracle_lib().ora_reference_les_k())
+
+
+def _ptr(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+@dataclass
+class OracleLattice:
+    """An oracle lattice with its own population array (numpy, host)."""
+
+    q: int
+    nx: int
+    ny: int
+    nz: int
+    storage: str = "f32"
+    collision: str = "bgk"
+    tau: float = 0.6
+    tau_minus: float = 0.0
+    trt_magic: float = 3.0 / 16.0
+    les_k: float = 0.0
+    accel: tuple = (0.0, 0.0, 0.0)
+    local_a: Optional[np.ndarray] = None
+    flags: Optional[np.ndarray] = None
+    wall_u: Optional[np.ndarray] = None
+    solid_fraction: Optional[np.ndarray] = None
+    scale: Optional[np.ndarray] = None
+    t: int = 0
+    f: np.ndarray = field(init=False)
+
+    def __post_init__(self):
+        n = self.cells
+        dt = {"f32": np.float32, "f64": np.float64, "f16s": np.uint16}[self.storage]
+        self.f = np.zeros(self.q * n, dtype=dt)
+        self._keep = {}
+        self._cfg = _OraCfg()
+        self._refresh()
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    def _arr(self, name, value, dtype):
+        if value is None:
+            self._keep[name] = None
+            return None
+        a = np.ascontiguousarray(value, dtype=dtype)
+        self._keep[name] = a
+        return a
+
+    def _refresh(self):
+        c = self._cfg
+        c.q, c.nx, c.ny, c.nz = self.q, self.nx, self.ny, self.nz
+        c.storage = STORE[self.storage]
+        c.collision = COLLISION[self.collision]
+        c.tau, c.tau_minus, c.trt_magic, c.les_k = self.tau, self.tau_minus, self.trt_magic, self.les_k
+        c.ax, c.ay, c.az = self.accel
+        c.local_a = _ptr(self._arr("local_a", self.local_a, np.float32), _f)
+        c.flags = _ptr(self._arr("flags", self.flags, np.uint8), _u8)
+        wall = self.wall_u
+        if wall is None and self.flags is not None:
+            wall = np.zeros((MAX_WALL_IDS, 3), np.float32)
+        c.wall_u = _ptr(self._arr("wall_u", wall, np.float32), _f)
+        c.solid_fraction = _ptr(self._arr("sf", self.solid_fraction, np.float32), _f)
+        c.scale = _ptr(self._arr("scale", self.scale, np.float32), _f)
+
+    def _call(self, rc):
+        if rc != 0:
+            raise ValueError("oracle rejected the configuration")
+
+    def init_uniform(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0):
+        self._refresh()
+        p = np.array([rho, ux, uy, uz], np.float32)
+        self._call(oracle_lib().ora_init(ctypes.byref(self._cfg), self.f.ctypes.data, 0, _ptr(p, _f), None))
+        self.t = 0
+
+    def init_taylor_green(self, amplitude=0.03):
+        self._refresh()
+        p = np.array([amplitude, 0, 0, 0], np.float32)
+        self._call(oracle_lib().ora_init(ctypes.byref(self._cfg), self.f.ctypes.data, 1, _ptr(p, _f), None))
+        self.t = 0
+
+    def init_fields(self, fields: np.ndarray):
+        self._refresh()
+        fl = np.ascontiguousarray(fields, np.float32).reshape(4 * self.cells)
+        self._call(oracle_lib().ora_init(ctypes.byref(self._cfg), self.f.ctypes.data, 2, None, _ptr(fl, _f)))
+        self.t = 0
+
+    def step(self, count=1):
+        self._refresh()
+        lib = oracle_lib()
+        for _ in range(count):
+            self._call(lib.ora_step(ctypes.byref(self._cfg), self.f.ctypes.data, self.t))
+            self.t += 1
+
+    def macroscopic(self):
+        self._refresh()
+        dt = np.float64 if self.storage == "f64" else np.float32
+        out = [np.zeros(self.cells, dt) for _ in range(4)]
+        self._call(oracle_lib().ora_macroscopic(ctypes.byref(self._cfg), self.f.ctypes.data, self.t,
+                                                *[o.ctypes.data for o in out]))
+        return out
+
+    def reduce(self):
+        self._refresh()
+        out = np.zeros(7, np.float64)
+        self._call(oracle_lib().ora_reduce(ctypes.byref(self._cfg), self.f.ctypes.data, self.t, _ptr(out, _d)))
+        return {"mass": out[0], "momentum": out[1:4].copy(), "kinetic_energy": out[4], "max_speed": out[5],
+                "nonfinite": int(out[6])}
+
+    def logical(self):
+        self._refresh()
+        dt = np.float64 if self.storage == "f64" else np.float32
+        out = np.zeros(self.q * self.cells, dt)
+        self._call(oracle_lib().ora_logical(ctypes.byref(self._cfg), self.f.ctypes.data, self.t, out.ctypes.data))
+        return out
+
+
+def f32_to_f16_bits(v: float) -> int:
+    return int(oracle_lib().ora_f32_to_f16(v))
+
+
+def f16_bits_to_f32(h: int) -> float:
+    return float(oracle_lib().ora_f16_to_f32(h))
+
+
+# ----------------------------------------------------------------- reference
+def reference_available(fast: bool = False) -> bool:
+    return (REF_FAST_SO if fast else REF_SO).exists()
+
+
+def ref_lib(fast: bool = False):
+    key = "fast" if fast else "exact"
+    if key not in _ref:
+        path = REF_FAST_SO if fast else REF_SO
+        if not path.exists():
+            raise RuntimeError(f"{path} is not built; run `make -C oracle ref` where the reference is present")
+        lib = ctypes.CDLL(str(path))
+        sz = ctypes.c_size_t
+        lib.ref_last_error.restype = ctypes.c_char_p
+        lib.ref_thread_capacity.restype = ctypes.c_uint
+        lib.ref_esoteric_run.argtypes = [ctypes.c_int, sz, sz, sz, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                         ctypes.c_float, ctypes.c_int, ctypes.c_int, _f, _u8, _f, sz, _f, _f, _f, _f,
+                                         _f, _d]
+        lib.ref_twogrid_run.argtypes = [ctypes.c_int, sz, sz, sz, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                        ctypes.c_float, ctypes.c_float, ctypes.c_int, _f, sz, _f, _f, _f, _f, _d]
+        lib.ref_precision_run.argtypes = [ctypes.c_int, sz, sz, sz, ctypes.c_double, ctypes.c_int, _d, sz, _d, _d,
+                                          _d, _d, _d]
+        lib.ref_compressed_run.argtypes = [ctypes.c_int, sz, sz, sz, ctypes.c_float, ctypes.c_int, _f, sz, _f, _f,
+                                           _f, _f, _d]
+        lib.ref_bench.argtypes = [ctypes.c_int, sz, sz, sz, ctypes.c_float, ctypes.c_int, _u8, sz, sz, ctypes.c_uint,
+                                  _d, _d]
+        lib.ref_bench.restype = ctypes.c_double
+        _ref[key] = lib
+    return _ref[key]
+
+
+def _init_args(init):
+    kind, *vals = init
+    if kind == "uniform":
+        p = np.array((list(vals) + [1.0, 0.0, 0.0, 0.0])[:4] if vals else [1.0, 0, 0, 0], np.float32)
+        return 0, p
+    p = np.array([vals[0] if vals else 0.03, 0, 0, 0], np.float32)
+    return 1, p
+
+
+def _check(lib, rc):
+    if rc != 0:
+        raise ValueError(lib.ref_last_error().decode())
+
+
+def ref_esoteric(q, nx, ny, nz, tau, steps, init=("tg", 0.03), accel=(0.0, 0.0, 0.0), les=False, mask=None,
+                 local_a=None, logical=False, fast=False):
+    """Run the reference EsotericPullSolver<D> (esoteric_pull.hpp:104-515)."""
+    lib = ref_lib(fast)
+    n = nx * ny * nz
+    kind, p = _init_args(init)
+    rho, ux, uy, uz = (np.zeros(n, np.float32) for _ in range(4))
+    pops = np.zeros(q * n, np.float32) if logical else None
+    out = np.zeros(3, np.float64)
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    la = None if local_a is None else np.ascontiguousarray(local_a, np.float32)
+    _check(lib, lib.ref_esoteric_run(q, nx, ny, nz, tau, *accel, int(les), kind, _ptr(p, _f), _ptr(m, _u8),
+                                     _ptr(la, _f), steps, _ptr(rho, _f), _ptr(ux, _f), _ptr(uy, _f), _ptr(uz, _f),
+                                     _ptr(pops, _f), _ptr(out, _d)))
+    return {"rho": rho, "ux": ux, "uy": uy, "uz": uz, "logical": pops, "mass": out[0], "kinetic_energy": out[1],
+            "max_speed": out[2]}
+
+
+def ref_twogrid(q, nx, ny, nz, tau, odd_tau, steps, init=("tg", 0.03), accel=(0.0, 0.0, 0.0)):
+    """Run the reference two-grid OneStepPullSolver<D>(config, odd_tau) (one_step_pull.hpp:16-215)."""
+    lib = ref_lib()
+    n = nx * ny * nz
+    kind, p = _init_args(init)
+    rho, ux, uy, uz = (np.zeros(n, np.float32) for _ in range(4))
+    mass = np.zeros(1, np.float64)
+    _check(lib, lib.ref_twogrid_run(q, nx, ny, nz, tau, odd_tau, *accel, kind, _ptr(p, _f), steps, _ptr(rho, _f),
+                                    _ptr(ux, _f), _ptr(uy, _f), _ptr(uz, _f), _ptr(mass, _d)))
+    return {"rho": rho, "ux": ux, "uy": uy, "uz": uz, "mass": mass[0]}
+
+
+def ref_precision(q, nx, ny, nz, tau, steps, init=("tg", 0.03)):
+    """Run the reference FP64 two-grid PrecisionPullSolver<D,double> (precision_pull.hpp:49-213)."""
+    lib = ref_lib()
+    n = nx * ny * nz
+    kind, p32 = _init_args(init)
+    p = np.array([init[1] if len(init) > 1 else 0.03, 0, 0, 0], np.float64) if kind == 1 else p32.astype(np.float64)
+    rho, ux, uy, uz = (np.zeros(n, np.float64) for _ in range(4))
+    mass = np.zeros(1, np.float64)
+    _check(lib, lib.ref_precision_run(q, nx, ny, nz, tau, kind, _ptr(p, _d), steps, _ptr(rho, _d), _ptr(ux, _d),
+                                      _ptr(uy, _d), _ptr(uz, _d), _ptr(mass, _d)))
+    return {"rho": rho, "ux": ux, "uy": uy, "uz": uz, "mass": mass[0]}
+
+
+def ref_compressed(q, nx, ny, nz, tau, steps, init=("tg", 0.03)):
+    """Run the reference shifted-FP16 two-grid solver (compressed_pull.hpp:72-147)."""
+    lib = ref_lib()
+    n = nx * ny * nz
+    kind, p = _init_args(init)
+    rho, ux, uy, uz = (np.zeros(n, np.float32) for _ in range(4))
+    mass = np.zeros(1, np.float64)
+    _check(lib, lib.ref_compressed_run(q, nx, ny, nz, tau, kind, _ptr(p, _f), steps, _ptr(rho, _f), _ptr(ux, _f),
+                                       _ptr(uy, _f), _ptr(uz, _f), _ptr(mass, _d)))
+    return {"rho": rho, "ux": ux, "uy": uy, "uz": uz, "mass": mass[0]}
+
+
+def ref_bench(q, nx, ny, nz, tau, warmup, steps, threads=0, les=False, mask=None):
+    """Time the reference in-place CPU step (optimised build).  Returns (MLUPS, seconds, mass_rel)."""
+    lib = ref_lib(fast=True)
+    sec = np.zeros(1, np.float64)
+    rel = np.zeros(1, np.float64)
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    mlups = lib.ref_bench(q, nx, ny, nz, tau, int(les), _ptr(m, _u8), warmup, steps, threads, _ptr(sec, _d),
+                          _ptr(rel, _d))
+    if mlups < 0:
+        raise ValueError(lib.ref_last_error().decode())
+    return mlups, float(sec[0]), float(rel[0])
+
+
+def ref_threads() -> int:
+    return int(ref_lib(fast=True).ref_thread_capacity())
+
+
+def cavity_flags(nx, ny, nz, lid_id=2):
+    """Lid-driven cavity flags: walls on x=0, x=nx-1, y=0, z=0, z=nz-1; moving lid on y=ny-1."""
+    fl = np.zeros((nz, ny, nx), np.uint8)
+    fl[:, :, 0] = 1
+    fl[:, :, nx - 1] = 1
+    fl[:, 0, :] = 1
+    fl[0, :, :] = 1
+    fl[nz - 1, :, :] = 1
+    fl[:, ny - 1, :] = lid_id
+    return fl.reshape(-1)
+
+
+if os.environ.get("CFDX_ORACLE_SELFTEST"):
+    print(reference_les_k())

@@ -1,0 +1,237 @@
+// Driver around the reference's own CPU solvers -- TEST INFRASTRUCTURE ONLY.
+//
+// Compiled by oracle/Makefile directly against the reference's headers and its
+// one instantiation unit (src/lbm/esoteric_pull.cpp) where they lie; no
+// reference source is copied into this repository.  Output goes to
+// oracle/_ref/ only.  It exposes a small C interface so the tests can run the
+// reference on the same seeded inputs as the CUDA path, and so bench.py can
+// time the reference's CPU path on the GPU box's host cores.
+//
+// Reference classes driven here:
+//   cfd::lbm::EsotericPullSolver<D>            include/cfd/solvers/lbm/esoteric_pull.hpp:104-515
+//   cfd::lbm::OneStepPullSolver<D> (TRT)       include/cfd/solvers/lbm/one_step_pull.hpp:16-215
+//   cfd::lbm::PrecisionPullSolver<D,double>    include/cfd/solvers/lbm/precision_pull.hpp:49-213
+//   cfd::lbm::CompressedPopulationPullSolver<D, ShiftedHalfCodec<D>>
+//                                              include/cfd/solvers/lbm/compressed_pull.hpp:95-147
+#include "cfd/core/parallel.hpp"
+#include "cfd/solvers/lbm/compressed_pull.hpp"
+#include "cfd/solvers/lbm/esoteric_pull.hpp"
+#include "cfd/solvers/lbm/one_step_pull.hpp"
+#include "cfd/solvers/lbm/precision_pull.hpp"
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <span>
+
+namespace {
+
+thread_local char g_error[512];
+
+void set_error(const char* text) {
+    std::strncpy(g_error, text, sizeof g_error - 1U);
+    g_error[sizeof g_error - 1U] = '\0';
+}
+
+template <class F> int guarded(F&& body) {
+    try {
+        body();
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return 1;
+    } catch (...) {
+        set_error("unknown exception");
+        return 2;
+    }
+}
+
+template <class Solver> void apply_init(Solver& s, int kind, const float* p) {
+    if (kind == 0)
+        s.initialize_uniform(p[0], p[1], p[2], p[3]);
+    else
+        s.initialize_taylor_green(p[0]);
+}
+
+template <class D>
+void esoteric_run(std::size_t nx, std::size_t ny, std::size_t nz, float tau, float ax, float ay, float az, int les,
+                  int init_kind, const float* init_p, const std::uint8_t* mask, const float* local_a,
+                  std::size_t steps, float* rho, float* ux, float* uy, float* uz, float* logical, double* out) {
+    cfd::lbm::InPlaceLbmConfig cfg{nx, ny, nz, tau, ax, ay, az};
+    cfg.smagorinsky_les = les != 0;
+    cfd::lbm::EsotericPullSolver<D> solver(cfg);
+    const std::size_t n = solver.cells();
+    if (mask) solver.set_solid_mask(std::span<const std::uint8_t>(mask, n));
+    if (local_a)
+        solver.set_local_body_acceleration(std::span<const float>(local_a, n), std::span<const float>(local_a + n, n),
+                                           std::span<const float>(local_a + 2 * n, n));
+    apply_init(solver, init_kind, init_p);
+    solver.step(steps);
+    const auto m = solver.compute_macroscopic();
+    std::memcpy(rho, m.rho.data(), n * sizeof(float));
+    std::memcpy(ux, m.ux.data(), n * sizeof(float));
+    std::memcpy(uy, m.uy.data(), n * sizeof(float));
+    std::memcpy(uz, m.uz.data(), n * sizeof(float));
+    if (logical) {
+        const auto pops = solver.logical_populations();
+        std::memcpy(logical, pops.data(), pops.size() * sizeof(float));
+    }
+    out[0] = solver.mass();
+    out[1] = solver.kinetic_energy();
+    out[2] = static_cast<double>(solver.max_speed());
+}
+
+template <class D>
+void twogrid_run(std::size_t nx, std::size_t ny, std::size_t nz, float tau, float odd_tau, float ax, float ay, float az,
+                 int init_kind, const float* init_p, std::size_t steps, float* rho, float* ux, float* uy, float* uz,
+                 double* mass) {
+    cfd::lbm::InPlaceLbmConfig cfg{nx, ny, nz, tau, ax, ay, az};
+    cfd::lbm::OneStepPullSolver<D> solver(cfg, odd_tau);
+    apply_init(solver, init_kind, init_p);
+    solver.step(steps);
+    const auto m = solver.compute_macroscopic();
+    const std::size_t n = solver.cells();
+    std::memcpy(rho, m.rho.data(), n * sizeof(float));
+    std::memcpy(ux, m.ux.data(), n * sizeof(float));
+    std::memcpy(uy, m.uy.data(), n * sizeof(float));
+    std::memcpy(uz, m.uz.data(), n * sizeof(float));
+    *mass = solver.mass();
+}
+
+template <class D>
+void precision_run(std::size_t nx, std::size_t ny, std::size_t nz, double tau, int init_kind, const double* init_p,
+                   std::size_t steps, double* rho, double* ux, double* uy, double* uz, double* mass) {
+    cfd::lbm::PrecisionPullSolver<D, double> solver(cfd::lbm::TypedLbmConfig<double>{nx, ny, nz, tau});
+    if (init_kind == 0)
+        solver.initialize_uniform(init_p[0], init_p[1], init_p[2], init_p[3]);
+    else
+        solver.initialize_taylor_green(init_p[0]);
+    solver.step(steps);
+    const auto m = solver.compute_macroscopic();
+    const std::size_t n = nx * ny * nz;
+    std::memcpy(rho, m.rho.data(), n * sizeof(double));
+    std::memcpy(ux, m.ux.data(), n * sizeof(double));
+    std::memcpy(uy, m.uy.data(), n * sizeof(double));
+    std::memcpy(uz, m.uz.data(), n * sizeof(double));
+    *mass = static_cast<double>(solver.mass());
+}
+
+template <class D>
+void compressed_run(std::size_t nx, std::size_t ny, std::size_t nz, float tau, int init_kind, const float* init_p,
+                    std::size_t steps, float* rho, float* ux, float* uy, float* uz, double* mass) {
+    using Solver = cfd::lbm::CompressedPopulationPullSolver<D, cfd::lbm::ShiftedHalfCodec<D>>;
+    Solver solver(typename Solver::Config{nx, ny, nz, tau});
+    apply_init(solver, init_kind, init_p);
+    solver.step(steps);
+    const auto m = solver.compute_macroscopic();
+    const std::size_t n = nx * ny * nz;
+    std::memcpy(rho, m.rho.data(), n * sizeof(float));
+    std::memcpy(ux, m.ux.data(), n * sizeof(float));
+    std::memcpy(uy, m.uy.data(), n * sizeof(float));
+    std::memcpy(uz, m.uz.data(), n * sizeof(float));
+    *mass = solver.mass();
+}
+
+// Times solver.step(steps) after solver.step(warmup), the way apps/cfd-bench.cpp:173-191 does.
+template <class D>
+double bench_run(std::size_t nx, std::size_t ny, std::size_t nz, float tau, int les, const std::uint8_t* mask,
+                 std::size_t warmup, std::size_t steps, unsigned threads, double* seconds, double* mass_rel) {
+    if (threads > 0U) cfd::core::set_cpu_threads(threads);
+    cfd::lbm::InPlaceLbmConfig cfg{nx, ny, nz, tau};
+    cfg.smagorinsky_les = les != 0;
+    cfd::lbm::EsotericPullSolver<D> solver(cfg);
+    if (mask) solver.set_solid_mask(std::span<const std::uint8_t>(mask, solver.cells()));
+    solver.initialize_uniform();
+    const double mass0 = solver.mass();
+    solver.step(warmup);
+    const auto begin = std::chrono::steady_clock::now();
+    solver.step(steps);
+    const auto end = std::chrono::steady_clock::now();
+    *seconds = std::chrono::duration<double>(end - begin).count();
+    *mass_rel = std::abs(solver.mass() - mass0) / mass0;
+    return static_cast<double>(solver.cells()) * static_cast<double>(steps) / *seconds / 1.0e6;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_error; }
+
+unsigned ref_thread_capacity(void) { return cfd::core::cpu_thread_capacity(); }
+
+int ref_esoteric_run(int q, std::size_t nx, std::size_t ny, std::size_t nz, float tau, float ax, float ay, float az,
+                     int les, int init_kind, const float* init_p, const std::uint8_t* mask, const float* local_a,
+                     std::size_t steps, float* rho, float* ux, float* uy, float* uz, float* logical, double* out) {
+    return guarded([&] {
+        if (q == 19)
+            esoteric_run<cfd::lbm::D3Q19Descriptor>(nx, ny, nz, tau, ax, ay, az, les, init_kind, init_p, mask,
+                                                    local_a, steps, rho, ux, uy, uz, logical, out);
+        else if (q == 27)
+            esoteric_run<cfd::lbm::D3Q27Descriptor>(nx, ny, nz, tau, ax, ay, az, les, init_kind, init_p, mask,
+                                                    local_a, steps, rho, ux, uy, uz, logical, out);
+        else
+            throw std::invalid_argument("q must be 19 or 27");
+    });
+}
+
+int ref_twogrid_run(int q, std::size_t nx, std::size_t ny, std::size_t nz, float tau, float odd_tau, float ax,
+                    float ay, float az, int init_kind, const float* init_p, std::size_t steps, float* rho, float* ux,
+                    float* uy, float* uz, double* mass) {
+    return guarded([&] {
+        if (q == 19)
+            twogrid_run<cfd::lbm::D3Q19Descriptor>(nx, ny, nz, tau, odd_tau, ax, ay, az, init_kind, init_p, steps, rho,
+                                                   ux, uy, uz, mass);
+        else if (q == 27)
+            twogrid_run<cfd::lbm::D3Q27Descriptor>(nx, ny, nz, tau, odd_tau, ax, ay, az, init_kind, init_p, steps, rho,
+                                                   ux, uy, uz, mass);
+        else
+            throw std::invalid_argument("q must be 19 or 27");
+    });
+}
+
+int ref_precision_run(int q, std::size_t nx, std::size_t ny, std::size_t nz, double tau, int init_kind,
+                      const double* init_p, std::size_t steps, double* rho, double* ux, double* uy, double* uz,
+                      double* mass) {
+    return guarded([&] {
+        if (q == 19)
+            precision_run<cfd::lbm::D3Q19Descriptor>(nx, ny, nz, tau, init_kind, init_p, steps, rho, ux, uy, uz, mass);
+        else if (q == 27)
+            precision_run<cfd::lbm::D3Q27Descriptor>(nx, ny, nz, tau, init_kind, init_p, steps, rho, ux, uy, uz, mass);
+        else
+            throw std::invalid_argument("q must be 19 or 27");
+    });
+}
+
+int ref_compressed_run(int q, std::size_t nx, std::size_t ny, std::size_t nz, float tau, int init_kind,
+                       const float* init_p, std::size_t steps, float* rho, float* ux, float* uy, float* uz,
+                       double* mass) {
+    return guarded([&] {
+        if (q == 19)
+            compressed_run<cfd::lbm::D3Q19Descriptor>(nx, ny, nz, tau, init_kind, init_p, steps, rho, ux, uy, uz, mass);
+        else if (q == 27)
+            compressed_run<cfd::lbm::D3Q27Descriptor>(nx, ny, nz, tau, init_kind, init_p, steps, rho, ux, uy, uz, mass);
+        else
+            throw std::invalid_argument("q must be 19 or 27");
+    });
+}
+
+// Returns MLUPS of the reference in-place CPU path (negative on error).
+double ref_bench(int q, std::size_t nx, std::size_t ny, std::size_t nz, float tau, int les, const std::uint8_t* mask,
+                 std::size_t warmup, std::size_t steps, unsigned threads, double* seconds, double* mass_rel) {
+    double mlups = -1.0;
+    const int rc = guarded([&] {
+        if (q == 19)
+            mlups = bench_run<cfd::lbm::D3Q19Descriptor>(nx, ny, nz, tau, les, mask, warmup, steps, threads, seconds,
+                                                         mass_rel);
+        else if (q == 27)
+            mlups = bench_run<cfd::lbm::D3Q27Descriptor>(nx, ny, nz, tau, les, mask, warmup, steps, threads, seconds,
+                                                         mass_rel);
+        else
+            throw std::invalid_argument("q must be 19 or 27");
+    });
+    return rc == 0 ? mlups : -1.0;
+}
+
+} // extern "C"

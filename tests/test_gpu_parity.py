@@ -1,0 +1,402 @@
+"""Parity of the sm_100a path with the reference and the CPU oracle (GPU).
+
+Every call goes through the C ABI (libcfdx_lbm.so via ctypes).  Gates:
+* FP32 fields vs the reference / oracle: max |d rho|, |d u| < 2e-5, the
+  reference's own CPU/SYCL gate (tests/test_main.cpp:608);
+* FP64 storage vs the FP64 oracle: 1e-12;
+* FP16 shifted storage vs the FP16 oracle (same rounding rule, different
+  FMA contraction): 5e-5; vs the FP64 oracle: the reference's shifted-FP16
+  gates (tests/test_v0141_lbm_les_qcriterion.cpp:175-176).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FP32_GATE = 2e-5
+
+
+def maxabs(a, b):
+    return float(np.max(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64))))
+
+
+def fields_err(a, b):
+    return max(maxabs(x, y) for x, y in zip(a, b))
+
+
+def make(cs, q, nx, ny, nz, **kw):
+    lattice = {19: "d3q19", 27: "d3q27"}[q]
+    return cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(nx=nx, ny=ny, nz=nz, lattice=lattice, **kw))
+
+
+# ------------------------------------------------------------ vs reference
+@pytest.mark.parametrize("q", [19, 27])
+def test_reference_sycl_parity_template(engine, golden, q):
+    """tests/test_main.cpp:587-615: 16x14x12, tau 0.72, forced, A = 0.018, 12 steps."""
+    data, meta = golden
+    with make(engine, q, 16, 14, 12, tau=0.72, acceleration_x=1e-6, acceleration_y=-0.5e-6,
+              acceleration_z=0.25e-6) as s:
+        s.initialize_taylor_green(0.018)
+        s.step(12)
+        got = s.compute_macroscopic()
+        ref = [data[f"sycl_parity_q{q}_{k}"] for k in ("rho", "ux", "uy", "uz")]
+        assert fields_err(got, ref) < FP32_GATE
+        assert maxabs(s.logical_populations(), data[f"sycl_parity_q{q}_logical"]) < FP32_GATE
+        red = s.reduce()
+        m = meta[f"sycl_parity_q{q}"]
+        assert red["mass"] == pytest.approx(m["mass"], rel=1e-6)
+        assert red["kinetic_energy"] == pytest.approx(m["kinetic_energy"], rel=1e-4)
+        assert red["max_speed"] == pytest.approx(m["max_speed"], rel=1e-4)
+
+
+def test_reference_smagorinsky(engine, golden):
+    data, meta = golden
+    with make(engine, 19, 20, 18, 16, tau=0.56, smagorinsky_les=True) as s:
+        s.initialize_taylor_green(0.05)
+        s.step(24)
+        assert maxabs(s.logical_populations(), data["les_q19_logical"]) < FP32_GATE
+        assert s.kinetic_energy() == pytest.approx(meta["les_q19"]["kinetic_energy"], rel=1e-4)
+
+
+def test_reference_plain_method_64cubed(engine, golden):
+    """Plain-method config (64^3 D3Q19 BGK, tau 0.6, A = 0.05, 10 + 100 steps)."""
+    data, meta = golden
+    m = meta["c1_d3q19_tg64"]
+    with make(engine, 19, 64, 64, 64, tau=0.6) as s:
+        s.initialize_taylor_green(0.05)
+        s.step(10)
+        s.step(100)
+        got = [a[:: m["stride"]] for a in s.compute_macroscopic()]
+        ref = [data[f"c1_d3q19_tg64_{k}"] for k in ("rho", "ux", "uy", "uz")]
+        assert fields_err(got, ref) < FP32_GATE
+        assert s.checksum() == pytest.approx(m["checksum"], rel=1e-7)
+
+
+def test_reference_phase02_checksum(engine, golden):
+    """Known answer: examples/phase02_lbm_taylor_green.cpp checksum 110609.77375653926."""
+    _, meta = golden
+    p = meta["phase02"]
+    with make(engine, 19, 48, 48, 48, tau=0.58, smagorinsky_les=True) as s:
+        s.initialize_taylor_green(0.04)
+        s.step(80)
+        assert s.checksum() == pytest.approx(p["checksum"], rel=1e-7)
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("steps", [7, 8])
+def test_reference_trt_two_grid(engine, golden, q, steps):
+    data, _ = golden
+    with make(engine, q, 18, 14, 10, tau=0.73, collision="trt", trt_tau_minus=1.1, acceleration_x=2e-6,
+              acceleration_y=-1e-6, acceleration_z=0.5e-6) as s:
+        s.initialize_taylor_green(0.017)
+        s.step(steps)
+        ref = [data[f"trt_q{q}_s{steps}_{k}"] for k in ("rho", "ux", "uy", "uz")]
+        assert fields_err(s.compute_macroscopic(), ref) < FP32_GATE
+
+
+# --------------------------------------------------------------- vs oracle
+CASES = [
+    # id, q, config kwargs, oracle kwargs, flags kind, gray, local force
+    ("bgk", {}, {}, None, False, False),
+    ("bgk_force", dict(acceleration_x=2e-5, acceleration_y=-1e-5, acceleration_z=5e-6), {}, None, False, False),
+    ("les_cs01", dict(smagorinsky_les=True, smagorinsky_cs=0.1), {}, None, False, False),
+    ("trt_magic", dict(collision="trt"), {}, None, False, False),
+    ("trt_les", dict(collision="trt", smagorinsky_les=True, smagorinsky_cs=0.1), {}, None, False, False),
+    ("walls", dict(acceleration_x=2e-5), {}, "random", False, False),
+    ("cavity_trt_les", dict(collision="trt", smagorinsky_les=True, smagorinsky_cs=0.1), {}, "cavity", False, False),
+    ("gray", dict(acceleration_x=1e-5, collision="trt"), {}, None, True, False),
+    ("gray_walls", dict(acceleration_x=1e-5), {}, "random", True, False),
+    ("local_force", dict(acceleration_x=1e-6), {}, None, False, True),
+]
+
+
+def oracle_config(O, q, nx, ny, nz, kw):
+    les_k = 0.0
+    if kw.get("smagorinsky_les"):
+        cs = kw.get("smagorinsky_cs", 0.0)
+        les_k = 18 * np.sqrt(2) * cs * cs if cs > 0 else O.reference_les_k()
+    return dict(q=q, nx=nx, ny=ny, nz=nz, collision=kw.get("collision", "bgk"), tau=kw.get("tau", 0.6),
+                tau_minus=kw.get("trt_tau_minus", 0.0), trt_magic=kw.get("trt_magic", 3 / 16), les_k=les_k,
+                accel=(kw.get("acceleration_x", 0.0), kw.get("acceleration_y", 0.0), kw.get("acceleration_z", 0.0)))
+
+
+def case_inputs(kind, gray, local, nx, ny, nz, seed=7):
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    flags = None
+    wall_u = None
+    if kind == "random":
+        flags = (rng.random(n) < 0.12).astype(np.uint8)
+    elif kind == "cavity":
+        from cfd_solvers_b200 import cavity_flags
+
+        flags = cavity_flags(nx, ny, nz)
+        wall_u = np.zeros((16, 3), np.float32)
+        wall_u[2] = (0.1, 0.0, 0.0)
+    ns = rng.uniform(0.0, 0.2, n).astype(np.float32) if gray else None
+    la = (rng.normal(0, 1e-6, 3 * n)).astype(np.float32) if local else None
+    return flags, wall_u, ns, la
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_oracle_feature_matrix(engine, oracle_mod, q, case):
+    name, kw, _, kind, gray, local = case
+    nx, ny, nz = 17, 15, 13
+    kw = dict(tau=0.62, **kw)
+    flags, wall_u, ns, la = case_inputs(kind, gray, local, nx, ny, nz)
+    L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, q, nx, ny, nz, kw), flags=flags, wall_u=wall_u,
+                                 solid_fraction=ns, local_a=la)
+    with make(engine, q, nx, ny, nz, **kw) as s:
+        if flags is not None:
+            s.set_flags(flags)
+            if wall_u is not None:
+                s.set_wall_velocity(2, *wall_u[2])
+        if ns is not None:
+            s.set_solid_fraction(ns)
+        if la is not None:
+            s.set_local_body_acceleration(la[: nx * ny * nz], la[nx * ny * nz: 2 * nx * ny * nz],
+                                          la[2 * nx * ny * nz:])
+        if kind == "cavity":
+            s.initialize_uniform()
+            L.init_uniform()
+        else:
+            s.initialize_taylor_green(0.04)
+            L.init_taylor_green(0.04)
+        for steps in (7, 1):  # odd then even total step count
+            s.step(steps)
+            L.step(steps)
+            assert fields_err(s.compute_macroscopic(), L.macroscopic()) < FP32_GATE, (name, L.t)
+            assert maxabs(s.logical_populations(), L.logical()) < FP32_GATE, (name, L.t)
+        got, ref = s.reduce(), L.reduce()
+        assert got["mass"] == pytest.approx(ref["mass"], rel=1e-6)
+        assert got["kinetic_energy"] == pytest.approx(ref["kinetic_energy"], rel=1e-3, abs=1e-9)
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_fp64_storage_matches_fp64_oracle(engine, oracle_mod, q):
+    nx, ny, nz = 17, 15, 13
+    kw = dict(tau=0.62, storage="fp64", collision="trt", smagorinsky_les=True, smagorinsky_cs=0.1,
+              acceleration_x=1e-5)
+    flags = (np.random.default_rng(3).random(nx * ny * nz) < 0.1).astype(np.uint8)
+    L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, q, nx, ny, nz, kw), storage="f64", flags=flags)
+    with make(engine, q, nx, ny, nz, **kw) as s:
+        s.set_flags(flags)
+        s.initialize_taylor_green(0.04)
+        L.init_taylor_green(0.04)
+        s.step(9)
+        L.step(9)
+        assert fields_err(s.compute_macroscopic(), L.macroscopic()) < 1e-12
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_fp16_storage_matches_fp16_oracle(engine, oracle_mod, q):
+    nx, ny, nz = 17, 15, 13
+    kw = dict(tau=0.62, storage="fp16s", collision="trt", acceleration_x=1e-5)
+    flags = (np.random.default_rng(4).random(nx * ny * nz) < 0.1).astype(np.uint8)
+    scale = np.array([2.0 ** round(np.log2(1 / w)) for w in oracle_weights(q)], np.float32)
+    L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, q, nx, ny, nz, kw), storage="f16s", flags=flags,
+                                 scale=scale)
+    with make(engine, q, nx, ny, nz, **kw) as s:
+        s.set_flags(flags)
+        s.initialize_taylor_green(0.04)
+        L.init_taylor_green(0.04)
+        s.step(9)
+        L.step(9)
+        assert fields_err(s.compute_macroscopic(), L.macroscopic()) < 5e-5
+
+
+def oracle_weights(q):
+    cx = [0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1]
+    cy = [0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1]
+    cz = [0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1]
+    out = []
+    for d in range(q):
+        l2 = cx[d] ** 2 + cy[d] ** 2 + cz[d] ** 2
+        if q == 19:
+            out.append([1 / 3, 1 / 18, 1 / 36][l2])
+        else:
+            out.append([8 / 27, 2 / 27, 1 / 54, 1 / 216][l2])
+    return out
+
+
+def test_fp16_against_fp64_reference_gates(engine):
+    """Shifted FP16 storage vs FP64 storage on the same run: the reference's FP16 gates."""
+    kw = dict(nx=28, ny=24, nz=16, tau=0.72)
+    with make(engine, 19, storage="fp16s", **kw) as h, make(engine, 19, storage="fp64", **kw) as d:
+        for s in (h, d):
+            s.initialize_taylor_green(0.025)
+            s.step(16)
+        m0 = 28 * 24 * 16
+        assert abs(h.mass() - d.mass()) / m0 < 2e-4
+        assert fields_err(h.compute_macroscopic(), d.compute_macroscopic()) < 4e-4
+
+
+# ------------------------------------------------------- physics / properties
+def test_poiseuille_profile(engine):
+    q, nx, ny, nz, tau, g = 19, 4, 14, 4, 0.8, 1e-5
+    mask = np.zeros((nz, ny, nx), np.uint8)
+    mask[:, 0, :] = 1
+    mask[:, ny - 1, :] = 1
+    with make(engine, q, nx, ny, nz, tau=tau, acceleration_x=g) as s:
+        s.set_solid_mask(mask.reshape(-1))
+        s.initialize_uniform()
+        s.step(5000)
+        ux = s.compute_macroscopic().ux.reshape(nz, ny, nx)
+    nu = (tau - 0.5) / 3
+    h = ny - 2
+    num = den = 0.0
+    for y in range(1, ny - 1):
+        wy = y - 0.5
+        exact = g * wy * (h - wy) / (2 * nu)
+        num += (ux[:, y, :].mean() - exact) ** 2
+        den += exact ** 2
+    assert np.sqrt(num / den) < 0.01
+
+
+def test_lid_driven_cavity_quasi_2d(engine):
+    """Gates of the reference's D2Q9 cavity (tests/test_main.cpp:479-499) on a periodic-z D3Q19 slab."""
+    n = 48
+    fl = np.zeros((2, n, n), np.uint8)
+    fl[:, :, 0] = 1
+    fl[:, :, n - 1] = 1
+    fl[:, 0, :] = 1
+    fl[:, n - 1, :] = 2
+    with make(engine, 19, n, n, 2, tau=0.8) as s:
+        s.set_flags(fl.reshape(-1))
+        s.set_wall_velocity(2, 0.05, 0.0, 0.0)
+        s.initialize_uniform()
+        s.step(6000)
+        ux = s.compute_macroscopic().ux.reshape(2, n, n)
+        assert ux[0, n - 2, n // 2] > 0.03
+        assert ux[0, n // 2, n // 2] < -0.003
+        assert s.max_speed() < 0.08
+
+
+def test_uniform_flow_invariance_and_mass_512(engine):
+    """Full-size (512^3 D3Q19 FP32) size-independent properties: uniform flow stays uniform, mass is conserved."""
+    with make(engine, 19, 512, 512, 512, tau=0.72) as s:
+        s.initialize_uniform(1.0, 0.015, -0.01, 0.005)
+        m0 = s.mass()
+        s.step(21)
+        red = s.reduce()
+        assert abs(red["mass"] - m0) / m0 < 1e-6
+        f = s.compute_macroscopic()
+        assert np.abs(f.rho - 1.0).max() < 2e-5
+        assert np.abs(f.ux - 0.015).max() < 2e-5
+        assert np.abs(f.uy + 0.01).max() < 2e-5
+        assert np.abs(f.uz - 0.005).max() < 2e-5
+        n = 512 ** 3
+        assert red["momentum"][0] / n == pytest.approx(0.015, rel=1e-4)
+
+
+def test_cavity_512_conservation_and_determinism(engine):
+    """512^3 TRT+LES cavity: stationary and tangential walls conserve mass; runs are bitwise reproducible."""
+    from cfd_solvers_b200 import cavity_flags
+
+    n = 512
+    fl = cavity_flags(n, n, n)
+    out = []
+    for _ in range(2):
+        with make(engine, 19, n, n, n, tau=0.51, collision="trt", smagorinsky_les=True, smagorinsky_cs=0.1) as s:
+            s.set_flags(fl)
+            s.set_wall_velocity(2, 0.1, 0.0, 0.0)
+            s.initialize_uniform()
+            m0 = s.mass()
+            s.step(30)
+            red = s.reduce()
+            assert red["nonfinite"] == 0
+            assert abs(red["mass"] - m0) / m0 < 1e-6
+            out.append((red["mass"], red["kinetic_energy"], red["max_speed"]))
+    assert out[0] == out[1]
+
+
+def test_reduction_consistent_with_fields(engine):
+    with make(engine, 27, 40, 36, 30, tau=0.7, acceleration_x=1e-5) as s:
+        s.initialize_taylor_green(0.03)
+        s.step(5)
+        f = s.compute_macroscopic()
+        red = s.reduce()
+        rho = f.rho.astype(np.float64)
+        assert red["mass"] == pytest.approx(rho.sum(), rel=1e-6)
+        ke = 0.5 * (rho * (f.ux.astype(np.float64) ** 2 + f.uy.astype(np.float64) ** 2 +
+                           f.uz.astype(np.float64) ** 2)).sum()
+        assert red["kinetic_energy"] == pytest.approx(ke, rel=1e-6)
+
+
+# ------------------------------------------------------------ API behaviour
+def test_gpu_residency_no_host_traffic_during_steps(engine):
+    """tests/test_v0155_gpu_residency.cpp:89-111: stepping moves no host bytes; download = 4 N floats."""
+    with make(engine, 19, 12, 10, 8, tau=0.7) as s:
+        s.initialize_taylor_green(0.02)
+        before = s.transfer_stats()
+        s.step(25)
+        s.wait()
+        mid = s.transfer_stats()
+        assert mid.host_transfer_bytes() == before.host_transfer_bytes()
+        s.download_macroscopic()
+        after = s.transfer_stats()
+        assert after.device_to_host_bytes - mid.device_to_host_bytes == 4 * 12 * 10 * 8 * 4
+        assert s.time_step() == 25
+        assert s.population_bytes() * 2 == s.two_lattice_population_bytes()
+        assert s.population_bytes() == 19 * 12 * 10 * 8 * 4
+
+
+def test_nonfinite_detection(engine):
+    import cfd_solvers_b200 as cs
+
+    n = 10 * 9 * 8
+    with make(engine, 19, 10, 9, 8, tau=0.7) as s:
+        rho = np.ones(n, np.float32)
+        rho[17] = np.nan
+        z = np.zeros(n, np.float32)
+        s.initialize_fields(rho, z, z, z)
+        with pytest.raises(cs.NonFiniteError, match="non-finite"):
+            s.reduce()
+        s.initialize_uniform()
+        assert s.reduce()["nonfinite"] == 0
+
+
+def test_allocation_failure_is_reported_and_recoverable(engine):
+    lib = engine.load()
+    lib.raw.cfdx_debug_fail_allocations(1)
+    try:
+        with pytest.raises(MemoryError, match="injected"):
+            make(engine, 19, 8, 8, 8)
+    finally:
+        lib.raw.cfdx_debug_fail_allocations(0)
+    with make(engine, 19, 8, 8, 8) as s:
+        s.step(2)
+        assert s.mass() == pytest.approx(512.0, rel=1e-6)
+
+
+def test_argument_errors(engine):
+    with make(engine, 19, 8, 8, 8) as s:
+        with pytest.raises(IndexError):
+            s.set_wall_velocity(1, 0.1, 0, 0)
+        with pytest.raises(ValueError, match="size mismatch"):
+            s.set_solid_mask(np.zeros(7, np.uint8))
+        with pytest.raises(ValueError, match="finite with positive density"):
+            s.initialize_uniform(-1.0)
+        with pytest.raises(ValueError, match="CFDX_STORE_F16S"):
+            s.set_storage_scale(np.ones(19, np.float32))
+
+
+def test_device_buffers_accept_torch_tensors(engine):
+    import torch
+
+    n = 12 * 10 * 8
+    with make(engine, 19, 12, 10, 8, tau=0.7) as s:
+        mask = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        mask[:96] = 1
+        s.set_flags(mask)
+        s.initialize_uniform()
+        s.step(3)
+        view = s.refresh_device_macroscopic()
+        s.wait()
+        assert view.cells == n
+        acc = s.device_local_acceleration(clear=True)
+        assert acc.cells == n
+        assert s.has_local_body_acceleration()
