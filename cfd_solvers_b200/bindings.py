@@ -129,7 +129,7 @@ SIGNATURES = {
     "cfdx_lbm_get_info": (_i, [_H, ctypes.POINTER(cfdx_lbm_info)]),
     "cfdx_lbm_stream": (_i, [_H, ctypes.POINTER(_vp)]),
     "cfdx_lbm_raw_populations": (_i, [_H, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
-    "cfdx_lbm_set_launch_shape": (_i, [_H, _i, _i]),
+    "cfdx_lbm_set_launch_shape": (_i, [_H, _i, _i, _i]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

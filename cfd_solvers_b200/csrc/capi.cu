@@ -139,17 +139,29 @@ struct cfdx_lbm {
 
     LbmArgs args() const {
         LbmArgs a{};
-        a.f = f;
+        char* base = static_cast<char*>(f);
+        const std::size_t es = static_cast<std::size_t>(storage_bytes(key.storage));
+        for (int d = 0; d < 27; ++d) a.fd[d] = d < key.q ? base + static_cast<std::size_t>(d) * N * es : nullptr;
+        a.rest = a.fd[0];
+        set_parity(a, static_cast<int>(t & 1U));
         a.flags = key.flags ? flags : nullptr;
-        a.local_a = local_a;
-        a.ns = ns;
-        a.nx = static_cast<long long>(cfg.nx);
-        a.ny = static_cast<long long>(cfg.ny);
-        a.nz = static_cast<long long>(cfg.nz);
-        a.N = N;
-        a.odd = static_cast<int>(t & 1U);
+        a.ax_field = local_a;
+        a.ay_field = local_a ? local_a + N : nullptr;
+        a.az_field = local_a ? local_a + 2 * N : nullptr;
+        a.ns = key.gray ? ns : nullptr;
+        a.nx = static_cast<std::uint32_t>(cfg.nx);
+        a.ny = static_cast<std::uint32_t>(cfg.ny);
+        a.nz = static_cast<std::uint32_t>(cfg.nz);
+        a.N = static_cast<std::uint32_t>(N);
+        a.has_force = (cfg.acceleration_x != 0.0F || cfg.acceleration_y != 0.0F || cfg.acceleration_z != 0.0F ||
+                       local_a != nullptr)
+                          ? 1
+                          : 0;
         a.tau = cfg.tau;
-        a.omega_minus = cfg.trt_tau_minus > 0.0F ? 1.0 / static_cast<double>(cfg.trt_tau_minus) : 0.0;
+        // > 0: fixed TRT antisymmetric rate; 0: from the magic parameter; < 0: BGK
+        a.omega_minus = key.collision == kBGK
+                            ? -1.0
+                            : (cfg.trt_tau_minus > 0.0F ? 1.0 / static_cast<double>(cfg.trt_tau_minus) : 0.0);
         a.trt_magic = cfg.trt_magic;
         a.les_k = les_k;
         a.ax = cfg.acceleration_x;
@@ -161,6 +173,20 @@ struct cfdx_lbm {
             a.inv_scale[d] = 1.0F / a.scale[d];
         }
         return a;
+    }
+    // Slot tables of the given parity: pa[p] is read at the neighbour
+    // n + c_{2p+2}, pb[p] at the cell itself (see LbmArgs).
+    void set_parity(LbmArgs& a, int odd) const {
+        a.odd = odd;
+        for (int p = 0; p < 13; ++p) {
+            const int i = 2 * p + 1, j = i + 1;
+            if (j < key.q) {
+                a.pa[p] = a.fd[odd ? j : i];
+                a.pb[p] = a.fd[odd ? i : j];
+            } else {
+                a.pa[p] = a.pb[p] = nullptr;
+            }
+        }
     }
     dim3 block() const { return cell_block(static_cast<long long>(cfg.nx), static_cast<long long>(cfg.ny), shape); }
     dim3 grid() const {
@@ -376,7 +402,8 @@ CFDX_API int cfdx_lbm_create(const cfdx_lbm_config* config, cfdx_lbm** out, char
         h->cfg = c;
         h->set_device();
         h->N = c.nx * c.ny * c.nz;
-        h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false};
+        require(h->N <= 0xffffffffULL, "lattice exceeds 2^32 - 1 cells");
+        h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false, 0};
         h->les_k = c.smagorinsky_les ? (c.smagorinsky_cs > 0.0F
                                             ? 18.0 * std::sqrt(2.0) * double(c.smagorinsky_cs) * double(c.smagorinsky_cs)
                                             : double(reference_les_k()))
@@ -548,7 +575,7 @@ CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
         const dim3 g = h->grid(), b = h->block();
         LbmArgs a = h->args();
         for (std::uint64_t i = 0; i < count; ++i) {
-            a.odd = static_cast<int>(h->t & 1U);
+            h->set_parity(a, static_cast<int>(h->t & 1U));
             check_cuda(launch_step(h->key, a, g, b, h->stream), "step kernel");
             ++h->t;
         }
@@ -735,15 +762,18 @@ CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* h, void** ptr, std::size_t* byte
     });
 }
 
-CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by) {
+CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int cells_per_thread) {
     return guarded([&] {
         require(h != nullptr, "null handle");
+        require(cells_per_thread == 0 || cells_per_thread == 1 || cells_per_thread == 2,
+                "cells per thread must be 0 (default), 1 or 2");
+        h->key.cells_per_thread = cells_per_thread;
         if (bx == 0 && by == 0) {
             h->shape = LaunchShape{};
             return;
         }
-        require(bx > 0 && by > 0 && bx * by <= 256 && (bx * by) % 32 == 0,
-                "block shape must have bx*by a multiple of 32 and at most 256");
+        require(bx > 0 && by > 0 && bx * by <= 128 && (bx * by) % 32 == 0,
+                "block shape must have bx*by a multiple of 32 and at most 128");
         h->shape = LaunchShape{bx, by};
     });
 }

@@ -22,16 +22,32 @@ constexpr std::uint8_t kFlagNearWall = 0x80;
 enum Storage : int { kStoreF32 = 0, kStoreF64 = 1, kStoreF16S = 2 };
 enum Collision : int { kBGK = 0, kTRT = 1 };
 
+// Cell indices are 32-bit: n = (z*ny + y)*nx + x < 2^32 for every lattice
+// that fits in HBM.  Population slots are addressed through per-parity base
+// pointers held in the parameter bank, so the kernels carry no [q][N]
+// offsets and no parity selects in registers:
+//   rest     base of direction 0
+//   pa[p]    base of the slot pair p reads at the neighbour nb = n + c_{2p+2}
+//            (direction 2p+1 at even parity, 2p+2 at odd parity)
+//   pb[p]    base of the slot pair p reads at the cell itself
+//            (direction 2p+2 at even parity, 2p+1 at odd parity)
+//   fd[d]    base of direction d (parity-free layouts: logical dumps, init)
 struct LbmArgs {
-    void* f;                   // populations, [q][N] structure of arrays
+    void* rest;
+    void* pa[13];
+    void* pb[13];
+    void* fd[27];
     const std::uint8_t* flags; // internal flags or nullptr
-    const float* local_a;      // 3*N per-cell acceleration (ax|ay|az) or nullptr
+    const float* ax_field;     // per-cell acceleration components or nullptr
+    const float* ay_field;
+    const float* az_field;
     const float* ns;           // N gray-LBM solid fractions or nullptr
-    long long nx, ny, nz;
-    std::size_t N;
+    std::uint32_t nx, ny, nz;
+    std::uint32_t N;
     int odd;                   // parity of the time step being executed / read
+    int has_force;             // uniform or per-cell acceleration present
     double tau;                // base symmetric relaxation time
-    double omega_minus;        // TRT antisymmetric rate when fixed (> 0), else from magic
+    double omega_minus;        // antisymmetric rate when fixed (> 0), else from magic / = omega+
     double trt_magic;
     double les_k;              // Smagorinsky K (0 = off)
     double ax, ay, az;         // uniform acceleration

@@ -1,27 +1,36 @@
 // Device side of the in-place Esoteric-Pull lattice-Boltzmann step (sm_100a).
 //
-// One thread owns one cell.  Every launch reads and writes each population
-// slot exactly once: a cell reads the q slots its pairs own at this parity and
-// writes the post-collision values back into the same q slots, so the update
-// is race-free with a single lattice in HBM (access pattern: Lehmann,
-// Computation 10(6) 92, 2022; reference esoteric_pull.hpp:349-382).
+// One thread owns CPT cells stacked in z.  Every launch reads and writes each
+// population slot exactly once: a cell reads the q slots its pairs own at this
+// parity and writes the post-collision values back into the same q slots, so
+// the update is race-free with a single lattice in HBM (access pattern:
+// Lehmann, Computation 10(6) 92, 2022; reference esoteric_pull.hpp:349-382).
 //
-// Layout in HBM: populations are a structure of arrays f[d*N + n] with
+// Layout in HBM: populations are a structure of arrays f[d][n] with
 // n = (z*ny + y)*nx + x (reference esoteric_pull.hpp:304-310), so a warp
 // reads 32 consecutive x cells of one direction: c_x = 0 directions are
-// aligned 128-byte (FP32) rows, c_x = +-1 directions are shifted by one
-// element and share their edge sector with the neighbouring warp, which L1/L2
-// absorb.
+// aligned rows, c_x = +-1 directions are shifted by one element and share
+// their edge sector with the neighbouring warp, which L1/L2 absorb.
+//
+// The step is HBM-bound (no tensor-core work: it is a stencil, not a
+// contraction).  What limits it is bytes in flight per SM and instruction
+// issue: all loads of a thread's CPT cells are issued before the first
+// collision; addressing is 32-bit off per-parity slot tables held in the
+// parameter bank (no parity selects, no 64-bit offsets in registers); the
+// collision works on opposite-pair sums and differences.
 #pragma once
 
 #include <cuda_fp16.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "lattice.cuh"
 #include "lbm_args.h"
 
 namespace cfdx {
+
+using u32 = std::uint32_t;
 
 // ------------------------------------------------------------- storage traits
 struct StF32 {
@@ -59,29 +68,29 @@ __device__ __forceinline__ void st(typename S::T* p, typename S::R v, const LbmA
 }
 
 // ------------------------------------------------------- periodic neighbours
-// Offsets of the x-1/x/x+1, y-1/y/y+1, z-1/z/z+1 neighbours, periodic wrap
-// (reference esoteric_pull.hpp:40-46).  Indexed by c + 1.
+// Offsets of the x-1/x/x+1, y-1/y/y+1, z-1/z/z+1 neighbours with periodic wrap
+// (reference esoteric_pull.hpp:40-46), indexed by c + 1.  Unsigned wrap-around
+// arithmetic keeps n + offset exact because the true neighbour index is in [0, N).
 struct Nbr {
-    long long ox[3], oy[3], oz[3];
+    u32 ox[3], oy[3], oz[3];
 };
 
-__device__ __forceinline__ Nbr make_nbr(const LbmArgs& a, long long x, long long y, long long z) {
+__device__ __forceinline__ Nbr make_nbr(const LbmArgs& a, u32 x, u32 y, u32 z) {
     Nbr o;
-    const long long plane = a.nx * a.ny;
-    o.ox[0] = x == 0 ? a.nx - 1 : -1;
-    o.ox[1] = 0;
-    o.ox[2] = x == a.nx - 1 ? -(a.nx - 1) : 1;
-    o.oy[0] = (y == 0 ? a.ny - 1 : -1) * a.nx;
-    o.oy[1] = 0;
-    o.oy[2] = (y == a.ny - 1 ? -(a.ny - 1) : 1) * a.nx;
-    o.oz[0] = (z == 0 ? a.nz - 1 : -1) * plane;
-    o.oz[1] = 0;
-    o.oz[2] = (z == a.nz - 1 ? -(a.nz - 1) : 1) * plane;
+    const u32 plane = a.nx * a.ny;
+    o.ox[0] = x == 0 ? a.nx - 1U : 0xffffffffU;
+    o.ox[1] = 0U;
+    o.ox[2] = x == a.nx - 1U ? 1U - a.nx : 1U;
+    o.oy[0] = y == 0 ? (a.ny - 1U) * a.nx : 0U - a.nx;
+    o.oy[1] = 0U;
+    o.oy[2] = y == a.ny - 1U ? 0U - (a.ny - 1U) * a.nx : a.nx;
+    o.oz[0] = z == 0 ? (a.nz - 1U) * plane : 0U - plane;
+    o.oz[1] = 0U;
+    o.oz[2] = z == a.nz - 1U ? 0U - (a.nz - 1U) * plane : plane;
     return o;
 }
 
-template <class L, int D>
-__device__ __forceinline__ long long nbr_off(const Nbr& o) {
+template <class L, int D> __device__ __forceinline__ u32 nbr_off(const Nbr& o) {
     return o.ox[L::cx(D) + 1] + o.oy[L::cy(D) + 1] + o.oz[L::cz(D) + 1];
 }
 
@@ -91,31 +100,43 @@ __device__ __forceinline__ long long nbr_off(const Nbr& o) {
 // nf = n + c_i the source of direction j.
 //   even step: fin_i = f[i][nb], fin_j = f[j][n]
 //   odd step:  fin_i = f[j][nb], fin_j = f[i][n]
+// i.e. fin_i = pa[p][nb], fin_j = pb[p][n] with the per-parity tables.
 // Half-way bounce-back in place: when the source is a wall, the incoming
 // value is this cell's own outgoing opposite population of the previous
-// step, which sits in the other slot of the same address -- the load swaps
-// the direction index.  Moving walls add 6 w_k rho (c_k . u_wall)
-// (reference src/lbm/d2q9.cpp:220-223) with rho this cell's pre-correction
-// density.
-template <class L, class S, bool FLAGS, int P = 0>
-__device__ __forceinline__ void gather_pairs(const LbmArgs& a, const typename S::T* __restrict__ f, long long n,
-                                             const Nbr& o, unsigned walls, bool odd, typename S::R* fin) {
+// step, which sits in the other slot of the same address -- the load takes
+// the other table.  Moving walls add 6 w_k rho (c_k . u_wall) (reference
+// src/lbm/d2q9.cpp:220-223) with rho this cell's pre-correction density.
+template <class S> __device__ __forceinline__ const typename S::T* slot(void* const* table, int p) {
+    return static_cast<const typename S::T*>(table[p]);
+}
+template <class S> __device__ __forceinline__ typename S::T* slot_mut(void* const* table, int p) {
+    return static_cast<typename S::T*>(table[p]);
+}
+
+template <class L, class S, int P = 0>
+__device__ __forceinline__ void gather_plain(const LbmArgs& a, u32 n, const Nbr& o, typename S::R* fin) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
-        const long long nb = n + nbr_off<L, j>(o);
-        const bool sb = FLAGS ? ((walls >> (2 * P)) & 1U) != 0U : false;
-        const bool sf = FLAGS ? ((walls >> (2 * P + 1)) & 1U) != 0U : false;
-        const std::size_t N = a.N;
-        const typename S::T* pb = f + ((odd != sb) ? j : i) * N + nb;
-        const typename S::T* pn = f + ((odd != sf) ? i : j) * N + n;
-        fin[i] = ld<S, L, i>(pb, a);
-        fin[j] = ld<S, L, j>(pn, a);
-        gather_pairs<L, S, FLAGS, P + 1>(a, f, n, o, walls, odd, fin);
+        fin[i] = ld<S, L, i>(slot<S>(a.pa, P) + (n + nbr_off<L, j>(o)), a);
+        fin[j] = ld<S, L, j>(slot<S>(a.pb, P) + n, a);
+        gather_plain<L, S, P + 1>(a, n, o, fin);
     }
 }
 
-template <class L, int P = 0>
-__device__ __forceinline__ unsigned wall_links(const LbmArgs& a, long long n, const Nbr& o) {
+template <class L, class S, int P = 0>
+__device__ __forceinline__ void gather_walls(const LbmArgs& a, u32 n, const Nbr& o, unsigned walls,
+                                             typename S::R* fin) {
+    if constexpr (P < L::PAIRS) {
+        constexpr int i = 2 * P + 1, j = i + 1;
+        const bool sb = ((walls >> (2 * P)) & 1U) != 0U;
+        const bool sf = ((walls >> (2 * P + 1)) & 1U) != 0U;
+        fin[i] = ld<S, L, i>(slot<S>(sb ? a.pb : a.pa, P) + (n + nbr_off<L, j>(o)), a);
+        fin[j] = ld<S, L, j>(slot<S>(sf ? a.pa : a.pb, P) + n, a);
+        gather_walls<L, S, P + 1>(a, n, o, walls, fin);
+    }
+}
+
+template <class L, int P = 0> __device__ __forceinline__ unsigned wall_links(const LbmArgs& a, u32 n, const Nbr& o) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
         const unsigned b = (a.flags[n + nbr_off<L, j>(o)] & kFlagTypeMask) != 0 ? 1U : 0U;
@@ -127,7 +148,7 @@ __device__ __forceinline__ unsigned wall_links(const LbmArgs& a, long long n, co
 }
 
 template <class L, class R, int P = 0>
-__device__ __forceinline__ void moving_wall_pairs(const LbmArgs& a, long long n, const Nbr& o, R rw, R* fin) {
+__device__ __forceinline__ void moving_wall_pairs(const LbmArgs& a, u32 n, const Nbr& o, R rw, R* fin) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
         const int idb = a.flags[n + nbr_off<L, j>(o)] & kFlagTypeMask;
@@ -147,16 +168,22 @@ __device__ __forceinline__ void moving_wall_pairs(const LbmArgs& a, long long n,
 }
 
 template <class L, class S, bool FLAGS>
-__device__ __forceinline__ void gather(const LbmArgs& a, const typename S::T* __restrict__ f, long long n,
-                                       const Nbr& o, std::uint8_t flag, typename S::R* fin) {
-    using R = typename S::R;
-    const bool odd = a.odd != 0;
-    unsigned walls = 0U;
+__device__ __forceinline__ void gather_loads(const LbmArgs& a, u32 n, const Nbr& o, std::uint8_t flag,
+                                             typename S::R* fin) {
+    fin[0] = ld<S, L, 0>(static_cast<const typename S::T*>(a.rest) + n, a);
     if constexpr (FLAGS) {
-        if (flag & kFlagNearWall) walls = wall_links<L>(a, n, o);
+        if (flag & kFlagNearWall) {
+            gather_walls<L, S>(a, n, o, wall_links<L>(a, n, o), fin);
+            return;
+        }
     }
-    fin[0] = ld<S, L, 0>(f + n, a);
-    gather_pairs<L, S, FLAGS>(a, f, n, o, walls, odd, fin);
+    gather_plain<L, S>(a, n, o, fin);
+}
+
+template <class L, class S, bool FLAGS>
+__device__ __forceinline__ void gather_fixup(const LbmArgs& a, u32 n, const Nbr& o, std::uint8_t flag,
+                                             typename S::R* fin) {
+    using R = typename S::R;
     if constexpr (FLAGS) {
         if (flag & kFlagNearMoving) {
             R rho0 = R(0);
@@ -168,55 +195,94 @@ __device__ __forceinline__ void gather(const LbmArgs& a, const typename S::T* __
     }
 }
 
+template <class L, class S, bool FLAGS>
+__device__ __forceinline__ void gather(const LbmArgs& a, u32 n, const Nbr& o, std::uint8_t flag,
+                                       typename S::R* fin) {
+    gather_loads<L, S, FLAGS>(a, n, o, flag, fin);
+    gather_fixup<L, S, FLAGS>(a, n, o, flag, fin);
+}
+
 // ------------------------------------------------------------------ scatter
 // Post-collision values go back to the slots the pair was read from
 // (reference esoteric_pull.hpp:367-382):
 //   even step: f[j][n] = fout_i, f[i][nb] = fout_j
 //   odd step:  f[i][n] = fout_i, f[j][nb] = fout_j
+// i.e. fout_i -> pb[p][n], fout_j -> pa[p][nb].
 template <class L, class S, int P = 0>
-__device__ __forceinline__ void scatter_pairs(const LbmArgs& a, typename S::T* __restrict__ f, long long n,
-                                              const Nbr& o, bool odd, const typename S::R* fout) {
+__device__ __forceinline__ void scatter_pairs(const LbmArgs& a, u32 n, const Nbr& o, const typename S::R* fout) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
-        const long long nb = n + nbr_off<L, j>(o);
-        const std::size_t N = a.N;
-        st<S, L, i>(f + (odd ? i : j) * N + n, fout[i], a);
-        st<S, L, j>(f + (odd ? j : i) * N + nb, fout[j], a);
-        scatter_pairs<L, S, P + 1>(a, f, n, o, odd, fout);
+        st<S, L, i>(slot_mut<S>(a.pb, P) + n, fout[i], a);
+        st<S, L, j>(slot_mut<S>(a.pa, P) + (n + nbr_off<L, j>(o)), fout[j], a);
+        scatter_pairs<L, S, P + 1>(a, n, o, fout);
     }
 }
 
+template <class L, class S>
+__device__ __forceinline__ void scatter(const LbmArgs& a, u32 n, const Nbr& o, const typename S::R* fout) {
+    st<S, L, 0>(static_cast<typename S::T*>(a.rest) + n, fout[0], a);
+    scatter_pairs<L, S>(a, n, o, fout);
+}
+
+// ------------------------------------------------------------------ helpers
+// Reciprocal: the FP32 path uses the hardware approximation (__fdividef,
+// ~2 ulp), well inside the FP32 parity tolerance; FP64 stays IEEE.
+__device__ __forceinline__ float rcp(float x) { return __fdividef(1.0F, x); }
+__device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+
 // ---------------------------------------------------------------- moments
+// rho and u of a cell (reference esoteric_pull.hpp:384-406), summed per
+// opposite pair: s_p = f_i + f_j, d_p = f_i - f_j (c_j = -c_i).
+template <class L, class R, int P = 0>
+__device__ __forceinline__ void pair_sums(const R* f, R* s, R* d) {
+    if constexpr (P < L::PAIRS) {
+        constexpr int i = 2 * P + 1, j = i + 1;
+        s[P] = f[i] + f[j];
+        d[P] = f[i] - f[j];
+        pair_sums<L, R, P + 1>(f, s, d);
+    }
+}
+
+template <class L, class R>
+__device__ __forceinline__ void pair_moments(R f0, const R* s, const R* d, R& rho, R& jx, R& jy, R& jz) {
+    R r = f0, x = R(0), y = R(0), z = R(0);
+#pragma unroll
+    for (int p = 0; p < L::PAIRS; ++p) {
+        const int i = 2 * p + 1;
+        r += s[p];
+        if (L::cx(i) > 0) x += d[p];
+        if (L::cx(i) < 0) x -= d[p];
+        if (L::cy(i) > 0) y += d[p];
+        if (L::cy(i) < 0) y -= d[p];
+        if (L::cz(i) > 0) z += d[p];
+        if (L::cz(i) < 0) z -= d[p];
+    }
+    rho = r;
+    jx = x;
+    jy = y;
+    jz = z;
+}
+
 template <class L, class R>
 __device__ __forceinline__ void moments(const R* fin, R& rho, R& ux, R& uy, R& uz) {
-    R r = R(0), jx = R(0), jy = R(0), jz = R(0);
-#pragma unroll
-    for (int d = 0; d < L::Q; ++d) {
-        r += fin[d];
-        if (L::cx(d) > 0) jx += fin[d];
-        if (L::cx(d) < 0) jx -= fin[d];
-        if (L::cy(d) > 0) jy += fin[d];
-        if (L::cy(d) < 0) jy -= fin[d];
-        if (L::cz(d) > 0) jz += fin[d];
-        if (L::cz(d) < 0) jz -= fin[d];
-    }
+    R s[L::PAIRS], d[L::PAIRS], jx, jy, jz;
+    pair_sums<L, R>(fin, s, d);
+    pair_moments<L, R>(fin[0], s, d, rho, jx, jy, jz);
     // reference esoteric_pull.hpp:397-405: u = 0 when rho <= 0
-    const R inv = r > R(0) ? R(1) / r : R(0);
-    rho = r;
+    const R inv = rho > R(0) ? rcp(rho) : R(0);
     ux = jx * inv;
     uy = jy * inv;
     uz = jz * inv;
 }
 
-template <class R>
-__device__ __forceinline__ void cell_acceleration(const LbmArgs& a, long long n, R& ax, R& ay, R& az) {
+template <class R> __device__ __forceinline__ void cell_acceleration(const LbmArgs& a, u32 n, R& ax, R& ay, R& az) {
     ax = R(a.ax);
     ay = R(a.ay);
     az = R(a.az);
-    if (a.local_a) {
-        ax += R(a.local_a[n]);
-        ay += R(a.local_a[a.N + n]);
-        az += R(a.local_a[2 * a.N + n]);
+    if (a.ax_field) {
+        ax += R(a.ax_field[n]);
+        ay += R(a.ay_field[n]);
+        az += R(a.az_field[n]);
     }
 }
 
@@ -224,22 +290,24 @@ __device__ __forceinline__ void cell_acceleration(const LbmArgs& a, long long n,
 // coefficient K = 18 sqrt(2) Cs^2 as a parameter).  The non-equilibrium
 // momentum flux is formed as sum c_a c_b f - rho (delta_ab / 3 + u_a u_b),
 // which equals sum c_a c_b (f - feq) on D3Q19/D3Q27 (both lattices are
-// fourth-order isotropic) and needs no per-direction equilibria.
+// fourth-order isotropic) and needs no per-direction equilibria; c_a c_b is
+// even in c, so the sums run over pair sums s_p.
 template <class L, class R>
-__device__ __forceinline__ R les_tau(const R* fin, R rho, R ux, R uy, R uz, R tau, R k) {
+__device__ __forceinline__ R les_tau(const R* s, R rho, R ux, R uy, R uz, R tau, R k) {
     if (!(rho > R(0))) return tau;
     R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
 #pragma unroll
-    for (int d = 1; d < L::Q; ++d) {
-        if (L::cx(d) != 0) sxx += fin[d];
-        if (L::cy(d) != 0) syy += fin[d];
-        if (L::cz(d) != 0) szz += fin[d];
-        if (L::cx(d) * L::cy(d) > 0) sxy += fin[d];
-        if (L::cx(d) * L::cy(d) < 0) sxy -= fin[d];
-        if (L::cx(d) * L::cz(d) > 0) sxz += fin[d];
-        if (L::cx(d) * L::cz(d) < 0) sxz -= fin[d];
-        if (L::cy(d) * L::cz(d) > 0) syz += fin[d];
-        if (L::cy(d) * L::cz(d) < 0) syz -= fin[d];
+    for (int p = 0; p < L::PAIRS; ++p) {
+        const int i = 2 * p + 1;
+        if (L::cx(i) != 0) sxx += s[p];
+        if (L::cy(i) != 0) syy += s[p];
+        if (L::cz(i) != 0) szz += s[p];
+        if (L::cx(i) * L::cy(i) > 0) sxy += s[p];
+        if (L::cx(i) * L::cy(i) < 0) sxy -= s[p];
+        if (L::cx(i) * L::cz(i) > 0) sxz += s[p];
+        if (L::cx(i) * L::cz(i) < 0) sxz -= s[p];
+        if (L::cy(i) * L::cz(i) > 0) syz += s[p];
+        if (L::cy(i) * L::cz(i) < 0) syz -= s[p];
     }
     const R third = R(1.0 / 3.0);
     const R pxx = sxx - rho * (third + ux * ux);
@@ -249,125 +317,162 @@ __device__ __forceinline__ R les_tau(const R* fin, R rho, R ux, R uy, R uz, R ta
     const R pxz = sxz - rho * ux * uz;
     const R pyz = syz - rho * uy * uz;
     const R q = pxx * pxx + pyy * pyy + pzz * pzz + R(2) * (pxy * pxy + pxz * pxz + pyz * pyz);
-    return R(0.5) * (tau + sqrt(tau * tau + k * sqrt(q) / rho));
+    return R(0.5) * (tau + sqrt(tau * tau + k * sqrt(q) * rcp(rho)));
 }
 
 // ---------------------------------------------------------------- collision
-// BGK (reference esoteric_pull.hpp:408-432) or TRT (reference
-// one_step_pull.hpp:187-204), both with Guo forcing, written per opposite
-// pair (i, j): the equilibrium splits into a symmetric part
-// w rho (1 - 1.5 u^2 + 4.5 (c.u)^2) and an antisymmetric part 3 w rho (c.u),
-// the Guo source into w (9 (c.u)(c.F) - 3 u.F) and 3 w (c.F).  Gray-LBM
-// partial bounce-back then mixes in the incoming opposite population:
-// f_i <- (1 - n_s) f_i* + n_s fin_j (Walsh, Burwinkle & Saar 2009).
-template <class L, class R, int COLL, bool GRAY, int P = 0>
-__device__ __forceinline__ void collide_pairs(R* f, R rho, R ux, R uy, R uz, R fx, R fy, R fz, R usq15, R uf3,
-                                              R omega, R omega_m, R gp, R gm, R ns) {
+// Two-relaxation-time collision with Guo forcing (reference
+// one_step_pull.hpp:187-204; BGK, esoteric_pull.hpp:408-432, is the case
+// omega- = omega+), evaluated per opposite pair on s = f_i + f_j and
+// d = f_i - f_j:
+//   equilibrium  s_eq = 2 w rho (1 - 1.5 u^2 + 4.5 (c.u)^2),  d_eq = 6 w rho (c.u)
+//   Guo source   s_F  = 2 w (9 (c.u)(c.F) - 3 u.F),          d_F  = 6 w (c.F)
+//   s' = s - omega+ (s - s_eq) + (1 - omega+/2) s_F
+//   d' = d - omega- (d - d_eq) + (1 - omega-/2) d_F
+//   f_i' = (s' + d') / 2,  f_j' = (s' - d') / 2
+// Gray-LBM partial bounce-back then mixes in the incoming opposite population:
+// f_i <- (1 - n_s) f_i' + n_s fin_j (Walsh, Burwinkle & Saar 2009).
+template <class L, class R, bool FORCE, bool GRAY, int P = 0>
+__device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, R rho, R ux, R uy, R uz, R fx, R fy, R fz,
+                                              R base, R uf3, R omega, R omega_m, R gp, R gm, R ns) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
-        constexpr R w = R(L::w(i));
+        constexpr R w2 = R(2.0 * L::w(i));
         const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
-        const R cf = R(L::cx(i)) * fx + R(L::cy(i)) * fy + R(L::cz(i)) * fz;
-        const R wr = w * rho;
-        const R eqp = wr * (R(1) - usq15 + R(4.5) * cu * cu);
-        const R eqm = wr * (R(3) * cu);
-        const R fp = w * (R(9) * cu * cf - uf3);
-        const R fm = w * (R(3) * cf);
-        const R fi = f[i], fj = f[j];
-        R oi, oj;
-        if constexpr (COLL == kBGK) {
-            oi = fi - omega * (fi - (eqp + eqm)) + gp * (fp + fm);
-            oj = fj - omega * (fj - (eqp - eqm)) + gp * (fp - fm);
-        } else {
-            const R sp = R(0.5) * (fi + fj) - eqp;
-            const R sm = R(0.5) * (fi - fj) - eqm;
-            const R common = gp * fp - omega * sp;
-            const R anti = gm * fm - omega_m * sm;
-            oi = fi + common + anti;
-            oj = fj + common - anti;
+        const R wr2 = w2 * rho;
+        const R s_eq = wr2 * (base + R(4.5) * cu * cu);
+        const R d_eq = wr2 * (R(3) * cu);
+        R sp = s[P] - omega * (s[P] - s_eq);
+        R dp = d[P] - omega_m * (d[P] - d_eq);
+        if constexpr (FORCE) {
+            const R cf = R(L::cx(i)) * fx + R(L::cy(i)) * fy + R(L::cz(i)) * fz;
+            sp += gp * (w2 * (R(9) * cu * cf - uf3));
+            dp += gm * (w2 * (R(3) * cf));
         }
+        R oi = R(0.5) * (sp + dp);
+        R oj = R(0.5) * (sp - dp);
         if constexpr (GRAY) {
+            const R fi = R(0.5) * (s[P] + d[P]);
+            const R fj = R(0.5) * (s[P] - d[P]);
             oi = (R(1) - ns) * oi + ns * fj;
             oj = (R(1) - ns) * oj + ns * fi;
         }
         f[i] = oi;
         f[j] = oj;
-        collide_pairs<L, R, COLL, GRAY, P + 1>(f, rho, ux, uy, uz, fx, fy, fz, usq15, uf3, omega, omega_m, gp, gm,
-                                               ns);
+        collide_pairs<L, R, FORCE, GRAY, P + 1>(f, s, d, rho, ux, uy, uz, fx, fy, fz, base, uf3, omega, omega_m, gp,
+                                                gm, ns);
     }
 }
 
-template <class L, class R, int COLL, bool LES, bool GRAY>
-__device__ __forceinline__ void collide(const LbmArgs& a, long long n, R* f) {
-    R rho, ux, uy, uz, ax, ay, az;
-    moments<L, R>(f, rho, ux, uy, uz);
-    cell_acceleration<R>(a, n, ax, ay, az);
-    ux += R(0.5) * ax;
-    uy += R(0.5) * ay;
-    uz += R(0.5) * az;
-    R tau = R(a.tau);
-    if constexpr (LES) tau = les_tau<L, R>(f, rho, ux, uy, uz, tau, R(a.les_k));
-    const R omega = R(1) / tau;
-    R omega_m = omega;
-    if constexpr (COLL == kTRT) {
-        // tau- = 1/2 + Lambda / (tau+ - 1/2): omega- = (tau+ - 1/2) / (Lambda + (tau+ - 1/2) / 2)
-        if (a.omega_minus > 0.0) {
-            omega_m = R(a.omega_minus);
-        } else {
-            const R sp = tau - R(0.5);
-            omega_m = sp / (R(a.trt_magic) + R(0.5) * sp);
-        }
+template <class L, class R, bool LES, bool GRAY, bool FORCE>
+__device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
+    R s[L::PAIRS], d[L::PAIRS];
+    pair_sums<L, R>(f, s, d);
+    R rho, jx, jy, jz;
+    pair_moments<L, R>(f[0], s, d, rho, jx, jy, jz);
+    const R inv = rho > R(0) ? rcp(rho) : R(0);
+    R ux = jx * inv, uy = jy * inv, uz = jz * inv;
+    R ax = R(0), ay = R(0), az = R(0);
+    if constexpr (FORCE) {
+        cell_acceleration<R>(a, n, ax, ay, az);
+        ux += R(0.5) * ax;
+        uy += R(0.5) * ay;
+        uz += R(0.5) * az;
     }
-    const R fx = rho * ax, fy = rho * ay, fz = rho * az;
-    const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
-    const R uf3 = R(3) * (ux * fx + uy * fy + uz * fz);
+    R tau = R(a.tau);
+    if constexpr (LES) tau = les_tau<L, R>(s, rho, ux, uy, uz, tau, R(a.les_k));
+    const R omega = rcp(tau);
+    R omega_m;
+    if (a.omega_minus > 0.0) {
+        omega_m = R(a.omega_minus);          // fixed TRT antisymmetric rate
+    } else if (a.omega_minus < 0.0) {
+        omega_m = omega;                     // BGK
+    } else {
+        // TRT magic: tau- = 1/2 + Lambda / (tau+ - 1/2)
+        const R sp = tau - R(0.5);
+        omega_m = sp * rcp(R(a.trt_magic) + R(0.5) * sp);
+    }
+    const R base = R(1) - R(1.5) * (ux * ux + uy * uy + uz * uz);
+    R fx = R(0), fy = R(0), fz = R(0), uf3 = R(0);
+    if constexpr (FORCE) {
+        fx = rho * ax;
+        fy = rho * ay;
+        fz = rho * az;
+        uf3 = R(3) * (ux * fx + uy * fy + uz * fz);
+    }
     const R gp = R(1) - R(0.5) * omega;
     const R gm = R(1) - R(0.5) * omega_m;
     R ns = R(0);
     if constexpr (GRAY) ns = R(a.ns[n]);
-    // rest population
     {
         constexpr R w0 = R(L::w(0));
         const R f0 = f[0];
-        R o0 = f0 - omega * (f0 - w0 * rho * (R(1) - usq15)) - gp * w0 * uf3;
+        R o0 = f0 - omega * (f0 - w0 * rho * base);
+        if constexpr (FORCE) o0 -= gp * w0 * uf3;
         if constexpr (GRAY) o0 = (R(1) - ns) * o0 + ns * f0;
         f[0] = o0;
     }
-    collide_pairs<L, R, COLL, GRAY>(f, rho, ux, uy, uz, fx, fy, fz, usq15, uf3, omega, omega_m, gp, gm, ns);
+    collide_pairs<L, R, FORCE, GRAY>(f, s, d, rho, ux, uy, uz, fx, fy, fz, base, uf3, omega, omega_m, gp, gm, ns);
 }
 
-// ------------------------------------------------------------------ kernels
-template <class L, class S, int COLL, bool LES, bool FLAGS, bool GRAY>
-__global__ void __launch_bounds__(256) k_step(const __grid_constant__ LbmArgs a) {
+// ---------------------------------------------------------------- the step
+// Cells per thread (stacked in z) of the step kernel: the loads of all of a
+// thread's cells are in flight together.  One cell per thread measured best
+// on B200 for every storage type (more cells cost occupancy through
+// registers); two stay selectable for tuning.
+template <class S> struct StepCells {
+    static constexpr int value = 1;
+};
+
+template <class L, class S, bool LES, bool FLAGS, bool GRAY, int CPT>
+__global__ void __launch_bounds__(128) k_step(const __grid_constant__ LbmArgs a) {
     using R = typename S::R;
-    const long long x = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const long long y = static_cast<long long>(blockIdx.y) * blockDim.y + threadIdx.y;
-    const long long z = blockIdx.z;
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z0 = blockIdx.z * CPT;
     if (x >= a.nx || y >= a.ny) return;
-    const long long n = (z * a.ny + y) * a.nx + x;
-    std::uint8_t flag = 0;
-    if constexpr (FLAGS) {
-        flag = a.flags[n];
-        if (flag & kFlagTypeMask) return; // walls hold no populations of their own
+    R fin[CPT][L::Q];
+    std::uint8_t flag[CPT];
+    bool live[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        const u32 z = z0 + c;
+        const u32 n = (z * a.ny + y) * a.nx + x;
+        live[c] = z < a.nz;
+        flag[c] = 0;
+        if constexpr (FLAGS) {
+            if (live[c]) {
+                flag[c] = a.flags[n];
+                live[c] = (flag[c] & kFlagTypeMask) == 0; // walls hold no populations of their own
+            }
+        }
+        if (live[c]) gather_loads<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag[c], fin[c]);
     }
-    const Nbr o = make_nbr(a, x, y, z);
-    typename S::T* f = static_cast<typename S::T*>(a.f);
-    R fin[L::Q];
-    gather<L, S, FLAGS>(a, f, n, o, flag, fin);
-    collide<L, R, COLL, LES, GRAY>(a, n, fin);
-    scatter_pairs<L, S>(a, f, n, o, a.odd != 0, fin);
-    st<S, L, 0>(f + n, fin[0], a);
+    const bool force = a.has_force != 0;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        if (!live[c]) continue;
+        const u32 z = z0 + c;
+        const u32 n = (z * a.ny + y) * a.nx + x;
+        const Nbr o = make_nbr(a, x, y, z);
+        gather_fixup<L, S, FLAGS>(a, n, o, flag[c], fin[c]);
+        if (force)
+            collide<L, R, LES, GRAY, true>(a, n, fin[c]);
+        else
+            collide<L, R, LES, GRAY, false>(a, n, fin[c]);
+        scatter<L, S>(a, n, o, fin[c]);
+    }
 }
 
 // Equilibrium initialisation into the esoteric slots of time step 0
 // (reference esoteric_pull.hpp:312-333; Taylor-Green field :121-137).  Wall
 // links additionally seed the partner slot, so that the first step's bounced
 // loads see the cell's own equilibrium exactly as the reference's first
-// solid step does.
+// solid step does.  Uses the parity-0 tables.
 template <class L, class S, bool FLAGS, int P = 0>
-__device__ __forceinline__ void init_pairs(const LbmArgs& a, typename S::T* f, long long n, const Nbr& o,
-                                           unsigned walls, typename S::R rho, typename S::R ux, typename S::R uy,
-                                           typename S::R uz, typename S::R usq15) {
+__device__ __forceinline__ void init_pairs(const LbmArgs& a, u32 n, const Nbr& o, unsigned walls, typename S::R rho,
+                                           typename S::R ux, typename S::R uy, typename S::R uz,
+                                           typename S::R usq15) {
     using R = typename S::R;
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
@@ -375,26 +480,25 @@ __device__ __forceinline__ void init_pairs(const LbmArgs& a, typename S::T* f, l
         const R wr = R(L::w(i)) * rho;
         const R fi = wr * (R(1) + R(3) * cu + R(4.5) * cu * cu - usq15);
         const R fj = wr * (R(1) - R(3) * cu + R(4.5) * cu * cu - usq15);
-        const long long nb = n + nbr_off<L, j>(o);
-        const std::size_t N = a.N;
-        st<S, L, i>(f + i * N + nb, fi, a);
-        st<S, L, j>(f + j * N + n, fj, a);
+        const u32 nb = n + nbr_off<L, j>(o);
+        st<S, L, i>(static_cast<typename S::T*>(a.fd[i]) + nb, fi, a);
+        st<S, L, j>(static_cast<typename S::T*>(a.fd[j]) + n, fj, a);
         if constexpr (FLAGS) {
-            if ((walls >> (2 * P)) & 1U) st<S, L, j>(f + j * N + nb, fi, a);
-            if ((walls >> (2 * P + 1)) & 1U) st<S, L, i>(f + i * N + n, fj, a);
+            if ((walls >> (2 * P)) & 1U) st<S, L, j>(static_cast<typename S::T*>(a.fd[j]) + nb, fi, a);
+            if ((walls >> (2 * P + 1)) & 1U) st<S, L, i>(static_cast<typename S::T*>(a.fd[i]) + n, fj, a);
         }
-        init_pairs<L, S, FLAGS, P + 1>(a, f, n, o, walls, rho, ux, uy, uz, usq15);
+        init_pairs<L, S, FLAGS, P + 1>(a, n, o, walls, rho, ux, uy, uz, usq15);
     }
 }
 
 template <class L, class S, bool FLAGS>
-__global__ void __launch_bounds__(256) k_init(const __grid_constant__ LbmArgs a, const InitSpec s) {
+__global__ void __launch_bounds__(128) k_init(const __grid_constant__ LbmArgs a, const InitSpec s) {
     using R = typename S::R;
-    const long long x = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const long long y = static_cast<long long>(blockIdx.y) * blockDim.y + threadIdx.y;
-    const long long z = blockIdx.z;
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
     if (x >= a.nx || y >= a.ny) return;
-    const long long n = (z * a.ny + y) * a.nx + x;
+    const u32 n = (z * a.ny + y) * a.nx + x;
     unsigned walls = 0U;
     const Nbr o = make_nbr(a, x, y, z);
     if constexpr (FLAGS) {
@@ -409,40 +513,42 @@ __global__ void __launch_bounds__(256) k_init(const __grid_constant__ LbmArgs a,
         uy = R(s.uy);
         uz = R(s.uz);
     } else if (s.kind == 1) {
-        const float two_pi = 2.0F * 3.14159265358979323846F;
-        const float xf = (static_cast<float>(x) + 0.5F) / static_cast<float>(a.nx);
-        const float yf = (static_cast<float>(y) + 0.5F) / static_cast<float>(a.ny);
-        const float zf = (static_cast<float>(z) + 0.5F) / static_cast<float>(a.nz);
-        const float sx = sinf(two_pi * xf), cx = cosf(two_pi * xf);
-        const float sy = sinf(two_pi * yf), cy = cosf(two_pi * yf);
-        const float cz = cosf(two_pi * zf);
+        // Evaluated in the arithmetic type, as the reference's FP32
+        // (esoteric_pull.hpp:121-137) and FP64 (precision_pull.hpp:75-95) solvers do.
+        const R two_pi = R(2) * R(3.14159265358979323846);
+        const R xf = (R(x) + R(0.5)) / R(a.nx);
+        const R yf = (R(y) + R(0.5)) / R(a.ny);
+        const R zf = (R(z) + R(0.5)) / R(a.nz);
+        const R sx = sin(two_pi * xf), cx = cos(two_pi * xf);
+        const R sy = sin(two_pi * yf), cy = cos(two_pi * yf);
+        const R cz = cos(two_pi * zf);
+        const R amp = R(s.amplitude);
         rho = R(1);
-        ux = R(s.amplitude * sx * cy * cz);
-        uy = R(-s.amplitude * cx * sy * cz);
+        ux = amp * sx * cy * cz;
+        uy = -amp * cx * sy * cz;
         uz = R(0);
     } else {
         rho = R(s.fields[n]);
-        ux = R(s.fields[a.N + n]);
-        uy = R(s.fields[2 * a.N + n]);
-        uz = R(s.fields[3 * a.N + n]);
+        ux = R(s.fields[std::size_t(a.N) + n]);
+        uy = R(s.fields[2 * std::size_t(a.N) + n]);
+        uz = R(s.fields[3 * std::size_t(a.N) + n]);
     }
-    typename S::T* f = static_cast<typename S::T*>(a.f);
     const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
-    st<S, L, 0>(f + n, R(L::w(0)) * rho * (R(1) - usq15), a);
-    init_pairs<L, S, FLAGS>(a, f, n, o, walls, rho, ux, uy, uz, usq15);
+    st<S, L, 0>(static_cast<typename S::T*>(a.fd[0]) + n, R(L::w(0)) * rho * (R(1) - usq15), a);
+    init_pairs<L, S, FLAGS>(a, n, o, walls, rho, ux, uy, uz, usq15);
 }
 
 // Macroscopic fields rho and u + a/2 (reference esoteric_pull.hpp:180-209 and
 // esoteric_pull_sycl.hpp:229-307); wall cells report rho = 0, u = 0.
 template <class L, class S, bool FLAGS, class OutT>
-__global__ void __launch_bounds__(256) k_macro(const __grid_constant__ LbmArgs a, OutT* rho_out, OutT* ux_out,
+__global__ void __launch_bounds__(128) k_macro(const __grid_constant__ LbmArgs a, OutT* rho_out, OutT* ux_out,
                                                OutT* uy_out, OutT* uz_out) {
     using R = typename S::R;
-    const long long x = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const long long y = static_cast<long long>(blockIdx.y) * blockDim.y + threadIdx.y;
-    const long long z = blockIdx.z;
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
     if (x >= a.nx || y >= a.ny) return;
-    const long long n = (z * a.ny + y) * a.nx + x;
+    const u32 n = (z * a.ny + y) * a.nx + x;
     std::uint8_t flag = 0;
     if constexpr (FLAGS) {
         flag = a.flags[n];
@@ -454,9 +560,8 @@ __global__ void __launch_bounds__(256) k_macro(const __grid_constant__ LbmArgs a
             return;
         }
     }
-    const Nbr o = make_nbr(a, x, y, z);
     R fin[L::Q];
-    gather<L, S, FLAGS>(a, static_cast<const typename S::T*>(a.f), n, o, flag, fin);
+    gather<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag, fin);
     R rho, ux, uy, uz, ax, ay, az;
     moments<L, R>(fin, rho, ux, uy, uz);
     cell_acceleration<R>(a, n, ax, ay, az);
@@ -468,13 +573,13 @@ __global__ void __launch_bounds__(256) k_macro(const __grid_constant__ LbmArgs a
 
 // Parity-independent populations [d][n] (reference esoteric_pull.hpp:257-267).
 template <class L, class S, bool FLAGS, class OutT>
-__global__ void __launch_bounds__(256) k_logical(const __grid_constant__ LbmArgs a, OutT* out) {
+__global__ void __launch_bounds__(128) k_logical(const __grid_constant__ LbmArgs a, OutT* out) {
     using R = typename S::R;
-    const long long x = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const long long y = static_cast<long long>(blockIdx.y) * blockDim.y + threadIdx.y;
-    const long long z = blockIdx.z;
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
     if (x >= a.nx || y >= a.ny) return;
-    const long long n = (z * a.ny + y) * a.nx + x;
+    const u32 n = (z * a.ny + y) * a.nx + x;
     R fin[L::Q];
     std::uint8_t flag = 0;
     bool wall = false;
@@ -482,10 +587,7 @@ __global__ void __launch_bounds__(256) k_logical(const __grid_constant__ LbmArgs
         flag = a.flags[n];
         wall = (flag & kFlagTypeMask) != 0;
     }
-    if (!wall) {
-        const Nbr o = make_nbr(a, x, y, z);
-        gather<L, S, FLAGS>(a, static_cast<const typename S::T*>(a.f), n, o, flag, fin);
-    }
+    if (!wall) gather<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag, fin);
 #pragma unroll
     for (int d = 0; d < L::Q; ++d) out[static_cast<std::size_t>(d) * a.N + n] = wall ? OutT(0) : OutT(fin[d]);
 }
@@ -521,7 +623,7 @@ __device__ __forceinline__ void block_combine(double (&acc)[kReduceFields]) {
     if (warp == 0) {
 #pragma unroll
         for (int k = 0; k < kReduceFields; ++k) {
-            double v = lane < kReduceThreads / 32 ? sm[lane][k] : (k == 5 ? 0.0 : 0.0);
+            const double v = lane < kReduceThreads / 32 ? sm[lane][k] : 0.0;
             acc[k] = k == 5 ? warp_max(v) : warp_sum(v);
         }
     }
@@ -531,19 +633,18 @@ template <class L, class S, bool FLAGS>
 __global__ void __launch_bounds__(kReduceThreads) k_reduce(const __grid_constant__ LbmArgs a, double* partials) {
     using R = typename S::R;
     double acc[kReduceFields] = {0, 0, 0, 0, 0, 0, 0};
-    const long long rows = a.ny * a.nz;
-    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
-        const long long y = row % a.ny, z = row / a.ny;
-        for (long long x = threadIdx.x; x < a.nx; x += blockDim.x) {
-            const long long n = row * a.nx + x;
+    const u32 rows = a.ny * a.nz;
+    for (u32 row = blockIdx.x; row < rows; row += gridDim.x) {
+        const u32 y = row % a.ny, z = row / a.ny;
+        for (u32 x = threadIdx.x; x < a.nx; x += blockDim.x) {
+            const u32 n = row * a.nx + x;
             std::uint8_t flag = 0;
             if constexpr (FLAGS) {
                 flag = a.flags[n];
                 if (flag & kFlagTypeMask) continue;
             }
-            const Nbr o = make_nbr(a, x, y, z);
             R fin[L::Q];
-            gather<L, S, FLAGS>(a, static_cast<const typename S::T*>(a.f), n, o, flag, fin);
+            gather<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag, fin);
             R rho, ux, uy, uz, ax, ay, az;
             moments<L, R>(fin, rho, ux, uy, uz);
             cell_acceleration<R>(a, n, ax, ay, az);
@@ -567,7 +668,8 @@ __global__ void __launch_bounds__(kReduceThreads) k_reduce(const __grid_constant
         for (int k = 0; k < kReduceFields; ++k) partials[static_cast<std::size_t>(blockIdx.x) * kReduceFields + k] = acc[k];
 }
 
-static __global__ void __launch_bounds__(kReduceThreads) k_reduce_final(const double* partials, int blocks, double* out) {
+static __global__ void __launch_bounds__(kReduceThreads) k_reduce_final(const double* partials, int blocks,
+                                                                        double* out) {
     double acc[kReduceFields] = {0, 0, 0, 0, 0, 0, 0};
     for (int b = threadIdx.x; b < blocks; b += blockDim.x)
 #pragma unroll
@@ -584,13 +686,13 @@ static __global__ void __launch_bounds__(kReduceThreads) k_reduce_final(const do
 // Derives the internal flag byte (wall id, near-wall bits) from the caller's
 // flags.  Near-wall bits let interior cells skip all neighbour-flag loads.
 template <class L>
-__global__ void __launch_bounds__(256) k_prepare_flags(const __grid_constant__ LbmArgs a, const std::uint8_t* user,
+__global__ void __launch_bounds__(128) k_prepare_flags(const __grid_constant__ LbmArgs a, const std::uint8_t* user,
                                                        std::uint8_t* out) {
-    const long long x = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const long long y = static_cast<long long>(blockIdx.y) * blockDim.y + threadIdx.y;
-    const long long z = blockIdx.z;
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
     if (x >= a.nx || y >= a.ny) return;
-    const long long n = (z * a.ny + y) * a.nx + x;
+    const u32 n = (z * a.ny + y) * a.nx + x;
     const std::uint8_t t = user[n] & kFlagTypeMask;
     if (t != 0) {
         out[n] = t;
@@ -600,7 +702,7 @@ __global__ void __launch_bounds__(256) k_prepare_flags(const __grid_constant__ L
     std::uint8_t b = 0;
 #pragma unroll
     for (int d = 1; d < L::Q; ++d) {
-        long long m = n + o.ox[L::cx(d) + 1] + o.oy[L::cy(d) + 1] + o.oz[L::cz(d) + 1];
+        const u32 m = n + o.ox[L::cx(d) + 1] + o.oy[L::cy(d) + 1] + o.oz[L::cz(d) + 1];
         const std::uint8_t u = user[m] & kFlagTypeMask;
         if (u != 0) b |= kFlagNearWall;
         if (u >= 2) b |= kFlagNearMoving;

@@ -23,6 +23,7 @@ struct KernelKey {
     bool les;
     bool flags;
     bool gray;
+    int cells_per_thread; // step kernel; 0 = default for the storage type
 };
 
 dim3 cell_block(long long nx, long long ny, const LaunchShape& s);

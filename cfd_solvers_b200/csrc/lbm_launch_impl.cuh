@@ -24,31 +24,42 @@ template <class F> cudaError_t with_lattice(int q, F&& f) {
     return cudaErrorInvalidValue;
 }
 
-template <class L, class S, int C, bool LES, bool FL>
-cudaError_t step_gray(bool gray, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    if (gray)
-        k_step<L, S, C, LES, FL, true><<<g, b, 0, s>>>(a);
-    else
-        k_step<L, S, C, LES, FL, false><<<g, b, 0, s>>>(a);
-    return cudaGetLastError();
+// Cells per thread of the step kernel: 0 = the storage type's default.
+template <class L, class S, bool LES, bool FL, bool GR>
+cudaError_t step_cpt(int cpt, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    if (cpt <= 0) cpt = StepCells<S>::value;
+    auto go = [&](auto kernel, unsigned c) {
+        dim3 gz(g.x, g.y, (a.nz + c - 1U) / c);
+        kernel<<<gz, b, 0, s>>>(a);
+        return cudaGetLastError();
+    };
+    switch (cpt) {
+    case 1: return go(k_step<L, S, LES, FL, GR, 1>, 1U);
+    case 2: return go(k_step<L, S, LES, FL, GR, 2>, 2U);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
-template <class L, class S, int C, bool LES>
+template <class L, class S, bool LES, bool FL>
+cudaError_t step_gray(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    return k.gray ? step_cpt<L, S, LES, FL, true>(k.cells_per_thread, a, g, b, s)
+                  : step_cpt<L, S, LES, FL, false>(k.cells_per_thread, a, g, b, s);
+}
+
+template <class L, class S, bool LES>
 cudaError_t step_flags(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    return k.flags ? step_gray<L, S, C, LES, true>(k.gray, a, g, b, s) : step_gray<L, S, C, LES, false>(k.gray, a, g, b, s);
+    return k.flags ? step_gray<L, S, LES, true>(k, a, g, b, s) : step_gray<L, S, LES, false>(k, a, g, b, s);
 }
 
-template <class L, class S, int C>
-cudaError_t step_les(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    return k.les ? step_flags<L, S, C, true>(k, a, g, b, s) : step_flags<L, S, C, false>(k, a, g, b, s);
-}
-
+// The collision operator (BGK or TRT) is a runtime parameter of the kernel
+// (LbmArgs::omega_minus); the template axes are lattice, storage, LES,
+// flags, gray and cells per thread.
 template <int STORAGE>
 cudaError_t Launcher<STORAGE>::step(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
     using S = typename StorageOf<STORAGE>::type;
     return with_lattice(k.q, [&](auto lat) {
         using L = decltype(lat);
-        return k.collision == kTRT ? step_les<L, S, kTRT>(k, a, g, b, s) : step_les<L, S, kBGK>(k, a, g, b, s);
+        return k.les ? step_flags<L, S, true>(k, a, g, b, s) : step_flags<L, S, false>(k, a, g, b, s);
     });
 }
 

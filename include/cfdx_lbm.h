@@ -218,8 +218,10 @@ CFDX_API int cfdx_lbm_stream(cfdx_lbm* lbm, void** stream);
  * Reference: raw_storage, esoteric_pull.hpp:276-278. */
 CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* lbm, void** device_ptr, size_t* bytes);
 
-/* Threads per block of the cell kernels (x, y); 0,0 restores the default. */
-CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y);
+/* Launch shape of the cell kernels: threads per block (x, y) and cells per
+ * thread of the step kernel (1 or 2, stacked in z); zeros restore the
+ * defaults. */
+CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, int cells_per_thread);
 
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths

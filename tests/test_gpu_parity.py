@@ -112,14 +112,20 @@ CASES = [
 ]
 
 
+def f32(v):
+    """The C ABI's config fields are float: mirror their rounding for the oracle."""
+    return float(np.float32(v))
+
+
 def oracle_config(O, q, nx, ny, nz, kw):
     les_k = 0.0
     if kw.get("smagorinsky_les"):
-        cs = kw.get("smagorinsky_cs", 0.0)
+        cs = f32(kw.get("smagorinsky_cs", 0.0))
         les_k = 18 * np.sqrt(2) * cs * cs if cs > 0 else O.reference_les_k()
-    return dict(q=q, nx=nx, ny=ny, nz=nz, collision=kw.get("collision", "bgk"), tau=kw.get("tau", 0.6),
-                tau_minus=kw.get("trt_tau_minus", 0.0), trt_magic=kw.get("trt_magic", 3 / 16), les_k=les_k,
-                accel=(kw.get("acceleration_x", 0.0), kw.get("acceleration_y", 0.0), kw.get("acceleration_z", 0.0)))
+    return dict(q=q, nx=nx, ny=ny, nz=nz, collision=kw.get("collision", "bgk"), tau=f32(kw.get("tau", 0.6)),
+                tau_minus=f32(kw.get("trt_tau_minus", 0.0)), trt_magic=f32(kw.get("trt_magic", 3 / 16)),
+                les_k=les_k, accel=(f32(kw.get("acceleration_x", 0.0)), f32(kw.get("acceleration_y", 0.0)),
+                                    f32(kw.get("acceleration_z", 0.0))))
 
 
 def case_inputs(kind, gray, local, nx, ny, nz, seed=7):
