@@ -134,6 +134,10 @@ struct cfdx_lbm {
     float wall_u[kMaxWallIds][3]{};
     float scale[27]{};
     LaunchShape shape{};
+    int variant = 0; // step kernel: 0 auto, 1 one cell per thread, 2 paired cells
+    // Automatic choice: the one-cell kernel measured faster on B200 for every
+    // configuration benchmarked, so auto selects it.
+    static constexpr bool paired_default = false;
     double les_k = 0.0;
     std::uint64_t h2d = 0, d2h = 0, syncs = 0;
 
@@ -143,6 +147,8 @@ struct cfdx_lbm {
         const std::size_t es = static_cast<std::size_t>(storage_bytes(key.storage));
         for (int d = 0; d < 27; ++d) a.fd[d] = d < key.q ? base + static_cast<std::size_t>(d) * N * es : nullptr;
         a.rest = a.fd[0];
+        a.base = f;
+        a.rest_off = 0U;
         set_parity(a, static_cast<int>(t & 1U));
         a.flags = key.flags ? flags : nullptr;
         a.ax_field = local_a;
@@ -178,15 +184,40 @@ struct cfdx_lbm {
     // n + c_{2p+2}, pb[p] at the cell itself (see LbmArgs).
     void set_parity(LbmArgs& a, int odd) const {
         a.odd = odd;
+        const bool offsets = static_cast<unsigned long long>(key.q) * N < (1ULL << 32);
         for (int p = 0; p < 13; ++p) {
             const int i = 2 * p + 1, j = i + 1;
             if (j < key.q) {
                 a.pa[p] = a.fd[odd ? j : i];
                 a.pb[p] = a.fd[odd ? i : j];
+                a.pa_off[p] = offsets ? static_cast<std::uint32_t>((odd ? j : i) * N) : 0U;
+                a.pb_off[p] = offsets ? static_cast<std::uint32_t>((odd ? i : j) * N) : 0U;
             } else {
                 a.pa[p] = a.pb[p] = nullptr;
+                a.pa_off[p] = a.pb_off[p] = 0U;
             }
         }
+    }
+    // The paired-cell step kernel needs FP32/FP16 storage, an even nx and
+    // element offsets that fit 32 bits.
+    bool paired_eligible() const {
+        return key.storage != kStoreF64 && cfg.nx % 2U == 0U &&
+               static_cast<unsigned long long>(key.q) * N < (1ULL << 32) &&
+               (shape.block_x == 0 || shape.block_x % 32 == 0);
+    }
+    void choose_variant() {
+        key.narrow = static_cast<unsigned long long>(key.q) * N < (1ULL << 32);
+        key.paired = variant == 2 || (variant == 0 && paired_default && paired_eligible());
+    }
+    dim3 step_block() const {
+        if (!key.paired) return block();
+        int bx = shape.block_x, by = shape.block_y;
+        if (bx <= 0 || by <= 0) {
+            const long long pairs = static_cast<long long>(cfg.nx / 2U);
+            bx = static_cast<int>(std::min<long long>(64, ((pairs + 31) / 32) * 32));
+            by = std::max(1, 128 / bx);
+        }
+        return dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by), 1U);
     }
     dim3 block() const { return cell_block(static_cast<long long>(cfg.nx), static_cast<long long>(cfg.ny), shape); }
     dim3 grid() const {
@@ -347,6 +378,7 @@ cudaError_t launch_reduce(const KernelKey& k, const LbmArgs& a, double* partials
     }
 }
 
+
 } // namespace cfdx
 
 extern "C" {
@@ -403,7 +435,8 @@ CFDX_API int cfdx_lbm_create(const cfdx_lbm_config* config, cfdx_lbm** out, char
         h->set_device();
         h->N = c.nx * c.ny * c.nz;
         require(h->N <= 0xffffffffULL, "lattice exceeds 2^32 - 1 cells");
-        h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false, 0};
+        h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false, 0, false, false};
+        h->choose_variant();
         h->les_k = c.smagorinsky_les ? (c.smagorinsky_cs > 0.0F
                                             ? 18.0 * std::sqrt(2.0) * double(c.smagorinsky_cs) * double(c.smagorinsky_cs)
                                             : double(reference_les_k()))
@@ -563,8 +596,13 @@ CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* h, const float* scale) {
         }
         for (int d = 0; d < h->key.q; ++d)
             require(std::isfinite(scale[d]) && scale[d] > 0.0F, "storage scales must be finite and positive");
-        for (int d = 1; d < h->key.q; d += 2)
-            require(scale[d] == scale[d + 1], "opposite directions must share a storage scale");
+        // Scales are applied per weight class inside the step kernel.
+        for (int d = 0; d < h->key.q; ++d) {
+            const double w = lattice_weight(h->key.q, d);
+            for (int e = 0; e < d; ++e)
+                if (lattice_weight(h->key.q, e) == w)
+                    require(scale[d] == scale[e], "directions of equal lattice weight must share a storage scale");
+        }
         for (int d = 0; d < h->key.q; ++d) h->scale[d] = scale[d];
     });
 }
@@ -572,7 +610,7 @@ CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* h, const float* scale) {
 CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
     return guarded([&] {
         checked(h);
-        const dim3 g = h->grid(), b = h->block();
+        const dim3 g = h->grid(), b = h->step_block();
         LbmArgs a = h->args();
         for (std::uint64_t i = 0; i < count; ++i) {
             h->set_parity(a, static_cast<int>(h->t & 1U));
@@ -762,19 +800,24 @@ CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* h, void** ptr, std::size_t* byte
     });
 }
 
-CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int cells_per_thread) {
+CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int variant) {
     return guarded([&] {
         require(h != nullptr, "null handle");
-        require(cells_per_thread == 0 || cells_per_thread == 1 || cells_per_thread == 2,
-                "cells per thread must be 0 (default), 1 or 2");
-        h->key.cells_per_thread = cells_per_thread;
+        require(variant >= 0 && variant <= 2, "step kernel variant must be 0 (auto), 1 (one cell) or 2 (paired)");
         if (bx == 0 && by == 0) {
             h->shape = LaunchShape{};
-            return;
+        } else {
+            require(bx > 0 && by > 0 && bx * by <= 128 && (bx * by) % 32 == 0,
+                    "block shape must have bx*by a multiple of 32 and at most 128");
+            h->shape = LaunchShape{bx, by};
         }
-        require(bx > 0 && by > 0 && bx * by <= 128 && (bx * by) % 32 == 0,
-                "block shape must have bx*by a multiple of 32 and at most 128");
-        h->shape = LaunchShape{bx, by};
+        h->variant = variant;
+        h->key.cells_per_thread = 1;
+        if (variant == 2)
+            require(h->paired_eligible(),
+                    "the paired-cell kernel needs FP32/FP16 storage, an even nx, q*cells < 2^32 and block_x a "
+                    "multiple of 32");
+        h->choose_variant();
     });
 }
 

@@ -50,4 +50,14 @@ struct D3Q27 {
     }
 };
 
+// Weight class of direction d: 0 rest, 1 axis, 2 face diagonal, 3 corner
+// (|c_x| + |c_y| + |c_z|); the weights, and the FP16 storage scales, are
+// constant within a class.
+template <class L> __host__ __device__ constexpr int weight_class(int d) {
+    return (L::cx(d) != 0 ? 1 : 0) + (L::cy(d) != 0 ? 1 : 0) + (L::cz(d) != 0 ? 1 : 0);
+}
+
+// A representative direction of each weight class.
+__host__ __device__ constexpr int class_rep(int k) { return k == 0 ? 0 : (k == 1 ? 1 : (k == 2 ? 7 : 19)); }
+
 } // namespace cfdx

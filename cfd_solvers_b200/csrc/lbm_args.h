@@ -32,11 +32,18 @@ enum Collision : int { kBGK = 0, kTRT = 1 };
 //   pb[p]    base of the slot pair p reads at the cell itself
 //            (direction 2p+2 at even parity, 2p+1 at odd parity)
 //   fd[d]    base of direction d (parity-free layouts: logical dumps, init)
+//   base, rest_off, pa_off[p], pb_off[p]: the same slots as element offsets
+//            from one base pointer (valid when q*N < 2^32; used by the
+//            paired-cell step kernel)
 struct LbmArgs {
     void* rest;
     void* pa[13];
     void* pb[13];
     void* fd[27];
+    void* base;
+    std::uint32_t rest_off;
+    std::uint32_t pa_off[13];
+    std::uint32_t pb_off[13];
     const std::uint8_t* flags; // internal flags or nullptr
     const float* ax_field;     // per-cell acceleration components or nullptr
     const float* ay_field;

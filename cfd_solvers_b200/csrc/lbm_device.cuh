@@ -33,37 +33,73 @@ namespace cfdx {
 using u32 = std::uint32_t;
 
 // ------------------------------------------------------------- storage traits
+// `delta` storage types hand the kernels the deviation f - w_d from the rest
+// weight instead of f itself; the collision then works in deviation space
+// (see collide), so decoding and encoding are one multiply each.
 struct StF32 {
     using T = float;
     using R = float;
+    static constexpr bool delta = false;
+    static constexpr bool scaled = false;
 };
 struct StF64 {
     using T = double;
     using R = double;
+    static constexpr bool delta = false;
+    static constexpr bool scaled = false;
 };
-// FP16 shifted storage: h = half((f - w_d) * s_d), f = w_d + float(h) / s_d.
+// FP16 shifted storage: h = half((f - w_d) * s_d); kernels see f - w_d = h / s_d.
 // Scales are equal within an opposite pair, so a bounced load that reads the
-// partner direction's slot decodes with the same constants.
+// partner direction's slot decodes with the same constant.
+// The step kernel keeps FP16 populations in storage units h (`scaled`) and
+// applies the scales per weight class (collide_scaled).
 struct StF16 {
     using T = __half;
     using R = float;
+    static constexpr bool delta = true;
+    static constexpr bool scaled = true;
 };
 
-template <class S, class L, int D>
+// RAW: FP16 values stay in storage units h (no scale applied).
+template <class S, class L, int D, bool RAW = false>
 __device__ __forceinline__ typename S::R ld(const typename S::T* p, const LbmArgs& a) {
     if constexpr (sizeof(typename S::T) == 2) {
-        return fmaf(__half2float(*p), a.inv_scale[D], static_cast<float>(L::w(D)));
+        if constexpr (RAW)
+            return __half2float(*p);
+        else
+            return __half2float(*p) * a.inv_scale[D];
     } else {
         return *p;
     }
 }
 
-template <class S, class L, int D>
+template <class S, class L, int D, bool RAW = false>
 __device__ __forceinline__ void st(typename S::T* p, typename S::R v, const LbmArgs& a) {
     if constexpr (sizeof(typename S::T) == 2) {
-        *p = __float2half_rn((v - static_cast<float>(L::w(D))) * a.scale[D]);
+        if constexpr (RAW)
+            *p = __float2half_rn(v);
+        else
+            *p = __float2half_rn(v * a.scale[D]);
     } else {
         *p = v;
+    }
+}
+
+// Value the kernels hold for an absolute population f of direction D.
+template <class S, class L, int D> __device__ __forceinline__ typename S::R held(typename S::R f) {
+    if constexpr (S::delta) {
+        return f - typename S::R(L::w(D));
+    } else {
+        return f;
+    }
+}
+
+// Absolute population from a held value.
+template <class S, class L> __device__ __forceinline__ typename S::R absolute(typename S::R v, int d) {
+    if constexpr (S::delta) {
+        return v + typename S::R(L::w(d));
+    } else {
+        return v;
     }
 }
 
@@ -106,33 +142,48 @@ template <class L, int D> __device__ __forceinline__ u32 nbr_off(const Nbr& o) {
 // step, which sits in the other slot of the same address -- the load takes
 // the other table.  Moving walls add 6 w_k rho (c_k . u_wall) (reference
 // src/lbm/d2q9.cpp:220-223) with rho this cell's pre-correction density.
-template <class S> __device__ __forceinline__ const typename S::T* slot(void* const* table, int p) {
-    return static_cast<const typename S::T*>(table[p]);
-}
-template <class S> __device__ __forceinline__ typename S::T* slot_mut(void* const* table, int p) {
-    return static_cast<typename S::T*>(table[p]);
-}
+// Slot addressing: NARROW kernels use 32-bit element offsets from one base
+// pointer (q*N < 2^32: one add and one wide multiply-add per access, no
+// per-access pointer loads); the wide form reads the 64-bit per-parity
+// pointer tables.
+template <class S, bool NARROW> struct Slots {
+    using T = typename S::T;
+    __device__ __forceinline__ static T* at(const LbmArgs& a, bool use_pa, int p, u32 idx) {
+        if constexpr (NARROW) {
+            return static_cast<T*>(a.base) + ((use_pa ? a.pa_off[p] : a.pb_off[p]) + idx);
+        } else {
+            return static_cast<T*>(use_pa ? a.pa[p] : a.pb[p]) + idx;
+        }
+    }
+    __device__ __forceinline__ static T* rest(const LbmArgs& a, u32 idx) {
+        if constexpr (NARROW) {
+            return static_cast<T*>(a.base) + (a.rest_off + idx);
+        } else {
+            return static_cast<T*>(a.rest) + idx;
+        }
+    }
+};
 
-template <class L, class S, int P = 0>
+template <class L, class S, bool NARROW, bool RAW = false, int P = 0>
 __device__ __forceinline__ void gather_plain(const LbmArgs& a, u32 n, const Nbr& o, typename S::R* fin) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
-        fin[i] = ld<S, L, i>(slot<S>(a.pa, P) + (n + nbr_off<L, j>(o)), a);
-        fin[j] = ld<S, L, j>(slot<S>(a.pb, P) + n, a);
-        gather_plain<L, S, P + 1>(a, n, o, fin);
+        fin[i] = ld<S, L, i, RAW>(Slots<S, NARROW>::at(a, true, P, n + nbr_off<L, j>(o)), a);
+        fin[j] = ld<S, L, j, RAW>(Slots<S, NARROW>::at(a, false, P, n), a);
+        gather_plain<L, S, NARROW, RAW, P + 1>(a, n, o, fin);
     }
 }
 
-template <class L, class S, int P = 0>
+template <class L, class S, bool NARROW, bool RAW = false, int P = 0>
 __device__ __forceinline__ void gather_walls(const LbmArgs& a, u32 n, const Nbr& o, unsigned walls,
                                              typename S::R* fin) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
         const bool sb = ((walls >> (2 * P)) & 1U) != 0U;
         const bool sf = ((walls >> (2 * P + 1)) & 1U) != 0U;
-        fin[i] = ld<S, L, i>(slot<S>(sb ? a.pb : a.pa, P) + (n + nbr_off<L, j>(o)), a);
-        fin[j] = ld<S, L, j>(slot<S>(sf ? a.pa : a.pb, P) + n, a);
-        gather_walls<L, S, P + 1>(a, n, o, walls, fin);
+        fin[i] = ld<S, L, i, RAW>(Slots<S, NARROW>::at(a, !sb, P, n + nbr_off<L, j>(o)), a);
+        fin[j] = ld<S, L, j, RAW>(Slots<S, NARROW>::at(a, sf, P, n), a);
+        gather_walls<L, S, NARROW, RAW, P + 1>(a, n, o, walls, fin);
     }
 }
 
@@ -167,17 +218,51 @@ __device__ __forceinline__ void moving_wall_pairs(const LbmArgs& a, u32 n, const
     }
 }
 
-template <class L, class S, bool FLAGS>
+template <class L, class S, bool FLAGS, bool NARROW = false, bool RAW = false>
 __device__ __forceinline__ void gather_loads(const LbmArgs& a, u32 n, const Nbr& o, std::uint8_t flag,
                                              typename S::R* fin) {
-    fin[0] = ld<S, L, 0>(static_cast<const typename S::T*>(a.rest) + n, a);
+    fin[0] = ld<S, L, 0, RAW>(Slots<S, NARROW>::rest(a, n), a);
     if constexpr (FLAGS) {
         if (flag & kFlagNearWall) {
-            gather_walls<L, S>(a, n, o, wall_links<L>(a, n, o), fin);
+            gather_walls<L, S, NARROW, RAW>(a, n, o, wall_links<L>(a, n, o), fin);
             return;
         }
     }
-    gather_plain<L, S>(a, n, o, fin);
+    gather_plain<L, S, NARROW, RAW>(a, n, o, fin);
+}
+
+// Moving-wall correction for values held in FP16 storage units: the
+// correction 6 w_k rho (c_k . u_wall) is scaled by s_k.
+template <class L, int P = 0>
+__device__ __forceinline__ void moving_wall_pairs_scaled(const LbmArgs& a, u32 n, const Nbr& o, float rw, float* h) {
+    if constexpr (P < L::PAIRS) {
+        constexpr int i = 2 * P + 1, j = i + 1;
+        const int idb = a.flags[n + nbr_off<L, j>(o)] & kFlagTypeMask;
+        if (idb >= 2) {
+            const float cu = float(L::cx(i)) * a.wall_u[idb][0] + float(L::cy(i)) * a.wall_u[idb][1] +
+                             float(L::cz(i)) * a.wall_u[idb][2];
+            h[i] += a.scale[i] * (6.0F * float(L::w(i)) * rw * cu);
+        }
+        const int idf = a.flags[n + nbr_off<L, i>(o)] & kFlagTypeMask;
+        if (idf >= 2) {
+            const float cu = float(L::cx(j)) * a.wall_u[idf][0] + float(L::cy(j)) * a.wall_u[idf][1] +
+                             float(L::cz(j)) * a.wall_u[idf][2];
+            h[j] += a.scale[j] * (6.0F * float(L::w(j)) * rw * cu);
+        }
+        moving_wall_pairs_scaled<L, P + 1>(a, n, o, rw, h);
+    }
+}
+
+template <class L>
+__device__ __forceinline__ void gather_fixup_scaled(const LbmArgs& a, u32 n, const Nbr& o, std::uint8_t flag,
+                                                    float* h) {
+    if (flag & kFlagNearMoving) {
+        float rho0 = 1.0F;
+#pragma unroll
+        for (int d = 0; d < L::Q; ++d) rho0 += h[d] * a.inv_scale[d];
+        const float rw = rho0 > 1.0e-8F ? rho0 : 1.0e-8F;
+        moving_wall_pairs_scaled<L>(a, n, o, rw, h);
+    }
 }
 
 template <class L, class S, bool FLAGS>
@@ -186,7 +271,7 @@ __device__ __forceinline__ void gather_fixup(const LbmArgs& a, u32 n, const Nbr&
     using R = typename S::R;
     if constexpr (FLAGS) {
         if (flag & kFlagNearMoving) {
-            R rho0 = R(0);
+            R rho0 = S::delta ? R(1) : R(0);
 #pragma unroll
             for (int d = 0; d < L::Q; ++d) rho0 += fin[d];
             const R rw = rho0 > R(1.0e-8) ? rho0 : R(1.0e-8);
@@ -208,20 +293,20 @@ __device__ __forceinline__ void gather(const LbmArgs& a, u32 n, const Nbr& o, st
 //   even step: f[j][n] = fout_i, f[i][nb] = fout_j
 //   odd step:  f[i][n] = fout_i, f[j][nb] = fout_j
 // i.e. fout_i -> pb[p][n], fout_j -> pa[p][nb].
-template <class L, class S, int P = 0>
+template <class L, class S, bool NARROW, bool RAW = false, int P = 0>
 __device__ __forceinline__ void scatter_pairs(const LbmArgs& a, u32 n, const Nbr& o, const typename S::R* fout) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
-        st<S, L, i>(slot_mut<S>(a.pb, P) + n, fout[i], a);
-        st<S, L, j>(slot_mut<S>(a.pa, P) + (n + nbr_off<L, j>(o)), fout[j], a);
-        scatter_pairs<L, S, P + 1>(a, n, o, fout);
+        st<S, L, i, RAW>(Slots<S, NARROW>::at(a, false, P, n), fout[i], a);
+        st<S, L, j, RAW>(Slots<S, NARROW>::at(a, true, P, n + nbr_off<L, j>(o)), fout[j], a);
+        scatter_pairs<L, S, NARROW, RAW, P + 1>(a, n, o, fout);
     }
 }
 
-template <class L, class S>
+template <class L, class S, bool NARROW = false, bool RAW = false>
 __device__ __forceinline__ void scatter(const LbmArgs& a, u32 n, const Nbr& o, const typename S::R* fout) {
-    st<S, L, 0>(static_cast<typename S::T*>(a.rest) + n, fout[0], a);
-    scatter_pairs<L, S>(a, n, o, fout);
+    st<S, L, 0, RAW>(Slots<S, NARROW>::rest(a, n), fout[0], a);
+    scatter_pairs<L, S, NARROW, RAW>(a, n, o, fout);
 }
 
 // ------------------------------------------------------------------ helpers
@@ -243,7 +328,8 @@ __device__ __forceinline__ void pair_sums(const R* f, R* s, R* d) {
     }
 }
 
-template <class L, class R>
+// DELTA: the values are deviations f - w, whose rest weights sum to 1.
+template <class L, class R, bool DELTA = false>
 __device__ __forceinline__ void pair_moments(R f0, const R* s, const R* d, R& rho, R& jx, R& jy, R& jz) {
     R r = f0, x = R(0), y = R(0), z = R(0);
 #pragma unroll
@@ -257,17 +343,17 @@ __device__ __forceinline__ void pair_moments(R f0, const R* s, const R* d, R& rh
         if (L::cz(i) > 0) z += d[p];
         if (L::cz(i) < 0) z -= d[p];
     }
-    rho = r;
+    rho = DELTA ? R(1) + r : r;
     jx = x;
     jy = y;
     jz = z;
 }
 
-template <class L, class R>
+template <class L, class R, bool DELTA = false>
 __device__ __forceinline__ void moments(const R* fin, R& rho, R& ux, R& uy, R& uz) {
     R s[L::PAIRS], d[L::PAIRS], jx, jy, jz;
     pair_sums<L, R>(fin, s, d);
-    pair_moments<L, R>(fin[0], s, d, rho, jx, jy, jz);
+    pair_moments<L, R, DELTA>(fin[0], s, d, rho, jx, jy, jz);
     // reference esoteric_pull.hpp:397-405: u = 0 when rho <= 0
     const R inv = rho > R(0) ? rcp(rho) : R(0);
     ux = jx * inv;
@@ -292,7 +378,7 @@ template <class R> __device__ __forceinline__ void cell_acceleration(const LbmAr
 // which equals sum c_a c_b (f - feq) on D3Q19/D3Q27 (both lattices are
 // fourth-order isotropic) and needs no per-direction equilibria; c_a c_b is
 // even in c, so the sums run over pair sums s_p.
-template <class L, class R>
+template <class L, class R, bool DELTA = false>
 __device__ __forceinline__ R les_tau(const R* s, R rho, R ux, R uy, R uz, R tau, R k) {
     if (!(rho > R(0))) return tau;
     R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
@@ -310,6 +396,11 @@ __device__ __forceinline__ R les_tau(const R* s, R rho, R ux, R uy, R uz, R tau,
         if (L::cy(i) * L::cz(i) < 0) syz -= s[p];
     }
     const R third = R(1.0 / 3.0);
+    if constexpr (DELTA) { // sum_d c_a c_b w_d = delta_ab / 3
+        sxx += third;
+        syy += third;
+        szz += third;
+    }
     const R pxx = sxx - rho * (third + ux * ux);
     const R pyy = syy - rho * (third + uy * uy);
     const R pzz = szz - rho * (third + uz * uz);
@@ -332,7 +423,9 @@ __device__ __forceinline__ R les_tau(const R* s, R rho, R ux, R uy, R uz, R tau,
 //   f_i' = (s' + d') / 2,  f_j' = (s' - d') / 2
 // Gray-LBM partial bounce-back then mixes in the incoming opposite population:
 // f_i <- (1 - n_s) f_i' + n_s fin_j (Walsh, Burwinkle & Saar 2009).
-template <class L, class R, bool FORCE, bool GRAY, int P = 0>
+// With DELTA the values are deviations f - w: the same update holds with
+// s_eq - 2w in place of s_eq (w_i = w_j within a pair, so d is unchanged).
+template <class L, class R, bool FORCE, bool GRAY, bool DELTA, int P = 0>
 __device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, R rho, R ux, R uy, R uz, R fx, R fy, R fz,
                                               R base, R uf3, R omega, R omega_m, R gp, R gm, R ns) {
     if constexpr (P < L::PAIRS) {
@@ -340,7 +433,7 @@ __device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, R rh
         constexpr R w2 = R(2.0 * L::w(i));
         const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
         const R wr2 = w2 * rho;
-        const R s_eq = wr2 * (base + R(4.5) * cu * cu);
+        const R s_eq = DELTA ? w2 * (rho * (base + R(4.5) * cu * cu) - R(1)) : wr2 * (base + R(4.5) * cu * cu);
         const R d_eq = wr2 * (R(3) * cu);
         R sp = s[P] - omega * (s[P] - s_eq);
         R dp = d[P] - omega_m * (d[P] - d_eq);
@@ -359,17 +452,17 @@ __device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, R rh
         }
         f[i] = oi;
         f[j] = oj;
-        collide_pairs<L, R, FORCE, GRAY, P + 1>(f, s, d, rho, ux, uy, uz, fx, fy, fz, base, uf3, omega, omega_m, gp,
-                                                gm, ns);
+        collide_pairs<L, R, FORCE, GRAY, DELTA, P + 1>(f, s, d, rho, ux, uy, uz, fx, fy, fz, base, uf3, omega, omega_m,
+                                                       gp, gm, ns);
     }
 }
 
-template <class L, class R, bool LES, bool GRAY, bool FORCE>
+template <class L, class R, bool LES, bool GRAY, bool FORCE, bool DELTA = false>
 __device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
     R s[L::PAIRS], d[L::PAIRS];
     pair_sums<L, R>(f, s, d);
     R rho, jx, jy, jz;
-    pair_moments<L, R>(f[0], s, d, rho, jx, jy, jz);
+    pair_moments<L, R, DELTA>(f[0], s, d, rho, jx, jy, jz);
     const R inv = rho > R(0) ? rcp(rho) : R(0);
     R ux = jx * inv, uy = jy * inv, uz = jz * inv;
     R ax = R(0), ay = R(0), az = R(0);
@@ -380,7 +473,7 @@ __device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
         uz += R(0.5) * az;
     }
     R tau = R(a.tau);
-    if constexpr (LES) tau = les_tau<L, R>(s, rho, ux, uy, uz, tau, R(a.les_k));
+    if constexpr (LES) tau = les_tau<L, R, DELTA>(s, rho, ux, uy, uz, tau, R(a.les_k));
     const R omega = rcp(tau);
     R omega_m;
     if (a.omega_minus > 0.0) {
@@ -407,24 +500,177 @@ __device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
     {
         constexpr R w0 = R(L::w(0));
         const R f0 = f[0];
-        R o0 = f0 - omega * (f0 - w0 * rho * base);
+        R o0 = f0 - omega * (f0 - (DELTA ? w0 * (rho * base - R(1)) : w0 * rho * base));
         if constexpr (FORCE) o0 -= gp * w0 * uf3;
         if constexpr (GRAY) o0 = (R(1) - ns) * o0 + ns * f0;
         f[0] = o0;
     }
-    collide_pairs<L, R, FORCE, GRAY>(f, s, d, rho, ux, uy, uz, fx, fy, fz, base, uf3, omega, omega_m, gp, gm, ns);
+    collide_pairs<L, R, FORCE, GRAY, DELTA>(f, s, d, rho, ux, uy, uz, fx, fy, fz, base, uf3, omega, omega_m, gp, gm,
+                                            ns);
+}
+
+// --------------------------------------------------- FP16 scaled collision
+// The same TRT/Guo/gray update as collide, for values held in FP16 storage
+// units h = (f - w) s_k, with s_k constant within each weight class k.
+// Pair sums stay in storage units: the moments scale each class's partial
+// sums once, and the scales are folded into the relaxation coefficients, so
+// decoding and encoding cost only the half <-> float conversions:
+//   h_i' = [a1 sh + A2_k s_eq + G1_k s_F] + [b1 dh + B2_k d_eq + G2_k d_F]
+//   h_j' = [ ...same... ]               - [ ...same... ]
+// with a1 = (1 - omega+)/2, A2_k = omega+ s_k / 2, G1_k = (1 - omega+/2) s_k / 2,
+// b1 = (1 - omega-)/2, B2_k = omega- s_k / 2, G2_k = (1 - omega-/2) s_k / 2,
+// s_eq = 2 w (rho (1 - 1.5 u^2 + 4.5 (c.u)^2) - 1) and d_eq = 6 w rho (c.u)
+// the deviation-space equilibria.
+template <class L, bool FORCE, bool GRAY, int P = 0>
+__device__ __forceinline__ void collide_pairs_scaled(const LbmArgs& a, float* h, const float* sh, const float* dh,
+                                                     float rho, float ux, float uy, float uz, float fx, float fy,
+                                                     float fz, float base, float uf3, float a1, float b1, float omega,
+                                                     float omega_m, float gp, float gm, float ns) {
+    if constexpr (P < L::PAIRS) {
+        constexpr int i = 2 * P + 1, j = i + 1;
+        constexpr float w2 = float(2.0 * L::w(i));
+        const float sk = a.scale[class_rep(weight_class<L>(i))];
+        const float cu = float(L::cx(i)) * ux + float(L::cy(i)) * uy + float(L::cz(i)) * uz;
+        const float s_eq = w2 * (rho * (base + 4.5F * cu * cu) - 1.0F);
+        const float d_eq = (3.0F * w2) * rho * cu;
+        float sp = a1 * sh[P] + (0.5F * omega * sk) * s_eq;
+        float dp = b1 * dh[P] + (0.5F * omega_m * sk) * d_eq;
+        if constexpr (FORCE) {
+            const float cf = float(L::cx(i)) * fx + float(L::cy(i)) * fy + float(L::cz(i)) * fz;
+            sp += (0.5F * gp * sk) * (w2 * (9.0F * cu * cf - uf3));
+            dp += (0.5F * gm * sk) * (w2 * (3.0F * cf));
+        }
+        float oi = sp + dp;
+        float oj = sp - dp;
+        if constexpr (GRAY) {
+            const float hi = 0.5F * (sh[P] + dh[P]);
+            const float hj = 0.5F * (sh[P] - dh[P]);
+            oi = (1.0F - ns) * oi + ns * hj;
+            oj = (1.0F - ns) * oj + ns * hi;
+        }
+        h[i] = oi;
+        h[j] = oj;
+        collide_pairs_scaled<L, FORCE, GRAY, P + 1>(a, h, sh, dh, rho, ux, uy, uz, fx, fy, fz, base, uf3, a1, b1,
+                                                    omega, omega_m, gp, gm, ns);
+    }
+}
+
+template <class L, bool LES, bool GRAY, bool FORCE>
+__device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, float* h) {
+    float sh[L::PAIRS], dh[L::PAIRS];
+    pair_sums<L, float>(h, sh, dh);
+    // Per weight class partial sums (classes 1..3), scaled once each.
+    float S[4] = {0, 0, 0, 0}, JX[4] = {0, 0, 0, 0}, JY[4] = {0, 0, 0, 0}, JZ[4] = {0, 0, 0, 0};
+    float XX[4] = {0, 0, 0, 0}, YY[4] = {0, 0, 0, 0}, ZZ[4] = {0, 0, 0, 0};
+    float XY[4] = {0, 0, 0, 0}, XZ[4] = {0, 0, 0, 0}, YZ[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int p = 0; p < L::PAIRS; ++p) {
+        const int i = 2 * p + 1;
+        const int k = weight_class<L>(i);
+        S[k] += sh[p];
+        if (L::cx(i) > 0) JX[k] += dh[p];
+        if (L::cx(i) < 0) JX[k] -= dh[p];
+        if (L::cy(i) > 0) JY[k] += dh[p];
+        if (L::cy(i) < 0) JY[k] -= dh[p];
+        if (L::cz(i) > 0) JZ[k] += dh[p];
+        if (L::cz(i) < 0) JZ[k] -= dh[p];
+        if constexpr (LES) {
+            if (L::cx(i) != 0) XX[k] += sh[p];
+            if (L::cy(i) != 0) YY[k] += sh[p];
+            if (L::cz(i) != 0) ZZ[k] += sh[p];
+            if (L::cx(i) * L::cy(i) > 0) XY[k] += sh[p];
+            if (L::cx(i) * L::cy(i) < 0) XY[k] -= sh[p];
+            if (L::cx(i) * L::cz(i) > 0) XZ[k] += sh[p];
+            if (L::cx(i) * L::cz(i) < 0) XZ[k] -= sh[p];
+            if (L::cy(i) * L::cz(i) > 0) YZ[k] += sh[p];
+            if (L::cy(i) * L::cz(i) < 0) YZ[k] -= sh[p];
+        }
+    }
+    constexpr int K = L::Q == 27 ? 3 : 2;
+    float inv[4];
+#pragma unroll
+    for (int k = 0; k <= K; ++k) inv[k] = a.inv_scale[class_rep(k)];
+    float rho = h[0] * inv[0], jx = 0.0F, jy = 0.0F, jz = 0.0F;
+#pragma unroll
+    for (int k = 1; k <= K; ++k) {
+        rho += S[k] * inv[k];
+        jx += JX[k] * inv[k];
+        jy += JY[k] * inv[k];
+        jz += JZ[k] * inv[k];
+    }
+    rho += 1.0F;
+    const float irho = rho > 0.0F ? rcp(rho) : 0.0F;
+    float ux = jx * irho, uy = jy * irho, uz = jz * irho;
+    float ax = 0.0F, ay = 0.0F, az = 0.0F;
+    if constexpr (FORCE) {
+        cell_acceleration<float>(a, n, ax, ay, az);
+        ux += 0.5F * ax;
+        uy += 0.5F * ay;
+        uz += 0.5F * az;
+    }
+    float tau = float(a.tau);
+    if constexpr (LES) {
+        if (rho > 0.0F) {
+            const float third = 1.0F / 3.0F;
+            float sxx = third, syy = third, szz = third, sxy = 0.0F, sxz = 0.0F, syz = 0.0F;
+#pragma unroll
+            for (int k = 1; k <= K; ++k) {
+                sxx += XX[k] * inv[k];
+                syy += YY[k] * inv[k];
+                szz += ZZ[k] * inv[k];
+                sxy += XY[k] * inv[k];
+                sxz += XZ[k] * inv[k];
+                syz += YZ[k] * inv[k];
+            }
+            const float pxx = sxx - rho * (third + ux * ux);
+            const float pyy = syy - rho * (third + uy * uy);
+            const float pzz = szz - rho * (third + uz * uz);
+            const float pxy = sxy - rho * ux * uy;
+            const float pxz = sxz - rho * ux * uz;
+            const float pyz = syz - rho * uy * uz;
+            const float q = pxx * pxx + pyy * pyy + pzz * pzz + 2.0F * (pxy * pxy + pxz * pxz + pyz * pyz);
+            tau = 0.5F * (tau + sqrtf(tau * tau + float(a.les_k) * sqrtf(q) * irho));
+        }
+    }
+    const float omega = rcp(tau);
+    float omega_m;
+    if (a.omega_minus > 0.0) {
+        omega_m = float(a.omega_minus);
+    } else if (a.omega_minus < 0.0) {
+        omega_m = omega;
+    } else {
+        const float sp = tau - 0.5F;
+        omega_m = sp * rcp(float(a.trt_magic) + 0.5F * sp);
+    }
+    const float base = 1.0F - 1.5F * (ux * ux + uy * uy + uz * uz);
+    float fx = 0.0F, fy = 0.0F, fz = 0.0F, uf3 = 0.0F;
+    if constexpr (FORCE) {
+        fx = rho * ax;
+        fy = rho * ay;
+        fz = rho * az;
+        uf3 = 3.0F * (ux * fx + uy * fy + uz * fz);
+    }
+    const float gp = 1.0F - 0.5F * omega;
+    const float gm = 1.0F - 0.5F * omega_m;
+    float ns = 0.0F;
+    if constexpr (GRAY) ns = a.ns[n];
+    {
+        constexpr float w0 = float(L::w(0));
+        const float h0 = h[0];
+        float o0 = (1.0F - omega) * h0 + a.scale[0] * (omega * w0 * (rho * base - 1.0F));
+        if constexpr (FORCE) o0 -= a.scale[0] * (gp * w0 * uf3);
+        if constexpr (GRAY) o0 = (1.0F - ns) * o0 + ns * h0;
+        h[0] = o0;
+    }
+    collide_pairs_scaled<L, FORCE, GRAY>(a, h, sh, dh, rho, ux, uy, uz, fx, fy, fz, base, uf3, 0.5F * (1.0F - omega),
+                                         0.5F * (1.0F - omega_m), omega, omega_m, gp, gm, ns);
 }
 
 // ---------------------------------------------------------------- the step
-// Cells per thread (stacked in z) of the step kernel: the loads of all of a
-// thread's cells are in flight together.  One cell per thread measured best
-// on B200 for every storage type (more cells cost occupancy through
-// registers); two stay selectable for tuning.
-template <class S> struct StepCells {
-    static constexpr int value = 1;
-};
-
-template <class L, class S, bool LES, bool FLAGS, bool GRAY, int CPT>
+// CPT cells per thread (stacked in z): the loads of all of a thread's cells are
+// issued before the first collision.  One cell per thread measured best on
+// B200 (more cells cost occupancy through registers), and the launcher uses 1.
+template <class L, class S, bool LES, bool FLAGS, bool GRAY, int CPT, bool NARROW>
 __global__ void __launch_bounds__(128) k_step(const __grid_constant__ LbmArgs a) {
     using R = typename S::R;
     const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -446,7 +692,7 @@ __global__ void __launch_bounds__(128) k_step(const __grid_constant__ LbmArgs a)
                 live[c] = (flag[c] & kFlagTypeMask) == 0; // walls hold no populations of their own
             }
         }
-        if (live[c]) gather_loads<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag[c], fin[c]);
+        if (live[c]) gather_loads<L, S, FLAGS, NARROW, S::scaled>(a, n, make_nbr(a, x, y, z), flag[c], fin[c]);
     }
     const bool force = a.has_force != 0;
 #pragma unroll
@@ -455,12 +701,20 @@ __global__ void __launch_bounds__(128) k_step(const __grid_constant__ LbmArgs a)
         const u32 z = z0 + c;
         const u32 n = (z * a.ny + y) * a.nx + x;
         const Nbr o = make_nbr(a, x, y, z);
-        gather_fixup<L, S, FLAGS>(a, n, o, flag[c], fin[c]);
-        if (force)
-            collide<L, R, LES, GRAY, true>(a, n, fin[c]);
-        else
-            collide<L, R, LES, GRAY, false>(a, n, fin[c]);
-        scatter<L, S>(a, n, o, fin[c]);
+        if constexpr (S::scaled) {
+            if constexpr (FLAGS) gather_fixup_scaled<L>(a, n, o, flag[c], fin[c]);
+            if (force)
+                collide_scaled<L, LES, GRAY, true>(a, n, fin[c]);
+            else
+                collide_scaled<L, LES, GRAY, false>(a, n, fin[c]);
+        } else {
+            gather_fixup<L, S, FLAGS>(a, n, o, flag[c], fin[c]);
+            if (force)
+                collide<L, R, LES, GRAY, true, S::delta>(a, n, fin[c]);
+            else
+                collide<L, R, LES, GRAY, false, S::delta>(a, n, fin[c]);
+        }
+        scatter<L, S, NARROW, S::scaled>(a, n, o, fin[c]);
     }
 }
 
@@ -481,11 +735,12 @@ __device__ __forceinline__ void init_pairs(const LbmArgs& a, u32 n, const Nbr& o
         const R fi = wr * (R(1) + R(3) * cu + R(4.5) * cu * cu - usq15);
         const R fj = wr * (R(1) - R(3) * cu + R(4.5) * cu * cu - usq15);
         const u32 nb = n + nbr_off<L, j>(o);
-        st<S, L, i>(static_cast<typename S::T*>(a.fd[i]) + nb, fi, a);
-        st<S, L, j>(static_cast<typename S::T*>(a.fd[j]) + n, fj, a);
+        const R hi = held<S, L, i>(fi), hj = held<S, L, j>(fj);
+        st<S, L, i>(static_cast<typename S::T*>(a.fd[i]) + nb, hi, a);
+        st<S, L, j>(static_cast<typename S::T*>(a.fd[j]) + n, hj, a);
         if constexpr (FLAGS) {
-            if ((walls >> (2 * P)) & 1U) st<S, L, j>(static_cast<typename S::T*>(a.fd[j]) + nb, fi, a);
-            if ((walls >> (2 * P + 1)) & 1U) st<S, L, i>(static_cast<typename S::T*>(a.fd[i]) + n, fj, a);
+            if ((walls >> (2 * P)) & 1U) st<S, L, j>(static_cast<typename S::T*>(a.fd[j]) + nb, hi, a);
+            if ((walls >> (2 * P + 1)) & 1U) st<S, L, i>(static_cast<typename S::T*>(a.fd[i]) + n, hj, a);
         }
         init_pairs<L, S, FLAGS, P + 1>(a, n, o, walls, rho, ux, uy, uz, usq15);
     }
@@ -534,7 +789,7 @@ __global__ void __launch_bounds__(128) k_init(const __grid_constant__ LbmArgs a,
         uz = R(s.fields[3 * std::size_t(a.N) + n]);
     }
     const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
-    st<S, L, 0>(static_cast<typename S::T*>(a.fd[0]) + n, R(L::w(0)) * rho * (R(1) - usq15), a);
+    st<S, L, 0>(static_cast<typename S::T*>(a.fd[0]) + n, held<S, L, 0>(R(L::w(0)) * rho * (R(1) - usq15)), a);
     init_pairs<L, S, FLAGS>(a, n, o, walls, rho, ux, uy, uz, usq15);
 }
 
@@ -563,7 +818,7 @@ __global__ void __launch_bounds__(128) k_macro(const __grid_constant__ LbmArgs a
     R fin[L::Q];
     gather<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag, fin);
     R rho, ux, uy, uz, ax, ay, az;
-    moments<L, R>(fin, rho, ux, uy, uz);
+    moments<L, R, S::delta>(fin, rho, ux, uy, uz);
     cell_acceleration<R>(a, n, ax, ay, az);
     rho_out[n] = OutT(rho);
     ux_out[n] = OutT(ux + R(0.5) * ax);
@@ -589,7 +844,8 @@ __global__ void __launch_bounds__(128) k_logical(const __grid_constant__ LbmArgs
     }
     if (!wall) gather<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag, fin);
 #pragma unroll
-    for (int d = 0; d < L::Q; ++d) out[static_cast<std::size_t>(d) * a.N + n] = wall ? OutT(0) : OutT(fin[d]);
+    for (int d = 0; d < L::Q; ++d)
+        out[static_cast<std::size_t>(d) * a.N + n] = wall ? OutT(0) : OutT(absolute<S, L>(fin[d], d));
 }
 
 // Fluid-cell reduction with FP64 accumulation (reference
@@ -646,7 +902,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_reduce(const __grid_constant
             R fin[L::Q];
             gather<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag, fin);
             R rho, ux, uy, uz, ax, ay, az;
-            moments<L, R>(fin, rho, ux, uy, uz);
+            moments<L, R, S::delta>(fin, rho, ux, uy, uz);
             cell_acceleration<R>(a, n, ax, ay, az);
             ux += R(0.5) * ax;
             uy += R(0.5) * ay;

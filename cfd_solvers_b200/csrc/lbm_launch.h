@@ -23,7 +23,9 @@ struct KernelKey {
     bool les;
     bool flags;
     bool gray;
-    int cells_per_thread; // step kernel; 0 = default for the storage type
+    int cells_per_thread; // reserved (one cell per thread)
+    bool paired;          // use the paired-cell step kernel (two adjacent x cells per thread)
+    bool narrow;          // 32-bit slot offsets (q * cells < 2^32)
 };
 
 dim3 cell_block(long long nx, long long ny, const LaunchShape& s);

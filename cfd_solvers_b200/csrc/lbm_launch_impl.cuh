@@ -4,6 +4,7 @@
 
 #include "lbm_device.cuh"
 #include "lbm_launch.h"
+#include "lbm_step_x2.cuh"
 
 namespace cfdx {
 
@@ -24,26 +25,35 @@ template <class F> cudaError_t with_lattice(int q, F&& f) {
     return cudaErrorInvalidValue;
 }
 
-// Cells per thread of the step kernel: 0 = the storage type's default.
+// One-cell step kernel; NARROW (32-bit slot offsets) whenever q*N < 2^32.
 template <class L, class S, bool LES, bool FL, bool GR>
-cudaError_t step_cpt(int cpt, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    if (cpt <= 0) cpt = StepCells<S>::value;
-    auto go = [&](auto kernel, unsigned c) {
-        dim3 gz(g.x, g.y, (a.nz + c - 1U) / c);
-        kernel<<<gz, b, 0, s>>>(a);
+cudaError_t step_single(bool narrow, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    if (narrow)
+        k_step<L, S, LES, FL, GR, 1, true><<<g, b, 0, s>>>(a);
+    else
+        k_step<L, S, LES, FL, GR, 1, false><<<g, b, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Paired-cell kernel (FP32 / FP16 storage): a thread owns x0 = 2t and x0 + 1.
+template <class L, class S, bool LES, bool FL, bool GR>
+cudaError_t step_paired(const LbmArgs& a, dim3 b, cudaStream_t s) {
+    if constexpr (sizeof(typename S::T) == 8) {
+        return cudaErrorInvalidValue;
+    } else {
+        const unsigned pairs = (a.nx + 1U) / 2U;
+        dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, a.nz);
+        k_step_x2<L, S, LES, FL, GR><<<g, b, 0, s>>>(a);
         return cudaGetLastError();
-    };
-    switch (cpt) {
-    case 1: return go(k_step<L, S, LES, FL, GR, 1>, 1U);
-    case 2: return go(k_step<L, S, LES, FL, GR, 2>, 2U);
-    default: return cudaErrorInvalidValue;
     }
 }
 
 template <class L, class S, bool LES, bool FL>
 cudaError_t step_gray(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    return k.gray ? step_cpt<L, S, LES, FL, true>(k.cells_per_thread, a, g, b, s)
-                  : step_cpt<L, S, LES, FL, false>(k.cells_per_thread, a, g, b, s);
+    if (k.paired)
+        return k.gray ? step_paired<L, S, LES, FL, true>(a, b, s) : step_paired<L, S, LES, FL, false>(a, b, s);
+    return k.gray ? step_single<L, S, LES, FL, true>(k.narrow, a, g, b, s)
+                  : step_single<L, S, LES, FL, false>(k.narrow, a, g, b, s);
 }
 
 template <class L, class S, bool LES>

@@ -355,9 +355,9 @@ class EsotericPullCudaSolver:
         s = _host(scale, np.float32, self._q, "storage scale")
         self._call("cfdx_lbm_set_storage_scale", ctypes.c_void_p(s.ctypes.data))
 
-    def set_launch_shape(self, block_x: int = 0, block_y: int = 0, cells_per_thread: int = 0):
-        """Threads per block and cells per thread of the step kernel (zeros: defaults)."""
-        self._call("cfdx_lbm_set_launch_shape", int(block_x), int(block_y), int(cells_per_thread))
+    def set_launch_shape(self, block_x: int = 0, block_y: int = 0, variant: int = 0):
+        """Threads per block and step-kernel variant (0 auto, 1 one cell, 2 paired cells)."""
+        self._call("cfdx_lbm_set_launch_shape", int(block_x), int(block_y), int(variant))
 
     def stream(self) -> int:
         p = ctypes.c_void_p()

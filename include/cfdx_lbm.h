@@ -168,8 +168,8 @@ CFDX_API int cfdx_lbm_device_local_acceleration(cfdx_lbm* lbm, float** accel);
  * No reference counterpart (Walsh, Burwinkle & Saar 2009). */
 CFDX_API int cfdx_lbm_set_solid_fraction(cfdx_lbm* lbm, const float* ns, int where);
 
-/* FP16S only: q per-direction scales s_d (opposite directions must share a
- * scale); NULL restores the default power-of-two scales near 1/w_d.
+/* FP16S only: q per-direction scales s_d (directions of equal lattice weight
+ * must share a scale); NULL restores the default power-of-two scales near 1/w_d.
  * Reference codec: ShiftedHalfCodec (s_d = 1), compressed_pull.hpp:71-79. */
 CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* lbm, const float* scale);
 
@@ -218,10 +218,11 @@ CFDX_API int cfdx_lbm_stream(cfdx_lbm* lbm, void** stream);
  * Reference: raw_storage, esoteric_pull.hpp:276-278. */
 CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* lbm, void** device_ptr, size_t* bytes);
 
-/* Launch shape of the cell kernels: threads per block (x, y) and cells per
- * thread of the step kernel (1 or 2, stacked in z); zeros restore the
- * defaults. */
-CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, int cells_per_thread);
+/* Launch shape of the cell kernels: threads per block (x, y) and the step
+ * kernel variant: 0 automatic (paired cells where eligible), 1 one cell per
+ * thread, 2 two adjacent x cells per thread (FP32/FP16 storage, even nx).
+ * Zeros restore the defaults. */
+CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, int variant);
 
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
