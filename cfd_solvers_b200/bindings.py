@@ -130,6 +130,7 @@ SIGNATURES = {
     "cfdx_lbm_stream": (_i, [_H, ctypes.POINTER(_vp)]),
     "cfdx_lbm_raw_populations": (_i, [_H, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
     "cfdx_lbm_set_launch_shape": (_i, [_H, _i, _i, _i]),
+    "cfdx_lbm_reduce_noalloc": (_i, [_H, ctypes.POINTER(ctypes.c_double)]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

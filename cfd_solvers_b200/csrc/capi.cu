@@ -19,6 +19,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "handle_access.h"
 #include "lbm_launch.h"
 
 namespace {
@@ -378,6 +379,28 @@ cudaError_t launch_reduce(const KernelKey& k, const LbmArgs& a, double* partials
     }
 }
 
+
+int handle_reduce_view(cfdx_lbm* h, ReduceView* view) {
+    return guarded([&] {
+        checked(h);
+        require(view != nullptr, "null view");
+        view->key = h->key;
+        view->args = h->args();
+        view->stream = h->stream;
+        view->device = h->cfg.device;
+    });
+}
+
+int record_error(int status, const char* message) {
+    g_error = message ? message : "";
+    g_error_status = status;
+    return status;
+}
+
+void record_download(cfdx_lbm* h, std::uint64_t bytes) {
+    h->d2h += bytes;
+    ++h->syncs;
+}
 
 } // namespace cfdx
 

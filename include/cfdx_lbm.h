@@ -224,6 +224,23 @@ CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* lbm, void** device_ptr, size_t* 
  * Zeros restore the defaults. */
 CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, int variant);
 
+/* The reduction of cfdx_lbm_reduce() without any allocation: no
+ * cudaMalloc, cudaFree or other allocating routine, for callers that cannot
+ * allocate at this point -- a process whose device memory is held by another
+ * allocator, a monitoring loop that must not take the device-wide
+ * synchronisation of cudaMalloc/cudaFree, or an FFI caller with no CUDA
+ * allocation API of its own.  No counterpart in the reference.
+ * `out` is host memory for CFDX_REDUCE_COUNT doubles, same layout and status
+ * codes as cfdx_lbm_reduce().  Scratch is a fixed static device array
+ * (229,432 bytes on every GPU that loads the library, held until exit) with
+ * partial sums for nz reduction blocks: lattices with nz > 4096 are rejected
+ * with CFDX_ERR_INVALID.  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the array: calls whose work overlaps on
+ * the GPU (different handles' streams, or threads) race and must be
+ * serialised by the caller. */
+CFDX_API int cfdx_lbm_reduce_noalloc(cfdx_lbm* lbm, double* out);
+
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */
