@@ -126,8 +126,6 @@ struct cfdx_lbm {
     float* local_a = nullptr;
     float* ns = nullptr;
     float* macro_scratch = nullptr; // 4*N floats, lazily allocated
-    int* status = nullptr;          // kernel error word
-    unsigned row_grid = 0;          // CTAs of the row-staged step kernel
     double* reduce_partials = nullptr;
     double* reduce_out = nullptr;
     double* host_reduce = nullptr; // pinned
@@ -138,9 +136,11 @@ struct cfdx_lbm {
     float scale[27]{};
     LaunchShape shape{};
     int variant = 0; // step kernel: 0 auto, 1 one cell per thread, 2 paired cells
-    // Automatic choice: the one-cell kernel measured faster on B200 for every
-    // configuration benchmarked, so auto selects it.
-    static constexpr bool paired_default = false;
+    // Automatic choice between the one-cell and the paired-cell kernel, from
+    // B200 measurements at 512^3: pairs win for D3Q19 FP16 storage (2-7%),
+    // lose for FP32 storage and for D3Q27 (the 26 neighbour words of a pair
+    // need more shuffles and registers than the kernel can hold).
+    static bool paired_default(int storage, int q) { return storage == kStoreF16S && q == 19; }
     double les_k = 0.0;
     std::uint64_t h2d = 0, d2h = 0, syncs = 0;
 
@@ -158,7 +158,6 @@ struct cfdx_lbm {
         a.ay_field = local_a ? local_a + N : nullptr;
         a.az_field = local_a ? local_a + 2 * N : nullptr;
         a.ns = key.gray ? ns : nullptr;
-        a.status = status;
         a.nx = static_cast<std::uint32_t>(cfg.nx);
         a.ny = static_cast<std::uint32_t>(cfg.ny);
         a.nz = static_cast<std::uint32_t>(cfg.nz);
@@ -209,42 +208,10 @@ struct cfdx_lbm {
                static_cast<unsigned long long>(key.q) * N < (1ULL << 32) &&
                (shape.block_x == 0 || shape.block_x % 32 == 0);
     }
-    // The row-staged kernel needs 16-byte rows (nx a multiple of 16), 32-bit
-    // slot offsets and at least two stages in shared memory.  Fills the
-    // pipeline shape into key; returns false when the lattice does not fit.
-    bool rows_config() {
-        key.row_stages = 0;
-        if (!key.narrow || cfg.nx % 16U != 0U || cfg.nx > 4096U) return false;
-        const std::size_t es = static_cast<std::size_t>(storage_bytes(key.storage));
-        const std::size_t stage = ((static_cast<std::size_t>(key.q) * cfg.nx * es + cfg.nx + 127U) / 128U) * 128U;
-        std::size_t depth = (113U * 1024U - 128U) / stage; // two CTAs per SM
-        if (depth < 2U) depth = (227U * 1024U - 128U) / stage;  // one CTA per SM
-        if (depth < 2U) return false;
-        key.row_stages = static_cast<unsigned>(std::min<std::size_t>(depth, 4U));
-        key.row_stage_bytes = static_cast<unsigned>(stage);
-        key.row_threads = static_cast<unsigned>(std::min<std::size_t>(512U, ((cfg.nx + 31U) / 32U) * 32U));
-        return true;
-    }
     void choose_variant() {
         key.narrow = static_cast<unsigned long long>(key.q) * N < (1ULL << 32);
-        key.paired = variant == 2 || (variant == 0 && paired_default && paired_eligible());
-        key.rows = false;
-        const bool rows_ok = rows_config();
-        if (variant == 3 || (variant == 0 && rows_ok && rows_default(key.storage))) {
-            if (!rows_ok) throw std::invalid_argument("the row-staged kernel needs nx a multiple of 16 (<= 4096) and "
-                                                      "q*cells < 2^32");
-            key.rows = true;
-            key.paired = false;
-            int sms = 0;
-            check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg.device), "device attribute");
-            const int per_sm = row_kernel_ctas_per_sm(key);
-            if (per_sm < 1) throw std::invalid_argument("the row-staged kernel does not fit on this device");
-            const unsigned long long rows = static_cast<unsigned long long>(cfg.ny) * cfg.nz;
-            row_grid = static_cast<unsigned>(std::min<unsigned long long>(rows, 1ULL * per_sm * sms));
-        }
+        key.paired = variant == 2 || (variant == 0 && paired_eligible() && paired_default(key.storage, key.q));
     }
-    // Automatic choice of the row-staged kernel per storage type.
-    static bool rows_default(int storage) { return storage == kStoreF16S; }
     dim3 step_block() const {
         if (!key.paired) return block();
         int bx = shape.block_x, by = shape.block_y;
@@ -320,14 +287,6 @@ void init_state(cfdx_lbm* h, const InitSpec& spec) {
     h->t = 0;
 }
 
-// Reads the kernel error word (set only when a bounded wait in a step kernel
-// ran out); the stream must be synchronised.
-void check_status(cfdx_lbm* h) {
-    int st = 0;
-    check_cuda(cudaMemcpy(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy (status)");
-    if (st != 0) fail(CFDX_ERR_CUDA, "a step kernel's bounded wait ran out (row staging pipeline); results are invalid");
-}
-
 void ensure_reduce(cfdx_lbm* h) {
     if (h->reduce_partials) return;
     int sms = 0;
@@ -349,7 +308,6 @@ void release(cfdx_lbm* h) {
     device_free(h->local_a);
     device_free(h->ns);
     device_free(h->macro_scratch);
-    device_free(h->status);
     device_free(h->reduce_partials);
     device_free(h->reduce_out);
     if (h->host_reduce) cudaFreeHost(h->host_reduce);
@@ -382,15 +340,6 @@ cudaError_t launch_step(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cu
     case kStoreF64: return Launcher<kStoreF64>::step(k, a, g, b, s);
     case kStoreF16S: return Launcher<kStoreF16S>::step(k, a, g, b, s);
     default: return cudaErrorInvalidValue;
-    }
-}
-
-int row_kernel_ctas_per_sm(const KernelKey& k) {
-    switch (k.storage) {
-    case kStoreF32: return Launcher<kStoreF32>::row_ctas(k);
-    case kStoreF64: return Launcher<kStoreF64>::row_ctas(k);
-    case kStoreF16S: return Launcher<kStoreF16S>::row_ctas(k);
-    default: return 0;
     }
 }
 
@@ -511,8 +460,7 @@ CFDX_API int cfdx_lbm_create(const cfdx_lbm_config* config, cfdx_lbm** out, char
         h->set_device();
         h->N = c.nx * c.ny * c.nz;
         require(h->N <= 0xffffffffULL, "lattice exceeds 2^32 - 1 cells");
-        h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false, 0, false, false,
-                           false, 0U, 0U, 0U};
+        h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false, 0, false, false};
         h->choose_variant();
         h->les_k = c.smagorinsky_les ? (c.smagorinsky_cs > 0.0F
                                             ? 18.0 * std::sqrt(2.0) * double(c.smagorinsky_cs) * double(c.smagorinsky_cs)
@@ -522,8 +470,6 @@ CFDX_API int cfdx_lbm_create(const cfdx_lbm_config* config, cfdx_lbm** out, char
         check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         h->f_bytes = static_cast<std::size_t>(c.lattice) * h->N * static_cast<std::size_t>(storage_bytes(c.storage));
         h->f = device_alloc(h->f_bytes, "population lattice");
-        h->status = static_cast<int*>(device_alloc(sizeof(int), "status word"));
-        check_cuda(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream), "cudaMemsetAsync");
         InitSpec spec{};
         spec.kind = 0;
         spec.rho = 1.0F;
@@ -693,7 +639,7 @@ CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* h, const float* scale) {
 CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
     return guarded([&] {
         checked(h);
-        const dim3 g = h->key.rows ? dim3(h->row_grid, 1U, 1U) : h->grid(), b = h->step_block();
+        const dim3 g = h->grid(), b = h->step_block();
         LbmArgs a = h->args();
         for (std::uint64_t i = 0; i < count; ++i) {
             h->set_parity(a, static_cast<int>(h->t & 1U));
@@ -707,7 +653,6 @@ CFDX_API int cfdx_lbm_synchronize(cfdx_lbm* h) {
     return guarded([&] {
         checked(h);
         h->sync();
-        check_status(h);
     });
 }
 
@@ -799,7 +744,6 @@ CFDX_API int cfdx_lbm_reduce(cfdx_lbm* h, double* out) {
                    "cudaMemcpyAsync (reduction)");
         h->d2h += sizeof(double) * kReduceFields;
         h->sync();
-        check_status(h);
         for (int k = 0; k < kReduceFields; ++k) out[k] = h->host_reduce[k];
         out[CFDX_REDUCE_KINETIC_ENERGY] *= 0.5;
         nonfinite = out[CFDX_REDUCE_NONFINITE] > 0.0;
@@ -888,8 +832,7 @@ CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* h, void** ptr, std::size_t* byte
 CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int variant) {
     return guarded([&] {
         checked(h);
-        require(variant >= 0 && variant <= 3,
-                "step kernel variant must be 0 (auto), 1 (one cell), 2 (paired) or 3 (row-staged)");
+        require(variant >= 0 && variant <= 2, "step kernel variant must be 0 (auto), 1 (one cell) or 2 (paired)");
         if (bx == 0 && by == 0) {
             h->shape = LaunchShape{};
         } else {

@@ -49,7 +49,6 @@ struct LbmArgs {
     const float* ay_field;
     const float* az_field;
     const float* ns;           // N gray-LBM solid fractions or nullptr
-    int* status;               // kernel error word (0 = ok), checked by the host
     std::uint32_t nx, ny, nz;
     std::uint32_t N;
     int odd;                   // parity of the time step being executed / read

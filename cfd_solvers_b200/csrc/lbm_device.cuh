@@ -310,9 +310,19 @@ __device__ __forceinline__ void scatter(const LbmArgs& a, u32 n, const Nbr& o, c
 }
 
 // ------------------------------------------------------------------ helpers
-// Reciprocal: the FP32 path uses the hardware approximation (__fdividef,
-// ~2 ulp), well inside the FP32 parity tolerance; FP64 stays IEEE.
+// Reciprocals.  rcp: the hardware approximation (__fdividef, within 2 ulp),
+// for relaxation rates, which enter a cell's mass and momentum alike.
+// rcp_unbiased, for 1/rho in u = j / rho: the collision returns the momentum
+// rho u, so an error in 1/rho that leans one way (an approximation's does)
+// moves every cell's momentum the same way each step.  One Newton-Raphson step
+// r + r (1 - x r) on the approximation leaves a symmetric error of about half
+// an ulp at the cost of two fused multiply-adds.
 __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0F, x); }
+__device__ __forceinline__ float rcp_unbiased(float x) {
+    const float r = __fdividef(1.0F, x);
+    return fmaf(r, fmaf(-x, r, 1.0F), r);
+}
+__device__ __forceinline__ double rcp_unbiased(double x) { return 1.0 / x; }
 __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
 
 // ---------------------------------------------------------------- moments
@@ -355,7 +365,7 @@ __device__ __forceinline__ void moments(const R* fin, R& rho, R& ux, R& uy, R& u
     pair_sums<L, R>(fin, s, d);
     pair_moments<L, R, DELTA>(fin[0], s, d, rho, jx, jy, jz);
     // reference esoteric_pull.hpp:397-405: u = 0 when rho <= 0
-    const R inv = rho > R(0) ? rcp(rho) : R(0);
+    const R inv = rho > R(0) ? rcp_unbiased(rho) : R(0);
     ux = jx * inv;
     uy = jy * inv;
     uz = jz * inv;
@@ -379,7 +389,7 @@ template <class R> __device__ __forceinline__ void cell_acceleration(const LbmAr
 // fourth-order isotropic) and needs no per-direction equilibria; c_a c_b is
 // even in c, so the sums run over pair sums s_p.
 template <class L, class R, bool DELTA = false>
-__device__ __forceinline__ R les_tau(const R* s, R rho, R ux, R uy, R uz, R tau, R k) {
+__device__ __forceinline__ R les_tau(const R* s, R rho, R irho, R ux, R uy, R uz, R tau, R k) {
     if (!(rho > R(0))) return tau;
     R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
 #pragma unroll
@@ -408,7 +418,7 @@ __device__ __forceinline__ R les_tau(const R* s, R rho, R ux, R uy, R uz, R tau,
     const R pxz = sxz - rho * ux * uz;
     const R pyz = syz - rho * uy * uz;
     const R q = pxx * pxx + pyy * pyy + pzz * pzz + R(2) * (pxy * pxy + pxz * pxz + pyz * pyz);
-    return R(0.5) * (tau + sqrt(tau * tau + k * sqrt(q) * rcp(rho)));
+    return R(0.5) * (tau + sqrt(tau * tau + k * sqrt(q) * irho));
 }
 
 // ---------------------------------------------------------------- collision
@@ -416,34 +426,53 @@ __device__ __forceinline__ R les_tau(const R* s, R rho, R ux, R uy, R uz, R tau,
 // one_step_pull.hpp:187-204; BGK, esoteric_pull.hpp:408-432, is the case
 // omega- = omega+), evaluated per opposite pair on s = f_i + f_j and
 // d = f_i - f_j:
-//   equilibrium  s_eq = 2 w rho (1 - 1.5 u^2 + 4.5 (c.u)^2),  d_eq = 6 w rho (c.u)
-//   Guo source   s_F  = 2 w (9 (c.u)(c.F) - 3 u.F),          d_F  = 6 w (c.F)
+//   equilibrium  s_eq = 2 w rho t,  t = 1 - 1.5 u^2 + 4.5 (c.u)^2,   d_eq = 2 w rho (3 c.u)
+//   Guo source   s_F  = 2 w (9 (c.u)(c.F) - 3 u.F),                d_F  = 6 w (c.F)
 //   s' = s - omega+ (s - s_eq) + (1 - omega+/2) s_F
 //   d' = d - omega- (d - d_eq) + (1 - omega-/2) d_F
 //   f_i' = (s' + d') / 2,  f_j' = (s' - d') / 2
-// Gray-LBM partial bounce-back then mixes in the incoming opposite population:
+// The halves s'/2 and d'/2 are formed directly with per-weight-class
+// coefficients computed once per cell, so a pair costs a handful of fused
+// multiply-adds.  With DELTA the values are deviations f - w: s_eq becomes
+// 2 w (rho t - 1) (w_i = w_j within a pair, so d is unchanged).  Gray-LBM
+// partial bounce-back then mixes in the incoming opposite population:
 // f_i <- (1 - n_s) f_i' + n_s fin_j (Walsh, Burwinkle & Saar 2009).
-// With DELTA the values are deviations f - w: the same update holds with
-// s_eq - 2w in place of s_eq (w_i = w_j within a pair, so d is unchanged).
+//
+// Rounding: the mass and momentum coefficients both derive from the per-cell
+// product w rho (rounded differently in every cell), then times omega+ or
+// omega-.  A coefficient formed from constants alone (3 omega- w) carries one
+// rounding error shared by every cell and every step, which the collision
+// turns into a steady gain or loss of momentum against mass: with
+// 3 omega- w rho, a 64^3 Taylor-Green vortex in FP32 gained kinetic energy at
+// 2.3e-7 relative per step against FP64.  What remains is the representation
+// error of the FP32 weights themselves, as in the reference.
+template <class R> struct ClassCoef {
+    R a;  // omega+ w rho          (s'/2 equilibrium term: a * t)
+    R a0; // omega+ w              (DELTA: subtracted)
+    R c;  // omega- w rho          (d'/2 equilibrium term: c * (3 c.u))
+    R g1; // 3 (1 - omega+/2) w    (s'/2 force term: g1 * ((3 c.u)(c.F) - u.F))
+    R g2; // 3 (1 - omega-/2) w    (d'/2 force term)
+};
+
 template <class L, class R, bool FORCE, bool GRAY, bool DELTA, int P = 0>
-__device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, R rho, R ux, R uy, R uz, R fx, R fy, R fz,
-                                              R base, R uf3, R omega, R omega_m, R gp, R gm, R ns) {
+__device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, const ClassCoef<R>* cc, R ux3, R uy3,
+                                              R uz3, R ux15, R uy15, R uz15, R fx, R fy, R fz, R base, R uf, R a1,
+                                              R b1, R ns) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
-        constexpr R w2 = R(2.0 * L::w(i));
-        const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
-        const R wr2 = w2 * rho;
-        const R s_eq = DELTA ? w2 * (rho * (base + R(4.5) * cu * cu) - R(1)) : wr2 * (base + R(4.5) * cu * cu);
-        const R d_eq = wr2 * (R(3) * cu);
-        R sp = s[P] - omega * (s[P] - s_eq);
-        R dp = d[P] - omega_m * (d[P] - d_eq);
+        const ClassCoef<R>& k = cc[weight_class<L>(i)];
+        const R cu3 = R(L::cx(i)) * ux3 + R(L::cy(i)) * uy3 + R(L::cz(i)) * uz3;     // 3 c.u
+        const R cu15 = R(L::cx(i)) * ux15 + R(L::cy(i)) * uy15 + R(L::cz(i)) * uz15; // 1.5 c.u
+        const R t = cu3 * cu15 + base;
+        R sp = DELTA ? k.a * t + (a1 * s[P] - k.a0) : k.a * t + a1 * s[P];
+        R dp = k.c * cu3 + b1 * d[P];
         if constexpr (FORCE) {
             const R cf = R(L::cx(i)) * fx + R(L::cy(i)) * fy + R(L::cz(i)) * fz;
-            sp += gp * (w2 * (R(9) * cu * cf - uf3));
-            dp += gm * (w2 * (R(3) * cf));
+            sp += k.g1 * (cu3 * cf - uf);
+            dp += k.g2 * cf;
         }
-        R oi = R(0.5) * (sp + dp);
-        R oj = R(0.5) * (sp - dp);
+        R oi = sp + dp;
+        R oj = sp - dp;
         if constexpr (GRAY) {
             const R fi = R(0.5) * (s[P] + d[P]);
             const R fj = R(0.5) * (s[P] - d[P]);
@@ -452,8 +481,36 @@ __device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, R rh
         }
         f[i] = oi;
         f[j] = oj;
-        collide_pairs<L, R, FORCE, GRAY, DELTA, P + 1>(f, s, d, rho, ux, uy, uz, fx, fy, fz, base, uf3, omega, omega_m,
-                                                       gp, gm, ns);
+        collide_pairs<L, R, FORCE, GRAY, DELTA, P + 1>(f, s, d, cc, ux3, uy3, uz3, ux15, uy15, uz15, fx, fy, fz, base,
+                                                       uf, a1, b1, ns);
+    }
+}
+
+// Relaxation rates of a cell: omega+ from tau (LES-adjusted) and omega- by
+// the configured rule.
+template <class R> __device__ __forceinline__ R omega_minus_of(const LbmArgs& a, R tau, R omega) {
+    if (a.omega_minus > 0.0) return R(a.omega_minus); // fixed TRT antisymmetric rate
+    if (a.omega_minus < 0.0) return omega;           // BGK
+    // TRT magic: tau- = 1/2 + Lambda / (tau+ - 1/2)
+    const R sp = tau - R(0.5);
+    return sp * rcp(R(a.trt_magic) + R(0.5) * sp);
+}
+
+// Per weight class coefficients; `scale` multiplies every term (FP16 storage
+// units), 1 otherwise.
+template <class L, class R>
+__device__ __forceinline__ void class_coefficients(ClassCoef<R>* cc, R rho, R omega, R omega_m, R gp, R gm,
+                                                   const R* scale) {
+    constexpr int K = L::Q == 27 ? 3 : 2;
+#pragma unroll
+    for (int k = 1; k <= K; ++k) {
+        const R w = R(L::w(class_rep(k))) * scale[k];
+        const R wr = w * rho;
+        cc[k].a0 = omega * w;
+        cc[k].a = omega * wr;
+        cc[k].c = omega_m * wr;
+        cc[k].g1 = R(3) * gp * w;
+        cc[k].g2 = R(3) * gm * w;
     }
 }
 
@@ -463,7 +520,7 @@ __device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
     pair_sums<L, R>(f, s, d);
     R rho, jx, jy, jz;
     pair_moments<L, R, DELTA>(f[0], s, d, rho, jx, jy, jz);
-    const R inv = rho > R(0) ? rcp(rho) : R(0);
+    const R inv = rho > R(0) ? rcp_unbiased(rho) : R(0);
     R ux = jx * inv, uy = jy * inv, uz = jz * inv;
     R ax = R(0), ay = R(0), az = R(0);
     if constexpr (FORCE) {
@@ -473,25 +530,16 @@ __device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
         uz += R(0.5) * az;
     }
     R tau = R(a.tau);
-    if constexpr (LES) tau = les_tau<L, R, DELTA>(s, rho, ux, uy, uz, tau, R(a.les_k));
+    if constexpr (LES) tau = les_tau<L, R, DELTA>(s, rho, inv, ux, uy, uz, tau, R(a.les_k));
     const R omega = rcp(tau);
-    R omega_m;
-    if (a.omega_minus > 0.0) {
-        omega_m = R(a.omega_minus);          // fixed TRT antisymmetric rate
-    } else if (a.omega_minus < 0.0) {
-        omega_m = omega;                     // BGK
-    } else {
-        // TRT magic: tau- = 1/2 + Lambda / (tau+ - 1/2)
-        const R sp = tau - R(0.5);
-        omega_m = sp * rcp(R(a.trt_magic) + R(0.5) * sp);
-    }
+    const R omega_m = omega_minus_of<R>(a, tau, omega);
     const R base = R(1) - R(1.5) * (ux * ux + uy * uy + uz * uz);
-    R fx = R(0), fy = R(0), fz = R(0), uf3 = R(0);
+    R fx = R(0), fy = R(0), fz = R(0), uf = R(0);
     if constexpr (FORCE) {
         fx = rho * ax;
         fy = rho * ay;
         fz = rho * az;
-        uf3 = R(3) * (ux * fx + uy * fy + uz * fz);
+        uf = ux * fx + uy * fy + uz * fz;
     }
     const R gp = R(1) - R(0.5) * omega;
     const R gm = R(1) - R(0.5) * omega_m;
@@ -500,61 +548,26 @@ __device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
     {
         constexpr R w0 = R(L::w(0));
         const R f0 = f[0];
-        R o0 = f0 - omega * (f0 - (DELTA ? w0 * (rho * base - R(1)) : w0 * rho * base));
-        if constexpr (FORCE) o0 -= gp * w0 * uf3;
+        R o0 = (R(1) - omega) * f0 + omega * (DELTA ? w0 * (rho * base - R(1)) : (w0 * rho) * base);
+        if constexpr (FORCE) o0 -= gp * w0 * (R(3) * uf);
         if constexpr (GRAY) o0 = (R(1) - ns) * o0 + ns * f0;
         f[0] = o0;
     }
-    collide_pairs<L, R, FORCE, GRAY, DELTA>(f, s, d, rho, ux, uy, uz, fx, fy, fz, base, uf3, omega, omega_m, gp, gm,
-                                            ns);
+    ClassCoef<R> cc[4];
+    const R unit[4] = {R(1), R(1), R(1), R(1)};
+    class_coefficients<L, R>(cc, rho, omega, omega_m, gp, gm, unit);
+    collide_pairs<L, R, FORCE, GRAY, DELTA>(f, s, d, cc, R(3) * ux, R(3) * uy, R(3) * uz, R(1.5) * ux, R(1.5) * uy,
+                                            R(1.5) * uz, fx, fy, fz, base, uf, R(0.5) * (R(1) - omega),
+                                            R(0.5) * (R(1) - omega_m), ns);
 }
 
 // --------------------------------------------------- FP16 scaled collision
 // The same TRT/Guo/gray update as collide, for values held in FP16 storage
 // units h = (f - w) s_k, with s_k constant within each weight class k.
 // Pair sums stay in storage units: the moments scale each class's partial
-// sums once, and the scales are folded into the relaxation coefficients, so
-// decoding and encoding cost only the half <-> float conversions:
-//   h_i' = [a1 sh + A2_k s_eq + G1_k s_F] + [b1 dh + B2_k d_eq + G2_k d_F]
-//   h_j' = [ ...same... ]               - [ ...same... ]
-// with a1 = (1 - omega+)/2, A2_k = omega+ s_k / 2, G1_k = (1 - omega+/2) s_k / 2,
-// b1 = (1 - omega-)/2, B2_k = omega- s_k / 2, G2_k = (1 - omega-/2) s_k / 2,
-// s_eq = 2 w (rho (1 - 1.5 u^2 + 4.5 (c.u)^2) - 1) and d_eq = 6 w rho (c.u)
-// the deviation-space equilibria.
-template <class L, bool FORCE, bool GRAY, int P = 0>
-__device__ __forceinline__ void collide_pairs_scaled(const LbmArgs& a, float* h, const float* sh, const float* dh,
-                                                     float rho, float ux, float uy, float uz, float fx, float fy,
-                                                     float fz, float base, float uf3, float a1, float b1, float omega,
-                                                     float omega_m, float gp, float gm, float ns) {
-    if constexpr (P < L::PAIRS) {
-        constexpr int i = 2 * P + 1, j = i + 1;
-        constexpr float w2 = float(2.0 * L::w(i));
-        const float sk = a.scale[class_rep(weight_class<L>(i))];
-        const float cu = float(L::cx(i)) * ux + float(L::cy(i)) * uy + float(L::cz(i)) * uz;
-        const float s_eq = w2 * (rho * (base + 4.5F * cu * cu) - 1.0F);
-        const float d_eq = (3.0F * w2) * rho * cu;
-        float sp = a1 * sh[P] + (0.5F * omega * sk) * s_eq;
-        float dp = b1 * dh[P] + (0.5F * omega_m * sk) * d_eq;
-        if constexpr (FORCE) {
-            const float cf = float(L::cx(i)) * fx + float(L::cy(i)) * fy + float(L::cz(i)) * fz;
-            sp += (0.5F * gp * sk) * (w2 * (9.0F * cu * cf - uf3));
-            dp += (0.5F * gm * sk) * (w2 * (3.0F * cf));
-        }
-        float oi = sp + dp;
-        float oj = sp - dp;
-        if constexpr (GRAY) {
-            const float hi = 0.5F * (sh[P] + dh[P]);
-            const float hj = 0.5F * (sh[P] - dh[P]);
-            oi = (1.0F - ns) * oi + ns * hj;
-            oj = (1.0F - ns) * oj + ns * hi;
-        }
-        h[i] = oi;
-        h[j] = oj;
-        collide_pairs_scaled<L, FORCE, GRAY, P + 1>(a, h, sh, dh, rho, ux, uy, uz, fx, fy, fz, base, uf3, a1, b1,
-                                                    omega, omega_m, gp, gm, ns);
-    }
-}
-
+// sums once, and the scales are folded into the per-class coefficients
+// (ClassCoef scaled by s_k), so decoding and encoding cost only the
+// half <-> float conversions.
 template <class L, bool LES, bool GRAY, bool FORCE>
 __device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, float* h) {
     float sh[L::PAIRS], dh[L::PAIRS];
@@ -599,7 +612,7 @@ __device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, float* h
         jz += JZ[k] * inv[k];
     }
     rho += 1.0F;
-    const float irho = rho > 0.0F ? rcp(rho) : 0.0F;
+    const float irho = rho > 0.0F ? rcp_unbiased(rho) : 0.0F;
     float ux = jx * irho, uy = jy * irho, uz = jz * irho;
     float ax = 0.0F, ay = 0.0F, az = 0.0F;
     if constexpr (FORCE) {
@@ -633,22 +646,14 @@ __device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, float* h
         }
     }
     const float omega = rcp(tau);
-    float omega_m;
-    if (a.omega_minus > 0.0) {
-        omega_m = float(a.omega_minus);
-    } else if (a.omega_minus < 0.0) {
-        omega_m = omega;
-    } else {
-        const float sp = tau - 0.5F;
-        omega_m = sp * rcp(float(a.trt_magic) + 0.5F * sp);
-    }
+    const float omega_m = omega_minus_of<float>(a, tau, omega);
     const float base = 1.0F - 1.5F * (ux * ux + uy * uy + uz * uz);
-    float fx = 0.0F, fy = 0.0F, fz = 0.0F, uf3 = 0.0F;
+    float fx = 0.0F, fy = 0.0F, fz = 0.0F, uf = 0.0F;
     if constexpr (FORCE) {
         fx = rho * ax;
         fy = rho * ay;
         fz = rho * az;
-        uf3 = 3.0F * (ux * fx + uy * fy + uz * fz);
+        uf = ux * fx + uy * fy + uz * fz;
     }
     const float gp = 1.0F - 0.5F * omega;
     const float gm = 1.0F - 0.5F * omega_m;
@@ -658,20 +663,52 @@ __device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, float* h
         constexpr float w0 = float(L::w(0));
         const float h0 = h[0];
         float o0 = (1.0F - omega) * h0 + a.scale[0] * (omega * w0 * (rho * base - 1.0F));
-        if constexpr (FORCE) o0 -= a.scale[0] * (gp * w0 * uf3);
+        if constexpr (FORCE) o0 -= a.scale[0] * (gp * w0 * (3.0F * uf));
         if constexpr (GRAY) o0 = (1.0F - ns) * o0 + ns * h0;
         h[0] = o0;
     }
-    collide_pairs_scaled<L, FORCE, GRAY>(a, h, sh, dh, rho, ux, uy, uz, fx, fy, fz, base, uf3, 0.5F * (1.0F - omega),
-                                         0.5F * (1.0F - omega_m), omega, omega_m, gp, gm, ns);
+    ClassCoef<float> cc[4];
+    float scl[4];
+#pragma unroll
+    for (int k = 0; k <= K; ++k) scl[k] = a.scale[class_rep(k)];
+    class_coefficients<L, float>(cc, rho, omega, omega_m, gp, gm, scl);
+    collide_pairs<L, float, FORCE, GRAY, true>(h, sh, dh, cc, 3.0F * ux, 3.0F * uy, 3.0F * uz, 1.5F * ux, 1.5F * uy,
+                                               1.5F * uz, fx, fy, fz, base, uf, 0.5F * (1.0F - omega),
+                                               0.5F * (1.0F - omega_m), ns);
 }
 
 // ---------------------------------------------------------------- the step
 // CPT cells per thread (stacked in z): the loads of all of a thread's cells are
 // issued before the first collision.  One cell per thread measured best on
 // B200 (more cells cost occupancy through registers), and the launcher uses 1.
+// Minimum resident 128-thread blocks per SM the step kernels are compiled for;
+// it caps registers at 65536 / (128 * blocks).  The step is latency bound at
+// the occupancy its natural register count allows: measured on B200 at 512^3,
+// 10 blocks (48 registers, a few spilled words that stay in L1) beat the
+// uncapped 64-96 registers by 10-55% for FP32 and FP16 storage; FP64 storage
+// keeps its full register set.  The macros exist for tuning builds.
+#ifndef CFDX_STEP_MIN_BLOCKS_Q19
+#define CFDX_STEP_MIN_BLOCKS_Q19 10
+#endif
+#ifndef CFDX_STEP_MIN_BLOCKS_Q27_F16
+#define CFDX_STEP_MIN_BLOCKS_Q27_F16 10
+#endif
+#ifndef CFDX_STEP_MIN_BLOCKS_Q27_F32
+#define CFDX_STEP_MIN_BLOCKS_Q27_F32 8
+#endif
+#ifndef CFDX_PAIR_MIN_BLOCKS
+#define CFDX_PAIR_MIN_BLOCKS 8
+#endif
+
+template <class L, class S> constexpr int step_min_blocks() {
+    return sizeof(typename S::T) == 8 ? 1
+         : (L::Q == 19 ? CFDX_STEP_MIN_BLOCKS_Q19
+                       : (sizeof(typename S::T) == 2 ? CFDX_STEP_MIN_BLOCKS_Q27_F16 : CFDX_STEP_MIN_BLOCKS_Q27_F32));
+}
+template <class S> constexpr int pair_min_blocks() { return sizeof(typename S::T) == 8 ? 1 : CFDX_PAIR_MIN_BLOCKS; }
+
 template <class L, class S, bool LES, bool FLAGS, bool GRAY, int CPT, bool NARROW>
-__global__ void __launch_bounds__(128) k_step(const __grid_constant__ LbmArgs a) {
+__global__ void __launch_bounds__(128, step_min_blocks<L, S>()) k_step(const __grid_constant__ LbmArgs a) {
     using R = typename S::R;
     const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;

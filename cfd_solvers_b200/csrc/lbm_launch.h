@@ -26,10 +26,6 @@ struct KernelKey {
     int cells_per_thread; // reserved (one cell per thread)
     bool paired;          // use the paired-cell step kernel (two adjacent x cells per thread)
     bool narrow;          // 32-bit slot offsets (q * cells < 2^32)
-    bool rows;            // use the row-staged (bulk-copy) step kernel
-    unsigned row_stages;  // its pipeline depth
-    unsigned row_stage_bytes;
-    unsigned row_threads; // its block size
 };
 
 dim3 cell_block(long long nx, long long ny, const LaunchShape& s);
@@ -37,7 +33,6 @@ dim3 cell_grid(long long nx, long long ny, long long nz, dim3 block);
 
 template <int STORAGE> struct Launcher {
     static cudaError_t step(const KernelKey& k, const LbmArgs& a, dim3 grid, dim3 block, cudaStream_t s);
-    static int row_ctas(const KernelKey& k);
     static cudaError_t init(const KernelKey& k, const LbmArgs& a, const InitSpec& spec, dim3 grid, dim3 block,
                             cudaStream_t s);
     static cudaError_t macro(const KernelKey& k, const LbmArgs& a, void* rho, void* ux, void* uy, void* uz,
@@ -49,8 +44,6 @@ template <int STORAGE> struct Launcher {
 };
 
 cudaError_t launch_step(const KernelKey& k, const LbmArgs& a, dim3 grid, dim3 block, cudaStream_t s);
-// Occupancy of the row-staged kernel for the key: CTAs per SM (0 = does not fit).
-int row_kernel_ctas_per_sm(const KernelKey& k);
 cudaError_t launch_init(const KernelKey& k, const LbmArgs& a, const InitSpec& spec, dim3 grid, dim3 block,
                         cudaStream_t s);
 cudaError_t launch_macro(const KernelKey& k, const LbmArgs& a, void* rho, void* ux, void* uy, void* uz,

@@ -4,7 +4,6 @@
 
 #include "lbm_device.cuh"
 #include "lbm_launch.h"
-#include "lbm_step_tma.cuh"
 #include "lbm_step_x2.cuh"
 
 namespace cfdx {
@@ -49,36 +48,8 @@ cudaError_t step_paired(const LbmArgs& a, dim3 b, cudaStream_t s) {
     }
 }
 
-// Row-staged kernel: persistent CTAs, dynamic shared memory for the stages;
-// grid.x carries the number of CTAs chosen by the host.
-template <class L, class S, bool LES, bool FL, bool GR>
-cudaError_t step_rows(const KernelKey& k, const LbmArgs& a, dim3 g, cudaStream_t s) {
-    auto kernel = k_step_rows<L, S, LES, FL, GR>;
-    const unsigned smem = 128U + k.row_stages * k.row_stage_bytes;
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    RowStages rs{k.row_stages, a.nx * static_cast<unsigned>(sizeof(typename S::T)), k.row_stage_bytes};
-    kernel<<<dim3(g.x, 1, 1), dim3(k.row_threads, 1, 1), smem, s>>>(a, rs);
-    return cudaGetLastError();
-}
-
-template <class L, class S, bool LES, bool FL, bool GR> int rows_occupancy(const KernelKey& k) {
-    auto kernel = k_step_rows<L, S, LES, FL, GR>;
-    const unsigned smem = 128U + k.row_stages * k.row_stage_bytes;
-    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
-        cudaSuccess)
-        return 0;
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, static_cast<int>(k.row_threads), smem) !=
-        cudaSuccess)
-        return 0;
-    return n;
-}
-
 template <class L, class S, bool LES, bool FL>
 cudaError_t step_gray(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
-    if (k.rows)
-        return k.gray ? step_rows<L, S, LES, FL, true>(k, a, g, s) : step_rows<L, S, LES, FL, false>(k, a, g, s);
     if (k.paired)
         return k.gray ? step_paired<L, S, LES, FL, true>(a, b, s) : step_paired<L, S, LES, FL, false>(a, b, s);
     return k.gray ? step_single<L, S, LES, FL, true>(k.narrow, a, g, b, s)
@@ -100,27 +71,6 @@ cudaError_t Launcher<STORAGE>::step(const KernelKey& k, const LbmArgs& a, dim3 g
         using L = decltype(lat);
         return k.les ? step_flags<L, S, true>(k, a, g, b, s) : step_flags<L, S, false>(k, a, g, b, s);
     });
-}
-
-template <int STORAGE> int Launcher<STORAGE>::row_ctas(const KernelKey& k) {
-    using S = typename StorageOf<STORAGE>::type;
-    int n = 0;
-    with_lattice(k.q, [&](auto lat) {
-        using L = decltype(lat);
-        if (k.les) {
-            if (k.flags)
-                n = k.gray ? rows_occupancy<L, S, true, true, true>(k) : rows_occupancy<L, S, true, true, false>(k);
-            else
-                n = k.gray ? rows_occupancy<L, S, true, false, true>(k) : rows_occupancy<L, S, true, false, false>(k);
-        } else {
-            if (k.flags)
-                n = k.gray ? rows_occupancy<L, S, false, true, true>(k) : rows_occupancy<L, S, false, true, false>(k);
-            else
-                n = k.gray ? rows_occupancy<L, S, false, false, true>(k) : rows_occupancy<L, S, false, false, false>(k);
-        }
-        return cudaSuccess;
-    });
-    return n;
 }
 
 template <int STORAGE>

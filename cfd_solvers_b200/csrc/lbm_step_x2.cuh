@@ -182,7 +182,7 @@ __device__ __forceinline__ void bounce_fixup(const LbmArgs& a, const typename S:
 }
 
 template <class L, class S, bool LES, bool FLAGS, bool GRAY>
-__global__ void __launch_bounds__(128) k_step_x2(const __grid_constant__ LbmArgs a) {
+__global__ void __launch_bounds__(128, pair_min_blocks<S>()) k_step_x2(const __grid_constant__ LbmArgs a) {
     using R = typename S::R;
     using T = typename S::T;
     PairCtx c;

@@ -356,7 +356,7 @@ class EsotericPullCudaSolver:
         self._call("cfdx_lbm_set_storage_scale", ctypes.c_void_p(s.ctypes.data))
 
     def set_launch_shape(self, block_x: int = 0, block_y: int = 0, variant: int = 0):
-        """Threads per block and step-kernel variant (0 auto, 1 one cell, 2 paired cells, 3 row-staged)."""
+        """Threads per block and step-kernel variant (0 auto, 1 one cell, 2 paired cells)."""
         self._call("cfdx_lbm_set_launch_shape", int(block_x), int(block_y), int(variant))
 
     def stream(self) -> int:

@@ -71,7 +71,14 @@ def test_reference_plain_method_64cubed(engine, golden):
         got = [a[:: m["stride"]] for a in s.compute_macroscopic()]
         ref = [data[f"c1_d3q19_tg64_{k}"] for k in ("rho", "ux", "uy", "uz")]
         assert fields_err(got, ref) < FP32_GATE
-        assert s.checksum() == pytest.approx(m["checksum"], rel=1e-7)
+        # FP32 populations drift in mass by O(1e-6) over 110 steps (the
+        # reference's own mass is 262144.70, not 262144), and the drift
+        # depends on the order of the per-cell float operations, so the sums
+        # carry an FP32 tolerance: mass within 1e-6, kinetic energy within 1e-5.
+        assert s.mass() == pytest.approx(m["mass"], rel=1e-6)
+        assert s.kinetic_energy() == pytest.approx(m["kinetic_energy"], rel=1e-5)
+        assert s.max_speed() == pytest.approx(m["max_speed"], rel=1e-5)
+        assert s.checksum() == pytest.approx(m["checksum"], rel=1e-6)
 
 
 def test_reference_phase02_checksum(engine, golden):
@@ -81,7 +88,9 @@ def test_reference_phase02_checksum(engine, golden):
     with make(engine, 19, 48, 48, 48, tau=0.58, smagorinsky_les=True) as s:
         s.initialize_taylor_green(0.04)
         s.step(80)
-        assert s.checksum() == pytest.approx(p["checksum"], rel=1e-7)
+        # The published checksum comes from the reference's FP32 build; the
+        # FP32 mass drift bound of the plain-method test applies.
+        assert s.checksum() == pytest.approx(p["checksum"], rel=1e-6)
 
 
 @pytest.mark.parametrize("q", [19, 27])

@@ -62,25 +62,3 @@ def test_paired_variant_requires_even_nx(engine):
         s.set_launch_shape(0, 0, 0)  # automatic falls back to one cell per thread
         s.step(3)
 
-
-ROW_SHAPES = [(32, 9, 7), (64, 6, 5), (16, 5, 4), (48, 4, 6)]
-
-
-@pytest.mark.parametrize("q", [19, 27])
-@pytest.mark.parametrize("storage", ["fp32", "fp16s"])
-@pytest.mark.parametrize("shape", ROW_SHAPES, ids=[f"{a}x{b}x{c}" for a, b, c in ROW_SHAPES])
-@pytest.mark.parametrize("flags_kind, gray", [(None, False), ("random", False), ("cavity", True)])
-@pytest.mark.parametrize("steps", [5, 6])
-def test_row_staged_matches_single_bitwise(engine, q, storage, shape, flags_kind, gray, steps):
-    """The row-staged kernel (rows streamed through shared memory by bulk copies) against one cell per thread."""
-    a_log, a_red = run(engine, 1, q, shape, storage, flags_kind, gray, steps)
-    b_log, b_red = run(engine, 3, q, shape, storage, flags_kind, gray, steps)
-    assert np.array_equal(a_log.view(np.uint32), b_log.view(np.uint32))
-    assert a_red["mass"] == b_red["mass"]
-
-
-def test_row_staged_variant_requires_16_aligned_rows(engine):
-    cs = engine
-    with cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(nx=24, ny=4, nz=4)) as s:
-        with pytest.raises(ValueError, match="row-staged"):
-            s.set_launch_shape(0, 0, 3)
