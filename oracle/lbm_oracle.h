@@ -89,6 +89,17 @@ int ora_reduce(const ora_cfg* c, const void* f, uint64_t t, double out[7]);
  * boundary handling).  Reference: esoteric_pull.hpp:257-267. */
 int ora_logical(const ora_cfg* c, const void* f, uint64_t t, void* out);
 
+/* FP64 discrete adjoint (lbm_adjoint_oracle.c), on logical populations x
+ * ([d][n], what ora_logical returns) with the forward's cfg (BGK/TRT, Guo
+ * forcing, gray n_s, stationary walls; no LES, no moving walls).
+ * ora_adjoint_forward: x_end = x after `steps` logical steps.
+ * ora_adjoint: for J with dJ/drho = g_rho (N, may be NULL) and dJ/du = g_u
+ * (3*N, ux | uy | uz) at the final state, grad_ns[n] = dJ/dn_s(n) and
+ * *grad_tau = dJ/dtau. */
+int ora_adjoint_forward(const ora_cfg* c, const double* x0, uint64_t steps, double* x_end);
+int ora_adjoint(const ora_cfg* c, const double* x0, uint64_t steps, const double* g_rho, const double* g_u,
+                double* grad_ns, double* grad_tau);
+
 /* IEEE binary16 round-to-nearest-even conversion used by the F16S storage. */
 uint16_t ora_f32_to_f16(float v);
 float ora_f16_to_f32(uint16_t h);

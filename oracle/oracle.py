@@ -79,7 +79,10 @@ def oracle_lib():
         lib.ora_f16_to_f32.argtypes = [ctypes.c_uint16]
         lib.ora_f16_to_f32.restype = ctypes.c_float
         lib.ora_reference_les_k.restype = ctypes.c_float
-        for name in ("ora_init", "ora_step", "ora_macroscopic", "ora_reduce", "ora_logical"):
+        lib.ora_adjoint_forward.argtypes = [P, _d, ctypes.c_uint64, _d]
+        lib.ora_adjoint.argtypes = [P, _d, ctypes.c_uint64, _d, _d, _d, _d]
+        for name in ("ora_init", "ora_step", "ora_macroscopic", "ora_reduce", "ora_logical", "ora_adjoint_forward",
+                     "ora_adjoint"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -203,6 +206,40 @@ class OracleLattice:
         out = np.zeros(self.q * self.cells, dt)
         self._call(oracle_lib().ora_logical(ctypes.byref(self._cfg), self.f.ctypes.data, self.t, out.ctypes.data))
         return out
+
+
+    # ------------------------------------------------ FP64 discrete adjoint
+    def adjoint_forward(self, x0: np.ndarray, steps: int) -> np.ndarray:
+        """Logical FP64 forward (lbm_adjoint_oracle.c): x after `steps` steps."""
+        self._refresh()
+        x0 = np.ascontiguousarray(x0, np.float64)
+        out = np.zeros_like(x0)
+        self._call(oracle_lib().ora_adjoint_forward(ctypes.byref(self._cfg), _ptr(x0, _d), steps, _ptr(out, _d)))
+        return out
+
+    def adjoint(self, x0: np.ndarray, steps: int, g_u: np.ndarray, g_rho: Optional[np.ndarray] = None):
+        """dJ/dn_s (per cell) and dJ/dtau for dJ/du = g_u (3, N) and dJ/drho = g_rho at the final state."""
+        self._refresh()
+        x0 = np.ascontiguousarray(x0, np.float64)
+        gu = np.ascontiguousarray(g_u, np.float64).reshape(3 * self.cells)
+        gr = None if g_rho is None else np.ascontiguousarray(g_rho, np.float64)
+        gns = np.zeros(self.cells, np.float64)
+        gtau = np.zeros(1, np.float64)
+        self._call(oracle_lib().ora_adjoint(ctypes.byref(self._cfg), _ptr(x0, _d), steps, _ptr(gr, _d), _ptr(gu, _d),
+                                            _ptr(gns, _d), _ptr(gtau, _d)))
+        return gns, float(gtau[0])
+
+
+def logical_velocity(x: np.ndarray, q: int, cells: int, accel=(0.0, 0.0, 0.0)):
+    """rho and u + a/2 of logical populations x ([d][n], float64)."""
+    cx = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1])[:q]
+    cy = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1])[:q]
+    cz = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1])[:q]
+    f = x.reshape(q, cells)
+    rho = f.sum(0)
+    safe = np.where(rho > 0, rho, 1.0)
+    u = np.stack([cx @ f, cy @ f, cz @ f]) / safe + 0.5 * np.asarray(accel, np.float64)[:, None]
+    return rho, np.where(rho > 0, u, 0.0)
 
 
 def f32_to_f16_bits(v: float) -> int:
