@@ -216,6 +216,161 @@ def measure_variant(torch, cs, n, lattice, storage, steps, device):
     return {"glups": glups, "ms_per_step": ms / steps, "achieved_gbs": gbs, "nonfinite": red["nonfinite"]}
 
 
+# ------------------------------------------------- differentiation (adjoint)
+def gray_solver(cs, lattice, n, storage, device, gx=1e-5, tau=0.6):
+    """Gray-LBM TRT (magic 3/16) channel, periodic in x, body force gx (the adjoint configurations)."""
+    from cfd_solvers_b200.cases import channel_flags
+
+    s = cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(
+        nx=n, ny=n, nz=n, tau=tau, lattice=lattice, collision="trt", trt_magic=3.0 / 16.0, acceleration_x=gx,
+        storage=storage, device=device))
+    flags = channel_flags(n, n, n)
+    s.set_flags(flags)
+    return s, flags == 0
+
+
+def misfit_target(s, ns_hidden, steps):
+    """u* = u(steps) of the forward model run with the hidden solid fraction (float64 host)."""
+    s.set_solid_fraction(ns_hidden)
+    s.initialize_uniform()
+    s.step(steps)
+    f = s.compute_macroscopic()
+    return np.stack([np.asarray(f.ux, np.float64), np.asarray(f.uy, np.float64), np.asarray(f.uz, np.float64)])
+
+
+def misfit(s, ns, fluid, target, steps):
+    """J = 1/2 sum over fluid cells |u(steps) - u*|^2, FP64 fields (FP64 storage)."""
+    s.set_solid_fraction(ns)
+    s.initialize_uniform()
+    s.step(steps)
+    import ctypes
+
+    from cfd_solvers_b200 import bindings as B
+
+    out = [np.zeros(s.cells(), np.float64) for _ in range(4)]
+    s.library.call("cfdx_lbm_macroscopic_f64", s.handle, *[ctypes.c_void_p(o.ctypes.data) for o in out], B.HOST)
+    r = (np.stack(out[1:]) - target) * fluid
+    return 0.5 * float(np.sum(r * r))
+
+
+def adjoint_gradient(torch, s, ns, fluid, target, steps, interval):
+    """(dJ/dn_s, dJ/dtau, timings) of the misfit through the discrete adjoint."""
+    stream = torch.cuda.ExternalStream(s.stream())
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    s.set_solid_fraction(ns)
+    s.initialize_uniform()
+    s.wait()
+    ev[0].record(stream)
+    s.adjoint_forward(steps, interval)
+    ev[1].record(stream)
+    f = s.compute_macroscopic()
+    g = ((np.stack([f.ux, f.uy, f.uz]).astype(np.float64) - target) * fluid).astype(np.float32)
+    gd = torch.from_numpy(g).cuda()
+    grad = torch.empty(s.cells(), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    gns, gtau = s.adjoint_backward(gd[0], gd[1], gd[2], grad_ns_out=grad)
+    ev[2].record(stream)
+    ev[2].synchronize()
+    return grad.cpu().numpy(), gtau, ev[0].elapsed_time(ev[1]), e2.elapsed_time(ev[2])
+
+
+def adjoint_case(torch, cs, lattice, n, storage, steps, interval, device, seeds=(1, 2)):
+    """One differentiation workload: timings of forward, checkpointed forward and reverse sweep."""
+    from cfd_solvers_b200.cases import gray_field
+
+    s, fluid = gray_solver(cs, lattice, n, storage, device)
+    try:
+        cells = n ** 3
+        ns = gray_field(cells, seeds[0])
+        target = misfit_target(s, gray_field(cells, seeds[1]), steps)
+        s.set_solid_fraction(ns)
+        s.initialize_uniform()
+        time_steps(torch, s, 3)
+        s.initialize_uniform()
+        fwd_ms = time_steps(torch, s, steps)
+        free0 = torch.cuda.mem_get_info()[0]
+        gns, gtau, afwd_ms, bwd_ms = adjoint_gradient(torch, s, ns, fluid, target, steps, interval)
+        mem = s.adjoint_memory()
+        s.adjoint_release()
+    finally:
+        s.close()
+    return {
+        "lattice": lattice, "n": n, "storage": storage, "steps": steps, "checkpoint_interval": interval,
+        "forward_ms_per_step": fwd_ms / steps, "checkpointed_forward_ms_per_step": afwd_ms / steps,
+        "adjoint_ms_per_step": bwd_ms / steps, "adjoint_over_forward": bwd_ms / fwd_ms,
+        "forward_glups": cells * steps / (fwd_ms / 1e3) / 1e9,
+        "adjoint_buffers_gb": mem / 1e9, "lattice_gb": None, "free_gb_before_adjoint": free0 / 1e9,
+        "grad_tau": gtau, "grad_ns_l2": float(np.linalg.norm(gns)),
+    }, gns, gtau
+
+
+def adjoint_fd_check(torch, cs, n, steps, interval, device, cells=32, seeds=(1, 2, 3), h=1e-5):
+    """FP32-storage adjoint vs FP64 central finite differences on `cells` random fluid cells."""
+    from cfd_solvers_b200.cases import gray_field
+
+    s64, fluid = gray_solver(cs, "d3q19", n, "fp64", device)
+    s32, _ = gray_solver(cs, "d3q19", n, "fp32", device)
+    try:
+        N = n ** 3
+        ns = gray_field(N, seeds[0])
+        target = misfit_target(s64, gray_field(N, seeds[1]), steps)
+        g32, gt32, _, _ = adjoint_gradient(torch, s32, ns, fluid, target, steps, interval)
+        g64, gt64, _, _ = adjoint_gradient(torch, s64, ns, fluid, target, steps, interval)
+        pick = np.random.default_rng(seeds[2]).choice(np.flatnonzero(fluid), cells, replace=False)
+        fd = []
+        for c in pick:
+            p, m = ns.copy(), ns.copy()
+            p[c] += np.float32(h)
+            m[c] -= np.float32(h)
+            fd.append((misfit(s64, p, fluid, target, steps) - misfit(s64, m, fluid, target, steps)) /
+                      (float(p[c]) - float(m[c])))
+        fd = np.array(fd)
+    finally:
+        s64.close()
+        s32.close()
+    def errors(g):
+        e = g[pick] - fd
+        return {"rel_l2": float(np.linalg.norm(e) / np.linalg.norm(fd)),
+                "max_rel_to_max": float(np.max(np.abs(e)) / np.max(np.abs(fd))),
+                "max_rel_per_cell": float(np.max(np.abs(e) / np.abs(fd)))}
+
+    return {
+        "lattice": f"D3Q19 {n}^3 copy", "steps": steps, "cells": cells, "fd_step": h,
+        "fd": "central differences of the FP64-storage GPU forward (FP64 arithmetic)",
+        "fp32_adjoint_vs_fd": errors(g32), "fp64_adjoint_vs_fd": errors(g64),
+        "fp32_vs_fp64_adjoint_grad_tau_rel": abs(gt32 - gt64) / abs(gt64),
+    }
+
+
+def grad_errors(g, ref, gt, gt_ref):
+    return {"grad_ns_rel_l2": float(np.linalg.norm(g - ref) / np.linalg.norm(ref)),
+            "grad_ns_max_rel_to_max": float(np.max(np.abs(g - ref)) / np.max(np.abs(ref))),
+            "grad_tau_rel": abs(gt - gt_ref) / abs(gt_ref)}
+
+
+def differentiation_variants(torch, cs, device, full=True):
+    """The two differentiation configurations: adjoint/forward time, memory, gradient error."""
+    out = {}
+    c4, _, _ = adjoint_case(torch, cs, "d3q19", 128, "fp32", 2000, 64, device)
+    c4["fd_check"] = adjoint_fd_check(torch, cs, 32, 2000, 64, device)
+    out["gray_d3q19_128_fp32"] = c4
+    if full:
+        c5, _, _ = adjoint_case(torch, cs, "d3q27", 256, "fp16s", 4000, 64, device)
+        # Gradient errors of FP16 storage against FP32 storage and the FP64 GPU adjoint (itself
+        # pinned to the FP64 CPU adjoint) at 128^3: the FP32/FP64 checkpoints of the 256^3 run
+        # would not fit in 180 GB with one level of checkpointing.
+        runs = {st: adjoint_case(torch, cs, "d3q27", 128, st, 4000, 64, device) for st in ("fp16s", "fp32", "fp64")}
+        c5["gradient_errors_128"] = {
+            "fp16_vs_fp32": grad_errors(runs["fp16s"][1], runs["fp32"][1], runs["fp16s"][2], runs["fp32"][2]),
+            "fp16_vs_fp64": grad_errors(runs["fp16s"][1], runs["fp64"][1], runs["fp16s"][2], runs["fp64"][2]),
+            "fp32_vs_fp64": grad_errors(runs["fp32"][1], runs["fp64"][1], runs["fp32"][2], runs["fp64"][2]),
+        }
+        out["gray_d3q27_256_fp16s"] = c5
+    return out
+
+
 # ----------------------------------------------------------- reference (CPU)
 def cpu_reference_sample(n, warmup, steps, threads=0):
     """The reference's CPU path on the closest feature set: EsotericPullSolver<D3Q19>

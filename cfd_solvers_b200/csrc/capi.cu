@@ -143,16 +143,41 @@ struct cfdx_lbm {
     static bool paired_default(int storage, int q) { return storage == kStoreF16S && q == 19; }
     double les_k = 0.0;
     std::uint64_t h2d = 0, d2h = 0, syncs = 0;
+    bool moving_walls = false; // some flag is a moving-wall id (2..15)
 
-    LbmArgs args() const {
+    // Discrete adjoint (cfdx_lbm_adjoint_*): forward checkpoints every
+    // `interval` steps, recompute frames for one segment, the adjoint lattice
+    // and the gradient accumulators.  Buffers are kept for reuse until
+    // cfdx_lbm_adjoint_release or destroy.
+    struct Adjoint {
+        std::uint64_t t0 = 0, steps = 0, t_end = 0;
+        std::uint32_t interval = 0;
+        bool ready = false;     // a forward pass has run and nothing has changed since
+        void* checkpoints = nullptr;
+        std::size_t checkpoint_bytes = 0;
+        void* frames = nullptr;
+        std::size_t frame_bytes = 0;
+        void* lam = nullptr;
+        std::size_t lam_bytes = 0;
+        double* grad_ns = nullptr;
+        double* tau_partials = nullptr;
+        std::size_t tau_blocks = 0;
+        double* tau_out = nullptr;
+        float* seed = nullptr; // 4*N staging for host-side seeds
+    } adj;
+
+    LbmArgs args() const { return args_at(f, storage_bytes(key.storage), static_cast<int>(t & 1U)); }
+    // Arguments for a lattice of this handle's shape at `lattice` (element
+    // size `es` bytes), with the slot tables of parity `odd`.
+    LbmArgs args_at(void* lattice, int elem_bytes, int odd) const {
         LbmArgs a{};
-        char* base = static_cast<char*>(f);
-        const std::size_t es = static_cast<std::size_t>(storage_bytes(key.storage));
+        char* base = static_cast<char*>(lattice);
+        const std::size_t es = static_cast<std::size_t>(elem_bytes);
         for (int d = 0; d < 27; ++d) a.fd[d] = d < key.q ? base + static_cast<std::size_t>(d) * N * es : nullptr;
         a.rest = a.fd[0];
-        a.base = f;
+        a.base = lattice;
         a.rest_off = 0U;
-        set_parity(a, static_cast<int>(t & 1U));
+        set_parity(a, odd);
         a.flags = key.flags ? flags : nullptr;
         a.ax_field = local_a;
         a.ay_field = local_a ? local_a + N : nullptr;
@@ -285,6 +310,7 @@ void init_state(cfdx_lbm* h, const InitSpec& spec) {
     check_cuda(cudaMemsetAsync(h->f, 0, h->f_bytes, h->stream), "cudaMemsetAsync");
     check_cuda(launch_init(h->key, h->args(), spec, h->grid(), h->block(), h->stream), "init kernel");
     h->t = 0;
+    h->adj.ready = false;
 }
 
 void ensure_reduce(cfdx_lbm* h) {
@@ -299,6 +325,18 @@ void ensure_reduce(cfdx_lbm* h) {
     check_cuda(cudaMallocHost(&h->host_reduce, sizeof(double) * kReduceFields), "cudaMallocHost");
 }
 
+void release_adjoint(cfdx_lbm* h) {
+    auto& A = h->adj;
+    device_free(A.checkpoints);
+    device_free(A.frames);
+    device_free(A.lam);
+    device_free(A.grad_ns);
+    device_free(A.tau_partials);
+    device_free(A.tau_out);
+    device_free(A.seed);
+    A = cfdx_lbm::Adjoint{};
+}
+
 void release(cfdx_lbm* h) {
     if (!h) return;
     cudaSetDevice(h->cfg.device);
@@ -310,6 +348,7 @@ void release(cfdx_lbm* h) {
     device_free(h->macro_scratch);
     device_free(h->reduce_partials);
     device_free(h->reduce_out);
+    release_adjoint(h);
     if (h->host_reduce) cudaFreeHost(h->host_reduce);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -381,6 +420,33 @@ cudaError_t launch_reduce(const KernelKey& k, const LbmArgs& a, double* partials
     }
 }
 
+cudaError_t launch_step_oop(const KernelKey& k, const LbmArgs& src, const LbmArgs& dst, dim3 g, dim3 b,
+                            cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::step_oop(k, src, dst, g, b, s);
+    case kStoreF64: return Launcher<kStoreF64>::step_oop(k, src, dst, g, b, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::step_oop(k, src, dst, g, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_adjoint_seed(const KernelKey& k, const AdjointArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::adjoint_seed(k, a, g, b, s);
+    case kStoreF64: return Launcher<kStoreF64>::adjoint_seed(k, a, g, b, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::adjoint_seed(k, a, g, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_adjoint_step(const KernelKey& k, const AdjointArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::adjoint_step(k, a, g, b, s);
+    case kStoreF64: return Launcher<kStoreF64>::adjoint_step(k, a, g, b, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::adjoint_step(k, a, g, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 int handle_reduce_view(cfdx_lbm* h, ReduceView* view) {
     return guarded([&] {
@@ -538,8 +604,10 @@ CFDX_API int cfdx_lbm_init_fields(cfdx_lbm* h, const float* fields, int where) {
 CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
     return guarded([&] {
         checked(h);
+        h->adj.ready = false;
         if (!flags) {
             h->key.flags = false;
+            h->moving_walls = false;
             h->choose_variant();
             return;
         }
@@ -547,6 +615,17 @@ CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int wher
         std::uint8_t* user = static_cast<std::uint8_t*>(device_alloc(h->N, "flag staging"));
         try {
             upload(h, user, flags, h->N, where);
+            // Record whether any cell is a moving wall (the adjoint does not cover them).
+            std::string host_copy;
+            const std::uint8_t* scan = flags;
+            if (where == CFDX_DEVICE) {
+                host_copy.resize(h->N);
+                check_cuda(cudaMemcpyAsync(host_copy.data(), user, h->N, cudaMemcpyDeviceToHost, h->stream),
+                           "cudaMemcpyAsync (flag scan)");
+                h->sync();
+                scan = reinterpret_cast<const std::uint8_t*>(host_copy.data());
+            }
+            h->moving_walls = std::any_of(scan, scan + h->N, [](std::uint8_t v) { return v >= CFDX_MOVING_WALL_MIN; });
             check_cuda(launch_prepare_flags(h->key.q, h->args(), user, h->flags, h->grid(), h->block(), h->stream),
                        "flag preparation kernel");
             h->sync();
@@ -563,6 +642,7 @@ CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int wher
 CFDX_API int cfdx_lbm_set_wall_velocity(cfdx_lbm* h, int id, float ux, float uy, float uz) {
     return guarded([&] {
         checked(h);
+        h->adj.ready = false;
         if (id < CFDX_MOVING_WALL_MIN || id >= CFDX_MAX_WALL_IDS)
             throw std::out_of_range("moving-wall id must be in [2, 15]");
         require(std::isfinite(ux) && std::isfinite(uy) && std::isfinite(uz), "wall velocity must be finite");
@@ -575,6 +655,7 @@ CFDX_API int cfdx_lbm_set_wall_velocity(cfdx_lbm* h, int id, float ux, float uy,
 CFDX_API int cfdx_lbm_set_local_acceleration(cfdx_lbm* h, const float* accel, int where) {
     return guarded([&] {
         checked(h);
+        h->adj.ready = false;
         if (!accel) {
             device_free(h->local_a);
             h->local_a = nullptr;
@@ -588,6 +669,7 @@ CFDX_API int cfdx_lbm_set_local_acceleration(cfdx_lbm* h, const float* accel, in
 CFDX_API int cfdx_lbm_device_local_acceleration(cfdx_lbm* h, float** accel) {
     return guarded([&] {
         checked(h);
+        h->adj.ready = false;
         require(accel != nullptr, "null output pointer");
         if (!h->local_a) {
             h->local_a = static_cast<float*>(device_alloc(3U * h->N * sizeof(float), "acceleration field"));
@@ -601,6 +683,7 @@ CFDX_API int cfdx_lbm_device_local_acceleration(cfdx_lbm* h, float** accel) {
 CFDX_API int cfdx_lbm_set_solid_fraction(cfdx_lbm* h, const float* ns, int where) {
     return guarded([&] {
         checked(h);
+        h->adj.ready = false;
         if (!ns) {
             device_free(h->ns);
             h->ns = nullptr;
@@ -618,6 +701,7 @@ CFDX_API int cfdx_lbm_set_solid_fraction(cfdx_lbm* h, const float* ns, int where
 CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* h, const float* scale) {
     return guarded([&] {
         checked(h);
+        h->adj.ready = false;
         require(h->key.storage == kStoreF16S, "storage scales apply to CFDX_STORE_F16S only");
         if (!scale) {
             default_scales(h);
@@ -639,6 +723,7 @@ CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* h, const float* scale) {
 CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
     return guarded([&] {
         checked(h);
+        h->adj.ready = false;
         const dim3 g = h->grid(), b = h->step_block();
         LbmArgs a = h->args();
         for (std::uint64_t i = 0; i < count; ++i) {
@@ -847,6 +932,223 @@ CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int variant)
                     "the paired-cell kernel needs FP32/FP16 storage, an even nx, q*cells < 2^32 and block_x a "
                     "multiple of 32");
         h->choose_variant();
+    });
+}
+
+CFDX_API int cfdx_lbm_set_tau(cfdx_lbm* h, float tau) {
+    return guarded([&] {
+        checked(h);
+        require(tau > 0.5F && std::isfinite(tau), "LBM tau must be > 0.5 for positive viscosity");
+        if (h->key.collision == kTRT && h->cfg.trt_tau_minus <= 0.0F)
+            require(h->cfg.trt_magic > 0.0F, "TRT needs trt_magic > 0");
+        h->adj.ready = false;
+        h->cfg.tau = tau;
+    });
+}
+
+// ------------------------------------------------------------------ adjoint
+namespace {
+
+// Grows an adjoint buffer to at least `bytes` (contents not kept).
+void adjoint_buffer(void** p, std::size_t* have, std::size_t bytes, const char* what) {
+    if (*have >= bytes && *p) return;
+    device_free(*p);
+    *p = nullptr;
+    *have = 0;
+    *p = device_alloc(bytes, what);
+    *have = bytes;
+}
+
+void adjoint_reserve(cfdx_lbm* h, std::uint64_t steps, std::uint32_t interval) {
+    auto& A = h->adj;
+    const std::uint64_t segments = (steps + interval - 1U) / interval;
+    // interval - 1 recompute frames; the forward pass also uses two of them
+    // as its ping-pong buffers.
+    const std::uint64_t frames = std::max<std::uint64_t>(std::min<std::uint64_t>(interval, steps) - 1U, 2U);
+    const std::size_t lam_es = h->key.storage == kStoreF64 ? 8U : 4U;
+    const dim3 g = h->grid();
+    const std::size_t blocks = static_cast<std::size_t>(g.x) * g.y * g.z;
+    try {
+        adjoint_buffer(&A.checkpoints, &A.checkpoint_bytes, segments * h->f_bytes, "adjoint checkpoints");
+        adjoint_buffer(&A.frames, &A.frame_bytes, frames * h->f_bytes, "adjoint recompute frames");
+        adjoint_buffer(&A.lam, &A.lam_bytes, static_cast<std::size_t>(h->key.q) * h->N * lam_es, "adjoint lattice");
+        if (!A.grad_ns) A.grad_ns = static_cast<double*>(device_alloc(h->N * sizeof(double), "n_s gradient"));
+        if (A.tau_blocks < blocks) {
+            device_free(A.tau_partials);
+            A.tau_partials = nullptr;
+            A.tau_partials = static_cast<double*>(device_alloc(blocks * sizeof(double), "tau gradient partials"));
+            A.tau_blocks = blocks;
+        }
+        if (!A.tau_out) A.tau_out = static_cast<double*>(device_alloc(sizeof(double), "tau gradient"));
+    } catch (...) {
+        release_adjoint(h);
+        throw;
+    }
+}
+
+void* adjoint_frame(cfdx_lbm* h, std::uint64_t segment, std::uint64_t k) {
+    char* base = k == 0U ? static_cast<char*>(h->adj.checkpoints) + segment * h->f_bytes
+                         : static_cast<char*>(h->adj.frames) + (k - 1U) * h->f_bytes;
+    return base;
+}
+
+} // namespace
+
+CFDX_API int cfdx_lbm_adjoint_forward(cfdx_lbm* h, std::uint64_t steps, std::uint32_t interval) {
+    return guarded([&] {
+        checked(h);
+        require(steps >= 1U && interval >= 1U, "adjoint forward needs steps >= 1 and a checkpoint interval >= 1");
+        require(!h->key.les, "the adjoint does not cover Smagorinsky LES (its tau depends on the populations)");
+        require(!h->moving_walls, "the adjoint does not cover moving walls");
+        require(h->key.narrow, "the adjoint needs q * cells < 2^32");
+        h->adj.ready = false;
+        adjoint_reserve(h, steps, interval);
+        auto& A = h->adj;
+        A.t0 = h->t;
+        A.steps = steps;
+        A.interval = interval;
+        // The forward runs the out-of-place kernel the reverse sweep
+        // recomputes with, so every recomputed frame equals the forward's
+        // state bit for bit.  Checkpoints and frames all keep the layout of
+        // parity P0 (gather with P0's tables, scatter with P0 ^ 1's); the
+        // very last step scatters into the live lattice in the layout its
+        // final time step reads.
+        const int es = storage_bytes(h->key.storage);
+        const int P0 = static_cast<int>(A.t0 & 1U);
+        const std::uint64_t t_end = A.t0 + steps;
+        const dim3 g = h->grid(), b = h->block();
+        check_cuda(cudaMemcpyAsync(adjoint_frame(h, 0, 0), h->f, h->f_bytes, cudaMemcpyDeviceToDevice, h->stream),
+                   "cudaMemcpyAsync (adjoint checkpoint)");
+        const std::uint64_t segments = (steps + interval - 1U) / interval;
+        void* work[2] = {adjoint_frame(h, 0, 1), adjoint_frame(h, 0, 2)};
+        void* cur = adjoint_frame(h, 0, 0);
+        for (std::uint64_t s = 0; s < segments; ++s) {
+            const std::uint64_t len = std::min<std::uint64_t>(interval, steps - s * interval);
+            for (std::uint64_t k = 1; k <= len; ++k) {
+                const bool last = s + 1U == segments && k == len;
+                void* dst = last ? h->f : (k == len ? adjoint_frame(h, s + 1U, 0) : work[k & 1U]);
+                const int scatter_parity = last && static_cast<int>(t_end & 1U) != P0 ? P0 : (P0 ^ 1);
+                check_cuda(launch_step_oop(h->key, h->args_at(cur, es, P0), h->args_at(dst, es, scatter_parity), g,
+                                           b, h->stream),
+                           "adjoint forward kernel");
+                cur = dst;
+                ++h->t;
+            }
+        }
+        A.t_end = h->t;
+        A.ready = true;
+    });
+}
+
+CFDX_API int cfdx_lbm_adjoint_backward(cfdx_lbm* h, const float* g_rho, const float* g_ux, const float* g_uy,
+                                       const float* g_uz, int where, double* grad_ns, int grad_where,
+                                       double* grad_tau) {
+    return guarded([&] {
+        checked(h);
+        auto& A = h->adj;
+        require(A.ready && h->t == A.t_end,
+                "cfdx_lbm_adjoint_backward needs cfdx_lbm_adjoint_forward first, with no call that changes the "
+                "lattice or its parameters in between");
+        require(g_ux && g_uy && g_uz, "null velocity gradient");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        require(grad_where == CFDX_HOST || grad_where == CFDX_DEVICE, "grad_where must be CFDX_HOST or CFDX_DEVICE");
+        const std::size_t N = h->N;
+        const float *gr = g_rho, *gx = g_ux, *gy = g_uy, *gz = g_uz;
+        if (where == CFDX_HOST) {
+            if (!A.seed) A.seed = static_cast<float*>(device_alloc(4U * N * sizeof(float), "adjoint seed staging"));
+            const float* src[4] = {g_rho, g_ux, g_uy, g_uz};
+            for (int k = 0; k < 4; ++k)
+                if (src[k]) upload(h, A.seed + k * N, src[k], N * sizeof(float), CFDX_HOST);
+            gr = g_rho ? A.seed : nullptr;
+            gx = A.seed + N;
+            gy = A.seed + 2 * N;
+            gz = A.seed + 3 * N;
+        }
+        // One tau partial per block of the adjoint grid (the launch shape may
+        // have changed since the forward pass).
+        const dim3 g = h->grid(), b = h->block();
+        const std::size_t blocks = static_cast<std::size_t>(g.x) * g.y * g.z;
+        if (A.tau_blocks < blocks) {
+            device_free(A.tau_partials);
+            A.tau_partials = nullptr;
+            A.tau_blocks = 0;
+            A.tau_partials = static_cast<double*>(device_alloc(blocks * sizeof(double), "tau gradient partials"));
+            A.tau_blocks = blocks;
+        }
+        check_cuda(cudaMemsetAsync(A.grad_ns, 0, N * sizeof(double), h->stream), "cudaMemsetAsync");
+        check_cuda(cudaMemsetAsync(A.tau_partials, 0, blocks * sizeof(double), h->stream), "cudaMemsetAsync");
+
+        const int es = storage_bytes(h->key.storage);
+        const int lam_es = h->key.storage == kStoreF64 ? 8 : 4;
+        const double tau = h->cfg.tau;
+        AdjointArgs X{};
+        X.grad_ns = A.grad_ns;
+        X.tau_partials = A.tau_partials;
+        X.dwp = -1.0 / (tau * tau);
+        if (h->key.collision == kBGK) {
+            X.dwm = X.dwp;
+        } else if (h->cfg.trt_tau_minus > 0.0F) {
+            X.dwm = 0.0;
+        } else {
+            const double lam = h->cfg.trt_magic, q = lam + 0.5 * (tau - 0.5);
+            X.dwm = lam / (q * q);
+        }
+        X.g_rho = gr;
+        X.g_ux = gx;
+        X.g_uy = gy;
+        X.g_uz = gz;
+        X.f = h->args();
+        X.l = h->args_at(A.lam, lam_es, 1);
+        check_cuda(launch_adjoint_seed(h->key, X, g, b, h->stream), "adjoint seed kernel");
+        const std::uint64_t segments = (A.steps + A.interval - 1U) / A.interval;
+        std::uint64_t parity = 0;
+        for (std::uint64_t s = segments; s-- > 0U;) {
+            const std::uint64_t ts = A.t0 + s * A.interval;
+            const std::uint64_t len = std::min<std::uint64_t>(A.interval, A.t0 + A.steps - ts);
+            const int P = static_cast<int>(A.t0 & 1U); // every checkpoint and frame keeps the layout of t0
+            for (std::uint64_t k = 1; k < len; ++k)
+                check_cuda(launch_step_oop(h->key, h->args_at(adjoint_frame(h, s, k - 1U), es, P),
+                                           h->args_at(adjoint_frame(h, s, k), es, P ^ 1), g, b, h->stream),
+                           "adjoint recompute kernel");
+            for (std::uint64_t k = len; k >= 1U; --k) {
+                X.f = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
+                X.l = h->args_at(A.lam, lam_es, static_cast<int>(parity & 1U));
+                check_cuda(launch_adjoint_step(h->key, X, g, b, h->stream), "adjoint step kernel");
+                ++parity;
+            }
+        }
+        check_cuda(launch_sum_partials(A.tau_partials, blocks, A.tau_out, h->stream), "adjoint tau reduction");
+        if (grad_ns) {
+            const cudaMemcpyKind kind = grad_where == CFDX_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+            check_cuda(cudaMemcpyAsync(grad_ns, A.grad_ns, N * sizeof(double), kind, h->stream),
+                       "cudaMemcpyAsync (n_s gradient)");
+            if (grad_where == CFDX_HOST) h->d2h += N * sizeof(double);
+        }
+        double tau_host = 0.0;
+        check_cuda(cudaMemcpyAsync(&tau_host, A.tau_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+                   "cudaMemcpyAsync (tau gradient)");
+        h->d2h += sizeof(double);
+        h->sync();
+        if (grad_tau) *grad_tau = tau_host;
+    });
+}
+
+CFDX_API int cfdx_lbm_adjoint_memory(cfdx_lbm* h, std::size_t* bytes) {
+    return guarded([&] {
+        checked(h);
+        require(bytes != nullptr, "null output pointer");
+        const auto& A = h->adj;
+        *bytes = A.checkpoint_bytes + A.frame_bytes + A.lam_bytes + (A.grad_ns ? h->N * sizeof(double) : 0U) +
+                 A.tau_blocks * sizeof(double) + (A.tau_out ? sizeof(double) : 0U) +
+                 (A.seed ? 4U * h->N * sizeof(float) : 0U);
+    });
+}
+
+CFDX_API int cfdx_lbm_adjoint_release(cfdx_lbm* h) {
+    return guarded([&] {
+        checked(h);
+        if (h->stream) h->sync();
+        release_adjoint(h);
     });
 }
 

@@ -1,0 +1,335 @@
+// Discrete adjoint of the gray-LBM step (sm_100a).
+//
+// Forward (logical form): x^t(n,i) = C(x^{t-1}(n - c_i))_i, or C(x^{t-1}(n))_{opp i}
+// when n - c_i is a wall, with C the per-cell TRT/BGK + Guo collision followed
+// by gray partial bounce-back C_i = (1 - n_s) f*_i + n_s x_{opp i} (Walsh,
+// Burwinkle & Saar 2009).  Its adjoint runs backwards in time:
+//   mu(m,k) = lambda^t(m + c_k, k)   (lambda^t(m, opp k) at a wall)
+//   lambda^{t-1}(m,.) = [dC/dx at x^{t-1}(m,.)]^T mu(m,.)
+//   dJ/dn_s(m) += mu . dC/dn_s,   dJ/dtau += mu . dC/dtau
+//
+// Storage.  Kept with its directions flipped, nu(n,i) = lambda(n, opp i), the
+// adjoint streams exactly like the forward: nu is gathered by a pull along
+// +c (gathered nu_in(m,k) = mu(m, opp k)) and written back by the same
+// in-place Esoteric-Pull scatter, bounce-back links included.  So the adjoint
+// lattice uses the forward's slot tables, at its own parity, and the
+// kernels below reuse the forward's gather/scatter unchanged.
+//
+// Forward states.  The Jacobian and dC/dn_s need the full incoming
+// populations of every step.  The forward keeps a checkpoint every k steps;
+// the reverse sweep recomputes a segment out of place (k_step_oop: read one
+// frame, write the next, so each frame stays readable), then walks it
+// backwards.  A frame written by k_step_oop is gather-ready at the same
+// parity as its source: the step gathers with the tables of parity P and
+// scatters with those of parity P ^ 1, which is exactly the layout parity P
+// reads (the slots a parity-P^1 gather would read).
+//
+// Jacobian of C at x (rho = sum x, u~ = j / rho, u = u~ + a/2, F = rho a):
+//   dC_i/dx_k = (1 - n_s) [A_ik + dG_i/drho + dG_i/du . (c_k - u~) / rho] + n_s delta(opp i, k)
+//   A_ik = delta_ik (1 - (w+ + w-)/2) - delta(opp i, k) (w+ - w-)/2
+//   G_i  = w+ feq+_i + w- feq-_i + (1 - w+/2) F+_i + (1 - w-/2) F-_i
+// G is linear in rho at fixed u, so with the moments of mu
+//   m0 = sum w mu, m = sum w mu c, M = sum w mu c c^T
+// the contractions are
+//   P  = sum mu dG/drho = w+ (m0 (1 - 1.5 u^2) + 4.5 u.M.u) + 3 w- m.u + g+ (9 u.M.a - 3 m0 u.a) + 3 g- m.a
+//   Vr = sum mu dG/du / rho = 9 M v - 3 m0 v + 3 w- m,   v = w+ u + g+ a
+// and in opposite-pair space (sigma = mu_i + mu_j, delta = mu_i - mu_j):
+//   lambda_i + lambda_j = (1 - n_s)(sigma (1 - w+) + 2 P - 2 Vr.u~) + n_s sigma
+//   lambda_i - lambda_j = (1 - n_s)(delta (1 - w-) + 2 Vr.c_i)     - n_s delta
+//   lambda_0            = (1 - n_s)(mu_0 (1 - w+) + P - Vr.u~)       + n_s mu_0
+// Scope: BGK/TRT, uniform or per-cell force, gray n_s, stationary walls,
+// periodic faces.  Smagorinsky LES (tau depends on the populations) and
+// moving walls are rejected by the host.
+#pragma once
+
+#include "lbm_device.cuh"
+
+namespace cfdx {
+
+// Adjoint lattice storage: FP64 next to FP64 forward storage, FP32 otherwise.
+template <class S> struct AdjointStorage {
+    using type = StF32;
+};
+template <> struct AdjointStorage<StF64> {
+    using type = StF64;
+};
+
+// Absolute populations from what gather_loads returns (deviations for FP16).
+template <class L, class S, int D = 0>
+__device__ __forceinline__ void to_absolute(typename S::R* f) {
+    if constexpr (D < L::Q) {
+        if constexpr (S::delta) f[D] += typename S::R(L::w(D));
+        to_absolute<L, S, D + 1>(f);
+    }
+}
+
+template <class R> struct CellState {
+    R rho, irho, utx, uty, utz, ux, uy, uz, ax, ay, az;
+};
+
+template <class L, class R>
+__device__ __forceinline__ CellState<R> cell_state(const LbmArgs& a, u32 n, const R* x, bool force) {
+    CellState<R> c;
+    R r = x[0], jx = R(0), jy = R(0), jz = R(0);
+#pragma unroll
+    for (int d = 1; d < L::Q; ++d) {
+        r += x[d];
+        jx += R(L::cx(d)) * x[d];
+        jy += R(L::cy(d)) * x[d];
+        jz += R(L::cz(d)) * x[d];
+    }
+    c.rho = r;
+    c.irho = rcp_unbiased(r);
+    c.utx = jx * c.irho;
+    c.uty = jy * c.irho;
+    c.utz = jz * c.irho;
+    c.ax = c.ay = c.az = R(0);
+    if (force) cell_acceleration<R>(a, n, c.ax, c.ay, c.az);
+    c.ux = c.utx + R(0.5) * c.ax;
+    c.uy = c.uty + R(0.5) * c.ay;
+    c.uz = c.utz + R(0.5) * c.az;
+    return c;
+}
+
+// One cell of the adjoint step: nin are the gathered adjoint values
+// (nin_k = mu_{opp k}), x the forward's incoming populations (absolute).
+// Writes the flipped result nout (nout_i = lambda_{opp i}) and this cell's
+// dJ/dn_s and dJ/dtau contributions.
+template <class L, class R>
+__device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x, const R* nin, R* nout, bool force,
+                                             R dwp, R dwm, double& g_ns, double& g_tau) {
+    const CellState<R> c = cell_state<L, R>(a, n, x, force);
+    const R tau = R(a.tau);
+    const R wp = rcp(tau);
+    const R wm = omega_minus_of<R>(a, tau, wp);
+    const R gp = R(1) - R(0.5) * wp, gm = R(1) - R(0.5) * wm;
+    const R ns = a.ns ? R(a.ns[n]) : R(0);
+    const R ux = c.ux, uy = c.uy, uz = c.uz;
+    const R Fx = c.rho * c.ax, Fy = c.rho * c.ay, Fz = c.rho * c.az;
+    const R base = R(1) - R(1.5) * (ux * ux + uy * uy + uz * uz);
+    const R uF = ux * Fx + uy * Fy + uz * Fz;
+
+    // rest direction: forward pieces and adjoint moments
+    constexpr R w0 = R(L::w(0));
+    const R mu0 = nin[0];
+    const R neq0 = x[0] - w0 * c.rho * base;
+    const R F0 = -R(3) * w0 * uF;
+    const R fs0 = x[0] - wp * neq0 + gp * F0;
+    R gns = mu0 * (x[0] - fs0);
+    R gtp = mu0 * (-neq0 - R(0.5) * F0);
+    R gtm = R(0);
+    R m0 = w0 * mu0, mx = R(0), my = R(0), mz = R(0);
+    R Mxx = R(0), Myy = R(0), Mzz = R(0), Mxy = R(0), Mxz = R(0), Myz = R(0);
+    R ms[L::PAIRS], md[L::PAIRS];
+#pragma unroll
+    for (int p = 0; p < L::PAIRS; ++p) {
+        const int i = 2 * p + 1, j = i + 1;
+        const R cx = R(L::cx(i)), cy = R(L::cy(i)), cz = R(L::cz(i));
+        const R w = R(L::w(i));
+        // mu_i = nin_j, mu_j = nin_i
+        const R sg = nin[i] + nin[j];
+        const R dl = nin[j] - nin[i];
+        ms[p] = sg;
+        md[p] = dl;
+        const R ws = w * sg, wd = w * dl;
+        m0 += ws;
+        mx += cx * wd;
+        my += cy * wd;
+        mz += cz * wd;
+        Mxx += cx * cx * ws;
+        Myy += cy * cy * ws;
+        Mzz += cz * cz * ws;
+        Mxy += cx * cy * ws;
+        Mxz += cx * cz * ws;
+        Myz += cy * cz * ws;
+        // forward pair quantities for dC/dn_s and dC/dtau
+        const R s = x[i] + x[j], d = x[i] - x[j];
+        const R cu = cx * ux + cy * uy + cz * uz;
+        const R cF = cx * Fx + cy * Fy + cz * Fz;
+        const R sneq = s - R(2) * w * c.rho * (base + R(4.5) * cu * cu);
+        const R dneq = d - R(6) * w * c.rho * cu;
+        const R sF = R(2) * w * (R(9) * cu * cF - R(3) * uF);
+        const R dF = R(6) * w * cF;
+        const R sst = s - wp * sneq + gp * sF;
+        const R dst = d - wm * dneq + gm * dF;
+        gns += R(0.5) * (sg * (s - sst) - dl * (d + dst));
+        gtp += R(0.5) * sg * (-sneq - R(0.5) * sF);
+        gtm += R(0.5) * dl * (-dneq - R(0.5) * dF);
+    }
+    g_ns = double(gns);
+    g_tau = double((R(1) - ns) * (dwp * gtp + dwm * gtm));
+
+    const R ax = c.ax, ay = c.ay, az = c.az;
+    const R Mux = Mxx * ux + Mxy * uy + Mxz * uz;
+    const R Muy = Mxy * ux + Myy * uy + Myz * uz;
+    const R Muz = Mxz * ux + Myz * uy + Mzz * uz;
+    const R Max = Mxx * ax + Mxy * ay + Mxz * az;
+    const R May = Mxy * ax + Myy * ay + Myz * az;
+    const R Maz = Mxz * ax + Myz * ay + Mzz * az;
+    const R P = wp * (m0 * base + R(4.5) * (ux * Mux + uy * Muy + uz * Muz)) +
+                R(3) * wm * (mx * ux + my * uy + mz * uz) +
+                gp * (R(9) * (ux * Max + uy * May + uz * Maz) - R(3) * m0 * (ux * ax + uy * ay + uz * az)) +
+                R(3) * gm * (mx * ax + my * ay + mz * az);
+    const R vx = wp * ux + gp * ax, vy = wp * uy + gp * ay, vz = wp * uz + gp * az;
+    const R Vx = R(9) * (wp * Mux + gp * Max) - R(3) * m0 * vx + R(3) * wm * mx;
+    const R Vy = R(9) * (wp * Muy + gp * May) - R(3) * m0 * vy + R(3) * wm * my;
+    const R Vz = R(9) * (wp * Muz + gp * Maz) - R(3) * m0 * vz + R(3) * wm * mz;
+    const R Vu = Vx * c.utx + Vy * c.uty + Vz * c.utz;
+    const R keep = R(1) - ns;
+    nout[0] = keep * (mu0 * (R(1) - wp) + P - Vu) + ns * mu0;
+    const R even0 = R(2) * (P - Vu);
+#pragma unroll
+    for (int p = 0; p < L::PAIRS; ++p) {
+        const int i = 2 * p + 1, j = i + 1;
+        const R ls = keep * (ms[p] * (R(1) - wp) + even0) + ns * ms[p];
+        const R ld = keep * (md[p] * (R(1) - wm) +
+                             R(2) * (R(L::cx(i)) * Vx + R(L::cy(i)) * Vy + R(L::cz(i)) * Vz)) -
+                     ns * md[p];
+        // lambda_i = (ls + ld) / 2 is stored in slot j (flipped), lambda_j in slot i
+        nout[i] = R(0.5) * (ls - ld);
+        nout[j] = R(0.5) * (ls + ld);
+    }
+}
+
+// Deterministic FP64 block sum of v added to partials[block] (every thread of
+// the block must call it).
+__device__ __forceinline__ void block_accumulate(double v, double* partials) {
+    __shared__ double warp_sum[32];
+    const unsigned tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const unsigned nthreads = blockDim.x * blockDim.y * blockDim.z;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffU, v, off);
+    if ((tid & 31U) == 0U) warp_sum[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0U) {
+        double s = 0.0;
+        for (unsigned w = 0; w < (nthreads + 31U) / 32U; ++w) s += warp_sum[w];
+        const unsigned b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        partials[b] += s;
+    }
+}
+
+// Out-of-place forward step for the segment recompute: gather from f (parity
+// P tables, source frame), collide exactly as k_step does, scatter through s
+// (parity P ^ 1 tables, destination frame).
+template <class L, class S, bool FLAGS, bool GRAY>
+__global__ void __launch_bounds__(128, step_min_blocks<L, S>()) k_step_oop(const __grid_constant__ LbmArgs f,
+                                                                          const __grid_constant__ LbmArgs s) {
+    using R = typename S::R;
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
+    if (x >= f.nx || y >= f.ny) return;
+    const u32 n = (z * f.ny + y) * f.nx + x;
+    std::uint8_t flag = 0;
+    if constexpr (FLAGS) {
+        flag = f.flags[n];
+        if (flag & kFlagTypeMask) return;
+    }
+    const Nbr o = make_nbr(f, x, y, z);
+    R fin[L::Q];
+    gather_loads<L, S, FLAGS, true, S::scaled>(f, n, o, flag, fin);
+    if constexpr (S::scaled) {
+        if (f.has_force)
+            collide_scaled<L, false, GRAY, true>(f, n, fin);
+        else
+            collide_scaled<L, false, GRAY, false>(f, n, fin);
+    } else {
+        if (f.has_force)
+            collide<L, R, false, GRAY, true, S::delta>(f, n, fin);
+        else
+            collide<L, R, false, GRAY, false, S::delta>(f, n, fin);
+    }
+    scatter<L, S, true, S::scaled>(s, n, o, fin);
+}
+
+// lambda^T from dJ/d(rho, u) of the state the forward left: for every fluid
+// cell, lambda_k = g_rho + g_u . (c_k - u~) / rho (u = u~ + a/2 is what the
+// macroscopic output reports), scattered flipped into the adjoint lattice
+// through A.l (parity 1 tables, so the first adjoint step gathers at parity 0).
+template <class L, class S, bool FLAGS>
+__global__ void __launch_bounds__(128) k_adjoint_seed(const __grid_constant__ AdjointArgs A) {
+    using R = typename S::R;
+    using LS = typename AdjointStorage<S>::type;
+    const LbmArgs& f = A.f;
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
+    if (x >= f.nx || y >= f.ny) return;
+    const u32 n = (z * f.ny + y) * f.nx + x;
+    std::uint8_t flag = 0;
+    if constexpr (FLAGS) {
+        flag = f.flags[n];
+        if (flag & kFlagTypeMask) return;
+    }
+    const Nbr o = make_nbr(f, x, y, z);
+    R xin[L::Q];
+    gather_loads<L, S, FLAGS, true, false>(f, n, o, flag, xin);
+    to_absolute<L, S>(xin);
+    const CellState<R> c = cell_state<L, R>(f, n, xin, false);
+    const R gr = A.g_rho ? R(A.g_rho[n]) : R(0);
+    const R gx = R(A.g_ux[n]) * c.irho, gy = R(A.g_uy[n]) * c.irho, gz = R(A.g_uz[n]) * c.irho;
+    const R g0 = gr - (gx * c.utx + gy * c.uty + gz * c.utz);
+    R nout[L::Q];
+    nout[0] = g0;
+#pragma unroll
+    for (int p = 0; p < L::PAIRS; ++p) {
+        const int i = 2 * p + 1, j = i + 1;
+        const R cg = R(L::cx(i)) * gx + R(L::cy(i)) * gy + R(L::cz(i)) * gz;
+        nout[i] = g0 - cg; // lambda_j, stored flipped in slot i
+        nout[j] = g0 + cg; // lambda_i
+    }
+    scatter<L, LS, true, false>(A.l, n, o, nout);
+}
+
+// One reverse step: gather the adjoint (A.l, in place at its parity) and the
+// forward's incoming populations of the matching forward step (A.f, a frame),
+// apply the transposed collision, scatter the adjoint back, accumulate the
+// gradients.
+template <class L, class S, bool FLAGS>
+__global__ void __launch_bounds__(128) k_adjoint_step(const __grid_constant__ AdjointArgs A) {
+    using R = typename S::R;
+    using LS = typename AdjointStorage<S>::type;
+    const LbmArgs& f = A.f;
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
+    double g_tau = 0.0;
+    if (x < f.nx && y < f.ny) {
+        const u32 n = (z * f.ny + y) * f.nx + x;
+        std::uint8_t flag = 0;
+        bool fluid = true;
+        if constexpr (FLAGS) {
+            flag = f.flags[n];
+            fluid = (flag & kFlagTypeMask) == 0;
+        }
+        if (fluid) {
+            const Nbr o = make_nbr(f, x, y, z);
+            R xin[L::Q], nin[L::Q], nout[L::Q];
+            gather_loads<L, S, FLAGS, true, false>(f, n, o, flag, xin);
+            gather_loads<L, LS, FLAGS, true, false>(A.l, n, o, flag, nin);
+            to_absolute<L, S>(xin);
+            double g_ns = 0.0;
+            adjoint_cell<L, R>(f, n, xin, nin, nout, f.has_force != 0, R(A.dwp), R(A.dwm), g_ns, g_tau);
+            scatter<L, LS, true, false>(A.l, n, o, nout);
+            A.grad_ns[n] += g_ns;
+        }
+    }
+    block_accumulate(g_tau, A.tau_partials);
+}
+
+// Sum of `count` FP64 partials in a fixed order (one block).
+static __global__ void __launch_bounds__(256) k_sum_partials(const double* partials, std::size_t count, double* out) {
+    __shared__ double part[256];
+    double s = 0.0;
+    for (std::size_t i = threadIdx.x; i < count; i += blockDim.x) s += partials[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (unsigned w = blockDim.x / 2U; w > 0U; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0U) *out = part[0];
+}
+
+} // namespace cfdx

@@ -63,6 +63,19 @@ struct LbmArgs {
     float inv_scale[27];
 };
 
+// Parameters of the adjoint kernels (lbm_adjoint.cuh).
+struct AdjointArgs {
+    LbmArgs f;            // forward state read by the step (a recompute frame or the live lattice)
+    LbmArgs l;            // adjoint lattice at the adjoint parity (updated in place)
+    double* grad_ns;      // N, dJ/dn_s accumulated over steps
+    double* tau_partials; // one per block, dJ/dtau accumulated over steps
+    double dwp, dwm;      // d omega+ / d tau, d omega- / d tau
+    const float* g_rho;   // seed: dJ/drho of the final state (N, may be null)
+    const float* g_ux;    // seed: dJ/du of the final state (N each)
+    const float* g_uy;
+    const float* g_uz;
+};
+
 // Initial state for k_init.
 struct InitSpec {
     int kind; // 0 uniform, 1 Taylor-Green, 2 per-cell fields

@@ -8,6 +8,12 @@ template struct Launcher<kStoreF32>;
 
 namespace cfdx {
 
+// The FP64 partial-sum kernel of the adjoint does not depend on the storage type.
+cudaError_t launch_sum_partials(const double* partials, std::size_t count, double* out, cudaStream_t s) {
+    k_sum_partials<<<1, 256, 0, s>>>(partials, count, out);
+    return cudaGetLastError();
+}
+
 // Flag preparation does not depend on the storage type; it lives here once.
 cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out, dim3 g, dim3 b,
                                  cudaStream_t s) {

@@ -41,6 +41,11 @@ template <int STORAGE> struct Launcher {
                                cudaStream_t s);
     static cudaError_t reduce(const KernelKey& k, const LbmArgs& a, double* partials, int blocks, double* out,
                               cudaStream_t s);
+    // Adjoint (lbm_adjoint.cuh); all three need 32-bit slot offsets.
+    static cudaError_t step_oop(const KernelKey& k, const LbmArgs& src, const LbmArgs& dst, dim3 grid, dim3 block,
+                                cudaStream_t s);
+    static cudaError_t adjoint_seed(const KernelKey& k, const AdjointArgs& a, dim3 grid, dim3 block, cudaStream_t s);
+    static cudaError_t adjoint_step(const KernelKey& k, const AdjointArgs& a, dim3 grid, dim3 block, cudaStream_t s);
 };
 
 cudaError_t launch_step(const KernelKey& k, const LbmArgs& a, dim3 grid, dim3 block, cudaStream_t s);
@@ -51,6 +56,11 @@ cudaError_t launch_macro(const KernelKey& k, const LbmArgs& a, void* rho, void* 
 cudaError_t launch_logical(const KernelKey& k, const LbmArgs& a, float* out, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t launch_reduce(const KernelKey& k, const LbmArgs& a, double* partials, int blocks, double* out,
                           cudaStream_t s);
+cudaError_t launch_step_oop(const KernelKey& k, const LbmArgs& src, const LbmArgs& dst, dim3 grid, dim3 block,
+                            cudaStream_t s);
+cudaError_t launch_adjoint_seed(const KernelKey& k, const AdjointArgs& a, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t launch_adjoint_step(const KernelKey& k, const AdjointArgs& a, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t launch_sum_partials(const double* partials, std::size_t count, double* out, cudaStream_t s);
 cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out, dim3 grid,
                                  dim3 block, cudaStream_t s);
 

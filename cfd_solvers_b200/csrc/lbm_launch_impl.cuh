@@ -2,6 +2,7 @@
 // one storage type.  Included by lbm_kernels_{f32,f16s,f64}.cu only.
 #pragma once
 
+#include "lbm_adjoint.cuh"
 #include "lbm_device.cuh"
 #include "lbm_launch.h"
 #include "lbm_step_x2.cuh"
@@ -139,6 +140,48 @@ cudaError_t Launcher<STORAGE>::reduce(const KernelKey& k, const LbmArgs& a, doub
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         k_reduce_final<<<1, kReduceThreads, 0, s>>>(partials, blocks, out);
+        return cudaGetLastError();
+    });
+}
+
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::step_oop(const KernelKey& k, const LbmArgs& src, const LbmArgs& dst, dim3 g, dim3 b,
+                                        cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        if (k.flags)
+            k.gray ? k_step_oop<L, S, true, true><<<g, b, 0, s>>>(src, dst)
+                   : k_step_oop<L, S, true, false><<<g, b, 0, s>>>(src, dst);
+        else
+            k.gray ? k_step_oop<L, S, false, true><<<g, b, 0, s>>>(src, dst)
+                   : k_step_oop<L, S, false, false><<<g, b, 0, s>>>(src, dst);
+        return cudaGetLastError();
+    });
+}
+
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::adjoint_seed(const KernelKey& k, const AdjointArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        if (k.flags)
+            k_adjoint_seed<L, S, true><<<g, b, 0, s>>>(a);
+        else
+            k_adjoint_seed<L, S, false><<<g, b, 0, s>>>(a);
+        return cudaGetLastError();
+    });
+}
+
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::adjoint_step(const KernelKey& k, const AdjointArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        if (k.flags)
+            k_adjoint_step<L, S, true><<<g, b, 0, s>>>(a);
+        else
+            k_adjoint_step<L, S, false><<<g, b, 0, s>>>(a);
         return cudaGetLastError();
     });
 }

@@ -15,6 +15,7 @@ duration of the call.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import math
 from dataclasses import dataclass
 from typing import NamedTuple, Optional
@@ -178,6 +179,11 @@ class EsotericPullCudaSolver:
                 raise ValueError(f"{name} size mismatch: expected {count}, got {array.numel()}")
             if not array.is_contiguous():
                 raise ValueError(f"{name} must be contiguous")
+            import torch
+
+            # The library reads device buffers on its own stream: finish the
+            # work that produced them on torch's stream first.
+            torch.cuda.current_stream(array.device).synchronize()
             return ctypes.c_void_p(array.data_ptr()), B.DEVICE, array
         a = _host(array, dtype, count, name)
         return ctypes.c_void_p(a.ctypes.data), B.HOST, a
@@ -358,6 +364,59 @@ class EsotericPullCudaSolver:
     def set_launch_shape(self, block_x: int = 0, block_y: int = 0, variant: int = 0):
         """Threads per block and step-kernel variant (0 auto, 1 one cell, 2 paired cells)."""
         self._call("cfdx_lbm_set_launch_shape", int(block_x), int(block_y), int(variant))
+
+    def set_tau(self, tau: float):
+        """Symmetric relaxation time of the following steps (the adjoint's dJ/dtau variable)."""
+        self._call("cfdx_lbm_set_tau", float(tau))
+        self._config = dataclasses.replace(self._config, tau=float(tau))
+
+    # ------------------------------------------------------ discrete adjoint
+    def adjoint_forward(self, steps: int, interval: int = 64):
+        """Run `steps` steps keeping a checkpoint every `interval` steps for adjoint_backward."""
+        self._call("cfdx_lbm_adjoint_forward", int(steps), int(interval))
+
+    def adjoint_backward(self, g_ux, g_uy, g_uz, g_rho=None, grad_ns_out=None):
+        """dJ/dn_s (per cell, float64) and dJ/dtau for dJ/du and dJ/drho of the final state.
+
+        Seeds are host numpy arrays or CUDA tensors (N float32 each).  The
+        n_s gradient is returned as a numpy array, or written into
+        `grad_ns_out` (a float64 CUDA tensor of N elements) when given.
+        """
+        n = self._cells
+        keep = []
+        ptrs = []
+        where = None
+        for name, g in (("g_rho", g_rho), ("g_ux", g_ux), ("g_uy", g_uy), ("g_uz", g_uz)):
+            if g is None:
+                ptrs.append(None)
+                continue
+            if _is_device(g):
+                g = g.float().contiguous()
+            ptr, w, k = self._pointer(g, np.float32, n, name)
+            if where is not None and w != where:
+                raise ValueError("adjoint seeds must all be host arrays or all device tensors")
+            where = w
+            keep.append(k)
+            ptrs.append(ptr)
+        tau = ctypes.c_double()
+        if grad_ns_out is not None:
+            if not _is_device(grad_ns_out) or grad_ns_out.numel() != n or not grad_ns_out.is_contiguous():
+                raise ValueError("grad_ns_out must be a contiguous CUDA tensor of N float64 values")
+            self._call("cfdx_lbm_adjoint_backward", *ptrs, where, ctypes.c_void_p(grad_ns_out.data_ptr()), B.DEVICE,
+                       ctypes.byref(tau))
+            return grad_ns_out, tau.value
+        out = np.zeros(n, np.float64)
+        self._call("cfdx_lbm_adjoint_backward", *ptrs, where, ctypes.c_void_p(out.ctypes.data), B.HOST,
+                   ctypes.byref(tau))
+        return out, tau.value
+
+    def adjoint_memory(self) -> int:
+        n = ctypes.c_size_t()
+        self._call("cfdx_lbm_adjoint_memory", ctypes.byref(n))
+        return n.value
+
+    def adjoint_release(self):
+        self._call("cfdx_lbm_adjoint_release")
 
     def stream(self) -> int:
         p = ctypes.c_void_p()

@@ -240,6 +240,44 @@ CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, 
  * serialised by the caller. */
 CFDX_API int cfdx_lbm_reduce_noalloc(cfdx_lbm* lbm, double* out);
 
+/* Symmetric relaxation time (> 0.5) for the following steps; the adjoint's
+ * dJ/dtau is taken with respect to it.  Reference: InPlaceLbmConfig::tau,
+ * esoteric_pull.hpp:20-29 (fixed at construction there). */
+CFDX_API int cfdx_lbm_set_tau(cfdx_lbm* lbm, float tau);
+
+/* ---- Discrete adjoint of the gray-LBM step (no reference counterpart: the
+ * reference has neither gray LBM nor an adjoint).  Scope: BGK/TRT, uniform
+ * or per-cell force, gray n_s, stationary walls, periodic faces; Smagorinsky
+ * LES and moving walls are rejected with CFDX_ERR_INVALID; q*cells < 2^32.
+ *
+ * cfdx_lbm_adjoint_forward: runs `steps` steps from the current state like
+ * cfdx_lbm_step, keeping a device copy of the lattice every `interval` steps
+ * (ceil(steps/interval) copies, in the storage precision) plus
+ * max(interval-1, 2) recompute frames.  It runs the out-of-place form of the
+ * step that the reverse sweep recomputes with, so the recomputed states equal
+ * the forward's bit for bit; the final state equals cfdx_lbm_step(steps)'s to
+ * within the last bit of the arithmetic type. */
+CFDX_API int cfdx_lbm_adjoint_forward(cfdx_lbm* lbm, uint64_t steps, uint32_t interval);
+
+/* Reverse sweep for an objective J of the final state, given dJ/drho (N
+ * floats, may be NULL) and dJ/du_x,y,z (N floats each) of the fields
+ * cfdx_lbm_macroscopic reports (u includes +a/2), all on `where` (host or
+ * device).  Writes dJ/dn_s per cell (N doubles, 0 on walls; `grad_where`;
+ * NULL skips) and dJ/dtau (*grad_tau, host; NULL skips).  Recomputes each
+ * segment from its checkpoint; the lattice and its parameters must not have
+ * changed since cfdx_lbm_adjoint_forward (else CFDX_ERR_INVALID).  FP32
+ * adjoint arithmetic for FP32/FP16 storage, FP64 for FP64 storage; the
+ * gradients are accumulated in FP64.  May be called again with another seed. */
+CFDX_API int cfdx_lbm_adjoint_backward(cfdx_lbm* lbm, const float* g_rho, const float* g_ux, const float* g_uy,
+                                       const float* g_uz, int where, double* grad_ns, int grad_where,
+                                       double* grad_tau);
+
+/* Device bytes the adjoint's buffers hold. */
+CFDX_API int cfdx_lbm_adjoint_memory(cfdx_lbm* lbm, size_t* bytes);
+
+/* Frees the adjoint's buffers (checkpoints, frames, adjoint lattice). */
+CFDX_API int cfdx_lbm_adjoint_release(cfdx_lbm* lbm);
+
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */
