@@ -371,6 +371,63 @@ def differentiation_variants(torch, cs, device, full=True):
     return out
 
 
+# ------------------------------------------------------- precision study
+def precision_study(torch, cs, device, shape=(512, 256, 256), steps=20000, seed=1):
+    """FP16-shifted and FP32 storage against FP64 storage (FP64 arithmetic) on the same GPU.
+
+    D3Q19 TRT (magic 3/16) channel, periodic in x, no-slip y/z walls, a seeded
+    random sphere pack (radii uniform in [4, 12], 10 % solid), gx = 1e-6,
+    tau 0.55, from rest.  The FP64-storage run is the at-scale FP64 reference
+    (the same kernels in double, pinned to the FP64 CPU oracle at 1e-12 on
+    small lattices).  Errors over fluid cells: L2 relative and max relative
+    (to max |u|) of u; mass drift of each run.
+    """
+    import ctypes
+
+    from cfd_solvers_b200 import bindings as B
+    from cfd_solvers_b200.cases import sphere_pack
+
+    nx, ny, nz = shape
+    cells = nx * ny * nz
+    flags = sphere_pack(nx, ny, nz, fraction=0.10, rmin=4.0, rmax=12.0, seed=seed)
+    fluid = torch.from_numpy(flags == 0).to(device)
+    runs = {}
+    for storage in ("fp64", "fp32", "fp16s"):
+        s = cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(
+            nx=nx, ny=ny, nz=nz, tau=0.55, collision="trt", trt_magic=3.0 / 16.0, acceleration_x=1e-6,
+            storage=storage, device=device))
+        try:
+            s.set_flags(flags)
+            s.initialize_uniform()
+            m0 = s.reduce()["mass"]
+            ms = time_steps(torch, s, steps)
+            red = s.reduce()
+            u = torch.empty((3, cells), dtype=torch.float64, device=device)
+            rho = torch.empty(cells, dtype=torch.float64, device=device)
+            torch.cuda.synchronize()
+            s.library.call("cfdx_lbm_macroscopic_f64", s.handle, ctypes.c_void_p(rho.data_ptr()),
+                           *[ctypes.c_void_p(u[k].data_ptr()) for k in range(3)], B.DEVICE)
+        finally:
+            s.close()
+        runs[storage] = {"u": u, "glups": cells * steps / (ms / 1e3) / 1e9, "mass0": m0, "mass": red["mass"],
+                         "nonfinite": red["nonfinite"]}
+    ref = runs["fp64"]["u"] * fluid
+    ref_norm = float(torch.linalg.vector_norm(ref))
+    ref_max = float(ref.abs().max())
+    out = {"workload": f"D3Q19 TRT channel {nx}x{ny}x{nz}, sphere pack 10% (r 4-12, seed {seed}), gx 1e-6, "
+                       f"tau 0.55, {steps} steps from rest",
+           "solid_fraction": float(np.count_nonzero(flags) / cells), "max_u_fp64": ref_max}
+    for storage, r in runs.items():
+        e = r["u"] * fluid - ref
+        out[storage] = {
+            "glups": r["glups"], "mass_drift_rel": (r["mass"] - r["mass0"]) / r["mass0"], "nonfinite": r["nonfinite"],
+            "u_l2_rel_vs_fp64": float(torch.linalg.vector_norm(e)) / ref_norm,
+            "u_max_rel_vs_fp64": float(e.abs().max()) / ref_max,
+        }
+    out["fp16s_speedup_vs_fp32"] = runs["fp16s"]["glups"] / runs["fp32"]["glups"]
+    return out
+
+
 # ----------------------------------------------------------- reference (CPU)
 def cpu_reference_sample(n, warmup, steps, threads=0):
     """The reference's CPU path on the closest feature set: EsotericPullSolver<D3Q19>

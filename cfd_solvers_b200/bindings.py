@@ -35,6 +35,8 @@ BGK = 0
 TRT = 1
 HOST = 0
 DEVICE = 1
+ROUND_NEAREST = 0
+ROUND_STOCHASTIC = 1
 FLUID = 0
 WALL = 1
 MAX_WALL_IDS = 16
@@ -78,6 +80,8 @@ class cfdx_lbm_config(ctypes.Structure):
         ("trt_magic", ctypes.c_float),
         ("trt_tau_minus", ctypes.c_float),
         ("device", ctypes.c_int),
+        ("fp16_rounding", ctypes.c_int),
+        ("rounding_seed", ctypes.c_uint32),
     ]
 
 

@@ -98,6 +98,16 @@ void copy_error(char* out, std::size_t cap, const std::string& text) {
 
 int storage_bytes(int storage) { return storage == kStoreF64 ? 8 : (storage == kStoreF16S ? 2 : 4); }
 
+// lowbias32 integer hash (C. Wellons, "hash-prospector", public domain).
+std::uint32_t lowbias32(std::uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
 // Reference Smagorinsky coefficient 16 sqrt(2) / (3 pi^2), evaluated in float
 // as include/cfd/solvers/lbm/esoteric_pull.hpp:94-95 does.
 float reference_les_k() {
@@ -166,7 +176,21 @@ struct cfdx_lbm {
         float* seed = nullptr; // 4*N staging for host-side seeds
     } adj;
 
-    LbmArgs args() const { return args_at(f, storage_bytes(key.storage), static_cast<int>(t & 1U)); }
+    LbmArgs args() const {
+        LbmArgs a = args_at(f, storage_bytes(key.storage), static_cast<int>(t & 1U));
+        a.round_seed = round_seed(t);
+        return a;
+    }
+    // Seed of the FP16 rounding bits of the step that starts at time step ts.
+    std::uint32_t round_seed(std::uint64_t ts) const {
+        return lowbias32(static_cast<std::uint32_t>(ts) * 0x9E3779B9U +
+                         lowbias32(cfg.rounding_seed ^ static_cast<std::uint32_t>(ts >> 32)));
+    }
+    // Slot tables and rounding seed of the step that starts at time step ts.
+    void set_step(LbmArgs& a, std::uint64_t ts) const {
+        set_parity(a, static_cast<int>(ts & 1U));
+        a.round_seed = round_seed(ts);
+    }
     // Arguments for a lattice of this handle's shape at `lattice` (element
     // size `es` bytes), with the slot tables of parity `odd`.
     LbmArgs args_at(void* lattice, int elem_bytes, int odd) const {
@@ -202,6 +226,10 @@ struct cfdx_lbm {
         a.ay = cfg.acceleration_y;
         a.az = cfg.acceleration_z;
         std::memcpy(a.wall_u, wall_u, sizeof wall_u);
+        const bool stochastic = key.storage == kStoreF16S && cfg.fp16_rounding == CFDX_ROUND_STOCHASTIC;
+        a.round_mask = stochastic ? 0xffffffffU : 0U;
+        a.round_add = stochastic ? 0U : 0x10001000U; // nearest: half a step in both 13-bit fields
+        a.round_seed = 0U;
         for (int d = 0; d < 27; ++d) {
             a.scale[d] = scale[d] == 0.0F ? 1.0F : scale[d];
             a.inv_scale[d] = 1.0F / a.scale[d];
@@ -494,6 +522,8 @@ CFDX_API int cfdx_lbm_config_default(cfdx_lbm_config* c) {
         c->trt_magic = 3.0F / 16.0F;
         c->trt_tau_minus = 0.0F;
         c->device = 0;
+        c->fp16_rounding = CFDX_ROUND_STOCHASTIC;
+        c->rounding_seed = 0U;
     });
 }
 
@@ -511,6 +541,8 @@ CFDX_API int cfdx_lbm_create(const cfdx_lbm_config* config, cfdx_lbm** out, char
         require(c.collision == CFDX_BGK || c.collision == CFDX_TRT, "collision must be CFDX_BGK or CFDX_TRT");
         require(c.storage == CFDX_STORE_F32 || c.storage == CFDX_STORE_F64 || c.storage == CFDX_STORE_F16S,
                 "unknown storage");
+        require(c.fp16_rounding == CFDX_ROUND_NEAREST || c.fp16_rounding == CFDX_ROUND_STOCHASTIC,
+                "fp16_rounding must be CFDX_ROUND_NEAREST or CFDX_ROUND_STOCHASTIC");
         require(std::isfinite(c.acceleration_x) && std::isfinite(c.acceleration_y) && std::isfinite(c.acceleration_z),
                 "acceleration must be finite");
         if (c.collision == CFDX_TRT)
@@ -727,7 +759,7 @@ CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
         const dim3 g = h->grid(), b = h->step_block();
         LbmArgs a = h->args();
         for (std::uint64_t i = 0; i < count; ++i) {
-            h->set_parity(a, static_cast<int>(h->t & 1U));
+            h->set_step(a, h->t);
             check_cuda(launch_step(h->key, a, g, b, h->stream), "step kernel");
             ++h->t;
         }
@@ -1028,8 +1060,9 @@ CFDX_API int cfdx_lbm_adjoint_forward(cfdx_lbm* h, std::uint64_t steps, std::uin
                 const bool last = s + 1U == segments && k == len;
                 void* dst = last ? h->f : (k == len ? adjoint_frame(h, s + 1U, 0) : work[k & 1U]);
                 const int scatter_parity = last && static_cast<int>(t_end & 1U) != P0 ? P0 : (P0 ^ 1);
-                check_cuda(launch_step_oop(h->key, h->args_at(cur, es, P0), h->args_at(dst, es, scatter_parity), g,
-                                           b, h->stream),
+                LbmArgs src = h->args_at(cur, es, P0);
+                src.round_seed = h->round_seed(h->t);
+                check_cuda(launch_step_oop(h->key, src, h->args_at(dst, es, scatter_parity), g, b, h->stream),
                            "adjoint forward kernel");
                 cur = dst;
                 ++h->t;
@@ -1106,10 +1139,13 @@ CFDX_API int cfdx_lbm_adjoint_backward(cfdx_lbm* h, const float* g_rho, const fl
             const std::uint64_t ts = A.t0 + s * A.interval;
             const std::uint64_t len = std::min<std::uint64_t>(A.interval, A.t0 + A.steps - ts);
             const int P = static_cast<int>(A.t0 & 1U); // every checkpoint and frame keeps the layout of t0
-            for (std::uint64_t k = 1; k < len; ++k)
-                check_cuda(launch_step_oop(h->key, h->args_at(adjoint_frame(h, s, k - 1U), es, P),
-                                           h->args_at(adjoint_frame(h, s, k), es, P ^ 1), g, b, h->stream),
+            for (std::uint64_t k = 1; k < len; ++k) {
+                LbmArgs src = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
+                src.round_seed = h->round_seed(ts + k - 1U); // the forward's step at this time
+                check_cuda(launch_step_oop(h->key, src, h->args_at(adjoint_frame(h, s, k), es, P ^ 1), g, b,
+                                           h->stream),
                            "adjoint recompute kernel");
+            }
             for (std::uint64_t k = len; k >= 1U; --k) {
                 X.f = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
                 X.l = h->args_at(A.lam, lam_es, static_cast<int>(parity & 1U));

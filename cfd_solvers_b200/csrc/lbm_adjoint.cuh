@@ -240,7 +240,8 @@ __global__ void __launch_bounds__(128, step_min_blocks<L, S>()) k_step_oop(const
         else
             collide<L, R, false, GRAY, false, S::delta>(f, n, fin);
     }
-    scatter<L, S, true, S::scaled>(s, n, o, fin);
+    // rounding bits of the forward's step at this time (seed in f)
+    scatter<L, S, true, S::scaled>(s, n, o, fin, sizeof(typename S::T) == 2 ? round_hash(f, n) : 0U);
 }
 
 // lambda^T from dJ/d(rho, u) of the state the forward left: for every fluid
@@ -279,15 +280,29 @@ __global__ void __launch_bounds__(128) k_adjoint_seed(const __grid_constant__ Ad
         nout[i] = g0 - cg; // lambda_j, stored flipped in slot i
         nout[j] = g0 + cg; // lambda_i
     }
-    scatter<L, LS, true, false>(A.l, n, o, nout);
+    scatter<L, LS, true, false>(A.l, n, o, nout, 0U);
 }
 
 // One reverse step: gather the adjoint (A.l, in place at its parity) and the
 // forward's incoming populations of the matching forward step (A.f, a frame),
 // apply the transposed collision, scatter the adjoint back, accumulate the
 // gradients.
+// Resident blocks per SM the reverse step is compiled for (register cap
+// 65536 / (128 * blocks)).  Measured on B200 (adjoint step alone): D3Q19 at 8
+// blocks (64 registers) 0.098 ms vs 0.125 uncapped at 128^3 FP32; D3Q27 at 5
+// (96 registers) 1.24 ms vs 1.43 uncapped at 256^3 FP16.
+#ifndef CFDX_ADJOINT_MIN_BLOCKS_Q19
+#define CFDX_ADJOINT_MIN_BLOCKS_Q19 8
+#endif
+#ifndef CFDX_ADJOINT_MIN_BLOCKS_Q27
+#define CFDX_ADJOINT_MIN_BLOCKS_Q27 5
+#endif
+template <class L, class S> constexpr int adjoint_min_blocks() {
+    return sizeof(typename S::T) == 8 ? 1 : (L::Q == 19 ? CFDX_ADJOINT_MIN_BLOCKS_Q19 : CFDX_ADJOINT_MIN_BLOCKS_Q27);
+}
+
 template <class L, class S, bool FLAGS>
-__global__ void __launch_bounds__(128) k_adjoint_step(const __grid_constant__ AdjointArgs A) {
+__global__ void __launch_bounds__(128, adjoint_min_blocks<L, S>()) k_adjoint_step(const __grid_constant__ AdjointArgs A) {
     using R = typename S::R;
     using LS = typename AdjointStorage<S>::type;
     const LbmArgs& f = A.f;
@@ -311,7 +326,7 @@ __global__ void __launch_bounds__(128) k_adjoint_step(const __grid_constant__ Ad
             to_absolute<L, S>(xin);
             double g_ns = 0.0;
             adjoint_cell<L, R>(f, n, xin, nin, nout, f.has_force != 0, R(A.dwp), R(A.dwm), g_ns, g_tau);
-            scatter<L, LS, true, false>(A.l, n, o, nout);
+            scatter<L, LS, true, false>(A.l, n, o, nout, 0U);
             A.grad_ns[n] += g_ns;
         }
     }

@@ -61,6 +61,12 @@ struct LbmArgs {
     float wall_u[kMaxWallIds][3];
     float scale[27];           // FP16S per-direction scale
     float inv_scale[27];
+    // FP16S store rounding: the rounding bits of cell n's stores derive from
+    // hash(n ^ round_seed) & round_mask, plus round_add (stochastic: mask ~0,
+    // add 0, seed per step; nearest: mask 0, add = half a step in each field).
+    std::uint32_t round_seed;
+    std::uint32_t round_mask;
+    std::uint32_t round_add;
 };
 
 // Parameters of the adjoint kernels (lbm_adjoint.cuh).

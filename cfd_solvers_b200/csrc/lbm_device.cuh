@@ -85,6 +85,48 @@ __device__ __forceinline__ void st(typename S::T* p, typename S::R v, const LbmA
     }
 }
 
+// ------------------------------------------------------- FP16 store rounding
+// FP16 stores go through sm_100a's cvt.rs (stochastic rounding): it converts
+// two FP32 values to an FP16 pair, adding rbits[12:0] (low half) and
+// rbits[28:16] (high half) below the FP16 mantissa and truncating.  Uniform
+// random bits make the rounding unbiased, so increments smaller than half an
+// FP16 step -- a small body force, a slow flow -- survive on average instead
+// of being rounded away every step.  Constant bits 0x1000 in both fields give
+// round-half-away-from-zero (the "nearest" mode).  The bits come from a hash
+// of the cell index and a per-step seed (LbmArgs::round_*), with one 32-bit
+// word per opposite pair: the same bits for a (cell, direction) in every
+// kernel, so the one-cell, paired and out-of-place steps stay bitwise equal.
+
+// lowbias32 integer hash (C. Wellons, "hash-prospector", public domain).
+__device__ __forceinline__ u32 round_hash(const LbmArgs& a, u32 n) {
+    u32 x = n ^ a.round_seed;
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x & a.round_mask;
+}
+
+// Rounding word of pair slot k (0: rest, p + 1: pair p) of a cell with hash h:
+// bits [12:0] round the pair's first direction 2p+1 (or the rest population),
+// bits [28:16] its second direction 2p+2.
+__device__ __forceinline__ u32 round_bits(const LbmArgs& a, u32 h, int k) {
+    return h * (0x9E3779B9U * (2U * static_cast<u32>(k) + 1U)) + a.round_add;
+}
+
+// (hi, lo) -> FP16 pair, rounded with rbits (see above).
+__device__ __forceinline__ u32 f16x2_rs(float hi, float lo, u32 rbits) {
+    u32 d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+
+// One FP16 store rounded with rbits[12:0].
+__device__ __forceinline__ void st_h16(__half* p, float v, u32 rbits) {
+    *reinterpret_cast<unsigned short*>(p) = static_cast<unsigned short>(f16x2_rs(0.0F, v, rbits));
+}
+
 // Value the kernels hold for an absolute population f of direction D.
 template <class S, class L, int D> __device__ __forceinline__ typename S::R held(typename S::R f) {
     if constexpr (S::delta) {
@@ -294,19 +336,36 @@ __device__ __forceinline__ void gather(const LbmArgs& a, u32 n, const Nbr& o, st
 //   odd step:  f[i][n] = fout_i, f[j][nb] = fout_j
 // i.e. fout_i -> pb[p][n], fout_j -> pa[p][nb].
 template <class L, class S, bool NARROW, bool RAW = false, int P = 0>
-__device__ __forceinline__ void scatter_pairs(const LbmArgs& a, u32 n, const Nbr& o, const typename S::R* fout) {
+__device__ __forceinline__ void scatter_pairs(const LbmArgs& a, u32 n, const Nbr& o, const typename S::R* fout,
+                                              u32 h) {
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
-        st<S, L, i, RAW>(Slots<S, NARROW>::at(a, false, P, n), fout[i], a);
-        st<S, L, j, RAW>(Slots<S, NARROW>::at(a, true, P, n + nbr_off<L, j>(o)), fout[j], a);
-        scatter_pairs<L, S, NARROW, RAW, P + 1>(a, n, o, fout);
+        auto* pi = Slots<S, NARROW>::at(a, false, P, n);
+        auto* pj = Slots<S, NARROW>::at(a, true, P, n + nbr_off<L, j>(o));
+        if constexpr (sizeof(typename S::T) == 2) {
+            const float vi = RAW ? fout[i] : fout[i] * a.scale[i];
+            const float vj = RAW ? fout[j] : fout[j] * a.scale[j];
+            const u32 w = f16x2_rs(vj, vi, round_bits(a, h, P + 1));
+            *reinterpret_cast<unsigned short*>(pi) = static_cast<unsigned short>(w);
+            *reinterpret_cast<unsigned short*>(pj) = static_cast<unsigned short>(w >> 16);
+        } else {
+            st<S, L, i, RAW>(pi, fout[i], a);
+            st<S, L, j, RAW>(pj, fout[j], a);
+        }
+        scatter_pairs<L, S, NARROW, RAW, P + 1>(a, n, o, fout, h);
     }
 }
 
-template <class L, class S, bool NARROW = false, bool RAW = false>
-__device__ __forceinline__ void scatter(const LbmArgs& a, u32 n, const Nbr& o, const typename S::R* fout) {
-    st<S, L, 0, RAW>(Slots<S, NARROW>::rest(a, n), fout[0], a);
-    scatter_pairs<L, S, NARROW, RAW>(a, n, o, fout);
+// h: the cell's rounding hash (round_hash; FP16 storage only).
+template <class L, class S, bool NARROW, bool RAW = false>
+__device__ __forceinline__ void scatter(const LbmArgs& a, u32 n, const Nbr& o, const typename S::R* fout, u32 h) {
+    if constexpr (sizeof(typename S::T) == 2) {
+        const float v0 = RAW ? fout[0] : fout[0] * a.scale[0];
+        st_h16(Slots<S, NARROW>::rest(a, n), v0, round_bits(a, h, 0));
+    } else {
+        st<S, L, 0, RAW>(Slots<S, NARROW>::rest(a, n), fout[0], a);
+    }
+    scatter_pairs<L, S, NARROW, RAW>(a, n, o, fout, h);
 }
 
 // ------------------------------------------------------------------ helpers
@@ -751,7 +810,8 @@ __global__ void __launch_bounds__(128, step_min_blocks<L, S>()) k_step(const __g
             else
                 collide<L, R, LES, GRAY, false, S::delta>(a, n, fin[c]);
         }
-        scatter<L, S, NARROW, S::scaled>(a, n, o, fin[c]);
+        const u32 h = sizeof(typename S::T) == 2 ? round_hash(a, n) : 0U;
+        scatter<L, S, NARROW, S::scaled>(a, n, o, fin[c], h);
     }
 }
 

@@ -55,6 +55,7 @@ template <> struct Pair<StF16> {
 // Per-thread context of one cell pair.
 struct PairCtx {
     u32 lane, x0, row, n0;
+    u32 h0, h1, h2; // FP16 rounding hashes of cells n0, n0+1 and n0+2 (lane+1's first cell)
     u32 oy[3], oz[3];
     unsigned live0_mask, live1_mask; // ballots over the warp
     bool live0, live1, valid;
@@ -124,18 +125,33 @@ __device__ __forceinline__ void pair_decode(const LbmArgs& a, const PairCtx& c, 
     }
 }
 
-// Writes the two values of one aligned word, or only the live one.
+// Writes the two values of one aligned word, or only the live one.  FP16:
+// rb holds the rounding bits of v0 in [12:0] and of v1 in [28:16] (the same
+// bits the one-cell kernel uses for these cells and this direction).
 template <class L, class S, int D>
 __device__ __forceinline__ void store_word(const LbmArgs& a, typename S::T* p, bool live0, bool live1,
-                                           typename S::R v0, typename S::R v1) {
+                                           typename S::R v0, typename S::R v1, u32 rb) {
     using V = typename Pair<S>::W;
-    if (live0 && live1) {
-        *reinterpret_cast<V*>(p) = Pair<S>::template encode<L, D>(v0, v1, a);
+    if constexpr (sizeof(typename S::T) == 2) {
+        if (live0 && live1) {
+            *reinterpret_cast<u32*>(p) = f16x2_rs(v1, v0, rb);
+        } else {
+            if (live0) st_h16(p, v0, rb);
+            if (live1) st_h16(p + 1, v1, rb >> 16);
+        }
     } else {
-        if (live0) st<S, L, D, S::scaled>(p, v0, a);
-        if (live1) st<S, L, D, S::scaled>(p + 1, v1, a);
+        if (live0 && live1) {
+            *reinterpret_cast<V*>(p) = Pair<S>::template encode<L, D>(v0, v1, a);
+        } else {
+            if (live0) st<S, L, D, S::scaled>(p, v0, a);
+            if (live1) st<S, L, D, S::scaled>(p + 1, v1, a);
+        }
     }
 }
+
+// Low (sel 0x5410) or high (0x7632) 16-bit halves of two rounding words.
+__device__ __forceinline__ u32 low_halves(u32 x, u32 y) { return __byte_perm(x, y, 0x5410); }
+__device__ __forceinline__ u32 high_halves(u32 x, u32 y) { return __byte_perm(x, y, 0x7632); }
 
 template <class L, class S, int P = 0>
 __device__ __forceinline__ void pair_stores(const LbmArgs& a, typename S::T* base, const PairCtx& c,
@@ -145,25 +161,44 @@ __device__ __forceinline__ void pair_stores(const LbmArgs& a, typename S::T* bas
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
         constexpr int s = L::cx(j);
+        constexpr bool h16 = sizeof(typename S::T) == 2;
+        // rounding words of this pair for cells n0, n0+1, n0+2 (FP16 only)
+        const u32 k0 = h16 ? round_bits(a, c.h0, P + 1) : 0U;
+        const u32 k1 = h16 ? round_bits(a, c.h1, P + 1) : 0U;
         // fout_i -> pb at the pair itself
-        store_word<L, S, i>(a, base + (a.pb_off[P] + c.n0), c.live0, c.live1, f0[i], f1[i]);
+        store_word<L, S, i>(a, base + (a.pb_off[P] + c.n0), c.live0, c.live1, f0[i], f1[i], low_halves(k0, k1));
         // fout_j -> pa at the neighbour nb = n + c_j
         const u32 rj = row_of<L, j>(c);
         if constexpr (s == 0) {
-            store_word<L, S, j>(a, base + (a.pa_off[P] + rj + c.x0), c.live0, c.live1, f0[j], f1[j]);
+            store_word<L, S, j>(a, base + (a.pa_off[P] + rj + c.x0), c.live0, c.live1, f0[j], f1[j],
+                                high_halves(k0, k1));
         } else {
             const bool next_live0 = c.lane < 31U && ((c.live0_mask >> (c.lane + 1U)) & 1U);
             const bool prev_live1 = c.lane > 0U && ((c.live1_mask >> (c.lane - 1U)) & 1U);
             const R next = __shfl_down_sync(0xffffffffU, f0[j], 1);
             typename S::T* pw = base + (a.pa_off[P] + rj + word_x(s, c.x0, a.nx));
             if (c.live1) {
-                if (next_live0)
-                    *reinterpret_cast<V*>(pw) = Pair<S>::template encode<L, j>(f1[j], next, a);
-                else
-                    st<S, L, j, S::scaled>(pw, f1[j], a);
+                if constexpr (h16) {
+                    // cells n0+1 (this thread) and n0+2 (lane+1's first cell)
+                    const u32 rb = high_halves(k1, round_bits(a, c.h2, P + 1));
+                    if (next_live0)
+                        *reinterpret_cast<u32*>(pw) = f16x2_rs(next, f1[j], rb);
+                    else
+                        st_h16(pw, f1[j], rb);
+                } else {
+                    if (next_live0)
+                        *reinterpret_cast<V*>(pw) = Pair<S>::template encode<L, j>(f1[j], next, a);
+                    else
+                        st<S, L, j, S::scaled>(pw, f1[j], a);
+                }
             }
-            if (c.live0 && !prev_live1)
-                st<S, L, j, S::scaled>(base + (a.pa_off[P] + rj + first_x(s, c.x0, a.nx)), f0[j], a);
+            if (c.live0 && !prev_live1) {
+                typename S::T* pf = base + (a.pa_off[P] + rj + first_x(s, c.x0, a.nx));
+                if constexpr (h16)
+                    st_h16(pf, f0[j], k0 >> 16);
+                else
+                    st<S, L, j, S::scaled>(pf, f0[j], a);
+            }
         }
         pair_stores<L, S, P + 1>(a, base, c, f0, f1);
     }
@@ -259,7 +294,15 @@ __global__ void __launch_bounds__(128, pair_min_blocks<S>()) k_step_x2(const __g
     if (c.live0) relax(c.n0, f0);
     if (c.live1) relax(c.n0 + 1U, f1);
 
-    store_word<L, S, 0>(a, base + (a.rest_off + c.n0), c.live0, c.live1, f0[0], f1[0]);
+    if constexpr (sizeof(T) == 2) {
+        c.h0 = round_hash(a, c.n0);
+        c.h1 = round_hash(a, c.n0 + 1U);
+        c.h2 = __shfl_down_sync(0xffffffffU, c.h0, 1); // lane 31's value is never used
+    } else {
+        c.h0 = c.h1 = c.h2 = 0U;
+    }
+    store_word<L, S, 0>(a, base + (a.rest_off + c.n0), c.live0, c.live1, f0[0], f1[0],
+                        low_halves(round_bits(a, c.h0, 0), round_bits(a, c.h1, 0)));
     pair_stores<L, S>(a, base, c, f0, f1);
 }
 

@@ -45,6 +45,8 @@ class InPlaceLbmConfig:
     trt_magic: float = 3.0 / 16.0
     trt_tau_minus: float = 0.0    # > 0: fixed antisymmetric relaxation time
     device: int = 0
+    fp16_rounding: str = "stochastic"  # FP16S stores: "stochastic" (unbiased) | "nearest"
+    rounding_seed: int = 0
 
     @property
     def q(self) -> int:
@@ -137,6 +139,10 @@ class EsotericPullCudaSolver:
         c.trt_magic = config.trt_magic
         c.trt_tau_minus = config.trt_tau_minus
         c.device = config.device
+        if config.fp16_rounding not in ("stochastic", "nearest"):
+            raise ValueError("fp16_rounding must be stochastic or nearest")
+        c.fp16_rounding = B.ROUND_STOCHASTIC if config.fp16_rounding == "stochastic" else B.ROUND_NEAREST
+        c.rounding_seed = int(config.rounding_seed) & 0xFFFFFFFF
         handle = ctypes.c_void_p()
         err = ctypes.create_string_buffer(1024)
         status = self._lib.raw.cfdx_lbm_create(ctypes.byref(c), ctypes.byref(handle), err, len(err))

@@ -85,6 +85,14 @@ typedef struct cfdx_lbm cfdx_lbm; /* opaque handle */
 
 /* Solver configuration.  The first eight fields are the reference's
  * InPlaceLbmConfig (esoteric_pull.hpp:20-29); the rest extend it. */
+/* Rounding of FP16-shifted population stores.  STOCHASTIC (sm_100a
+ * cvt.rs with per-cell, per-step hashed random bits) keeps increments
+ * smaller than half an FP16 step from being lost every step (small forces,
+ * slow flows) -- an unbiased rounding, reproducible run to run for a given
+ * seed.  NEAREST rounds half away from zero (the reference codec's rule,
+ * compressed_pull.hpp:27,35). */
+enum { CFDX_ROUND_NEAREST = 0, CFDX_ROUND_STOCHASTIC = 1 };
+
 typedef struct cfdx_lbm_config {
     size_t nx, ny, nz;
     float tau;               /* > 0.5 */
@@ -99,6 +107,8 @@ typedef struct cfdx_lbm_config {
     float trt_magic;         /* TRT magic parameter Lambda (default 3/16) */
     float trt_tau_minus;     /* > 0: fixed antisymmetric relaxation time instead of Lambda */
     int device;              /* CUDA device ordinal */
+    int fp16_rounding;       /* CFDX_STORE_F16S stores: CFDX_ROUND_STOCHASTIC (default) or CFDX_ROUND_NEAREST */
+    uint32_t rounding_seed;  /* seed of the stochastic rounding bits */
 } cfdx_lbm_config;
 
 /* Handle information. */

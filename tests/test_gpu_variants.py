@@ -1,7 +1,8 @@
 """The paired-cell step kernel against the one-cell kernel (GPU).
 
-Both variants evaluate the same per-cell collision with the same rounding,
-so after any number of steps their populations must agree bit for bit.
+Both variants evaluate the same per-cell collision with the same rounding
+(FP16 stores: the same stochastic rounding bits per cell and direction), so
+after any number of steps their populations must agree bit for bit.
 The cases cover partial warps (nx/2 not a multiple of 32), multi-warp rows,
 the x-periodic wrap of shifted word accesses, random walls next to fluid
 cells inside one thread's pair, moving walls, gray cells and both parities.
@@ -20,9 +21,10 @@ def run(cs, variant, q, shape, storage, flags_kind, gray, steps, seed=11):
     nx, ny, nz = shape
     n = nx * ny * nz
     rng = np.random.default_rng(seed)
+    storage, _, rounding = storage.partition(":")
     cfg = cs.InPlaceLbmConfig(nx=nx, ny=ny, nz=nz, tau=0.6, lattice={19: "d3q19", 27: "d3q27"}[q],
                               storage=storage, collision="trt", smagorinsky_les=True, smagorinsky_cs=0.1,
-                              acceleration_x=1e-5)
+                              acceleration_x=1e-5, fp16_rounding=rounding or "stochastic")
     with cs.EsotericPullCudaSolver(cfg) as s:
         s.set_launch_shape(0, 0, variant)
         if flags_kind == "random":
@@ -43,7 +45,7 @@ def run(cs, variant, q, shape, storage, flags_kind, gray, steps, seed=11):
 
 
 @pytest.mark.parametrize("q", [19, 27])
-@pytest.mark.parametrize("storage", ["fp32", "fp16s"])
+@pytest.mark.parametrize("storage", ["fp32", "fp16s", "fp16s:nearest"])
 @pytest.mark.parametrize("shape", SHAPES, ids=[f"{a}x{b}x{c}" for a, b, c in SHAPES])
 @pytest.mark.parametrize("flags_kind, gray", [(None, False), ("random", False), ("cavity", True)])
 @pytest.mark.parametrize("steps", [5, 6])
