@@ -50,6 +50,10 @@ def parse_args(argv=None):
     p.add_argument("--no-variants", action="store_true", help="skip the FP16S / D3Q27 side measurements")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-differentiation", action="store_true",
+                   help="skip the adjoint workloads (128^3 D3Q19 FP32 and 256^3 D3Q27 FP16 gray TRT)")
+    p.add_argument("--no-precision", action="store_true",
+                   help="skip the 512x256x256 sphere-pack FP16/FP32/FP64 precision study (20000 steps)")
     return p.parse_args(argv)
 
 
@@ -428,6 +432,26 @@ def precision_study(torch, cs, device, shape=(512, 256, 256), steps=20000, seed=
     return out
 
 
+def target_summary(line, variants):
+    """The three headline targets, read off the measurements above."""
+    t = {"fp32_d3q19_512_roofline_frac": line["roofline"]["frac"]}
+    if "d3q19_fp16s" in variants:
+        t["fp16_speedup_vs_fp32_cavity512"] = variants["d3q19_fp16s"]["speedup_vs_fp32"]
+    p = variants.get("precision_study")
+    if p:
+        t["fp16_speedup_vs_fp32_sphere_pack"] = p["fp16s_speedup_vs_fp32"]
+        t["fp16_u_l2_rel_vs_fp64_sphere_pack"] = p["fp16s"]["u_l2_rel_vs_fp64"]
+        t["fp32_u_l2_rel_vs_fp64_sphere_pack"] = p["fp32"]["u_l2_rel_vs_fp64"]
+    d = variants.get("differentiation")
+    if d:
+        c4 = d["gray_d3q19_128_fp32"]
+        t["adjoint_over_forward_d3q19_128_fp32"] = c4["adjoint_over_forward"]
+        t["grad_vs_fd_rel_l2_fp32_adjoint"] = c4["fd_check"]["fp32_adjoint_vs_fd"]["rel_l2"]
+        if "gray_d3q27_256_fp16s" in d:
+            t["adjoint_over_forward_d3q27_256_fp16s"] = d["gray_d3q27_256_fp16s"]["adjoint_over_forward"]
+    return t
+
+
 # ----------------------------------------------------------- reference (CPU)
 def cpu_reference_sample(n, warmup, steps, threads=0):
     """The reference's CPU path on the closest feature set: EsotericPullSolver<D3Q19>
@@ -578,11 +602,16 @@ def main(argv=None):
             d27 = measure_variant(torch, cs, n, "d3q27", "fp32", vs, local_rank)
             d27["roofline_frac"] = d27["achieved_gbs"] / hbm_peak()[0]
             variants["d3q27_fp32"] = d27
+        if not args.no_differentiation:
+            variants["differentiation"] = differentiation_variants(torch, cs, local_rank)
+        if not args.no_precision:
+            variants["precision_study"] = precision_study(torch, cs, local_rank)
 
     if rank == 0:
         line["e2e"] = e2e
         if variants:
             line["variants"] = variants
+            line["targets"] = target_summary(line, variants)
         if not args.no_cpu_baseline and world == 1:
             edge = min(n, 256)
             mlups, secs, cores = cpu_reference_sample(edge, 1, 5)

@@ -133,6 +133,7 @@ struct cfdx_lbm {
     void* f = nullptr;
     std::size_t f_bytes = 0;
     std::uint8_t* flags = nullptr; // internal flag bytes
+    std::uint32_t* wall_mask = nullptr; // wall-link bits of near-wall fluid cells
     float* local_a = nullptr;
     float* ns = nullptr;
     float* macro_scratch = nullptr; // 4*N floats, lazily allocated
@@ -203,6 +204,7 @@ struct cfdx_lbm {
         a.rest_off = 0U;
         set_parity(a, odd);
         a.flags = key.flags ? flags : nullptr;
+        a.wall_mask = key.flags ? wall_mask : nullptr;
         a.ax_field = local_a;
         a.ay_field = local_a ? local_a + N : nullptr;
         a.az_field = local_a ? local_a + 2 * N : nullptr;
@@ -225,6 +227,14 @@ struct cfdx_lbm {
         a.ax = cfg.acceleration_x;
         a.ay = cfg.acceleration_y;
         a.az = cfg.acceleration_z;
+        a.tau_f = static_cast<float>(a.tau);
+        a.omega_minus_f = static_cast<float>(a.omega_minus);
+        a.trt_magic_f = static_cast<float>(a.trt_magic);
+        a.les_k_f = static_cast<float>(a.les_k);
+        a.ax_f = static_cast<float>(a.ax);
+        a.ay_f = static_cast<float>(a.ay);
+        a.az_f = static_cast<float>(a.az);
+        a.minus_mode = a.omega_minus > 0.0 ? 1 : (a.omega_minus < 0.0 ? -1 : 0);
         std::memcpy(a.wall_u, wall_u, sizeof wall_u);
         const bool stochastic = key.storage == kStoreF16S && cfg.fp16_rounding == CFDX_ROUND_STOCHASTIC;
         a.round_mask = stochastic ? 0xffffffffU : 0U;
@@ -371,6 +381,7 @@ void release(cfdx_lbm* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     device_free(h->f);
     device_free(h->flags);
+    device_free(h->wall_mask);
     device_free(h->local_a);
     device_free(h->ns);
     device_free(h->macro_scratch);
@@ -644,6 +655,8 @@ CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int wher
             return;
         }
         if (!h->flags) h->flags = static_cast<std::uint8_t*>(device_alloc(h->N, "flag field"));
+        if (!h->wall_mask)
+            h->wall_mask = static_cast<std::uint32_t*>(device_alloc(h->N * sizeof(std::uint32_t), "wall-link masks"));
         std::uint8_t* user = static_cast<std::uint8_t*>(device_alloc(h->N, "flag staging"));
         try {
             upload(h, user, flags, h->N, where);
@@ -658,7 +671,8 @@ CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int wher
                 scan = reinterpret_cast<const std::uint8_t*>(host_copy.data());
             }
             h->moving_walls = std::any_of(scan, scan + h->N, [](std::uint8_t v) { return v >= CFDX_MOVING_WALL_MIN; });
-            check_cuda(launch_prepare_flags(h->key.q, h->args(), user, h->flags, h->grid(), h->block(), h->stream),
+            check_cuda(launch_prepare_flags(h->key.q, h->args(), user, h->flags, h->wall_mask, h->grid(), h->block(),
+                                            h->stream),
                        "flag preparation kernel");
             h->sync();
         } catch (...) {

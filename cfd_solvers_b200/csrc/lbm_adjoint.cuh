@@ -63,6 +63,14 @@ __device__ __forceinline__ void to_absolute(typename S::R* f) {
     }
 }
 
+// Compile-time loop: f(std::integral_constant<int, k>) for k in [B, E).
+template <int B, int E, class F> __device__ __forceinline__ void static_for(F&& f) {
+    if constexpr (B < E) {
+        f(std::integral_constant<int, B>{});
+        static_for<B + 1, E>(f);
+    }
+}
+
 template <class R> struct CellState {
     R rho, irho, utx, uty, utz, ux, uy, uz, ax, ay, az;
 };
@@ -71,13 +79,17 @@ template <class L, class R>
 __device__ __forceinline__ CellState<R> cell_state(const LbmArgs& a, u32 n, const R* x, bool force) {
     CellState<R> c;
     R r = x[0], jx = R(0), jy = R(0), jz = R(0);
-#pragma unroll
-    for (int d = 1; d < L::Q; ++d) {
-        r += x[d];
-        jx += R(L::cx(d)) * x[d];
-        jy += R(L::cy(d)) * x[d];
-        jz += R(L::cz(d)) * x[d];
-    }
+    static_for<0, L::PAIRS>([&](auto P) {
+        constexpr int i = 2 * decltype(P)::value + 1, j = i + 1;
+        const R s = x[i] + x[j], d = x[i] - x[j];
+        r += s;
+        if constexpr (L::cx(i) > 0) jx += d;
+        if constexpr (L::cx(i) < 0) jx -= d;
+        if constexpr (L::cy(i) > 0) jy += d;
+        if constexpr (L::cy(i) < 0) jy -= d;
+        if constexpr (L::cz(i) > 0) jz += d;
+        if constexpr (L::cz(i) < 0) jz -= d;
+    });
     c.rho = r;
     c.irho = rcp_unbiased(r);
     c.utx = jx * c.irho;
@@ -99,7 +111,7 @@ template <class L, class R>
 __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x, const R* nin, R* nout, bool force,
                                              R dwp, R dwm, double& g_ns, double& g_tau) {
     const CellState<R> c = cell_state<L, R>(a, n, x, force);
-    const R tau = R(a.tau);
+    const R tau = p_tau<R>(a);
     const R wp = rcp(tau);
     const R wm = omega_minus_of<R>(a, tau, wp);
     const R gp = R(1) - R(0.5) * wp, gm = R(1) - R(0.5) * wm;
@@ -121,10 +133,10 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
     R m0 = w0 * mu0, mx = R(0), my = R(0), mz = R(0);
     R Mxx = R(0), Myy = R(0), Mzz = R(0), Mxy = R(0), Mxz = R(0), Myz = R(0);
     R ms[L::PAIRS], md[L::PAIRS];
-#pragma unroll
-    for (int p = 0; p < L::PAIRS; ++p) {
-        const int i = 2 * p + 1, j = i + 1;
-        const R cx = R(L::cx(i)), cy = R(L::cy(i)), cz = R(L::cz(i));
+    static_for<0, L::PAIRS>([&](auto PP) {
+        constexpr int p = decltype(PP)::value;
+        constexpr int i = 2 * p + 1, j = i + 1;
+        constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
         const R w = R(L::w(i));
         // mu_i = nin_j, mu_j = nin_i
         const R sg = nin[i] + nin[j];
@@ -133,19 +145,19 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
         md[p] = dl;
         const R ws = w * sg, wd = w * dl;
         m0 += ws;
-        mx += cx * wd;
-        my += cy * wd;
-        mz += cz * wd;
-        Mxx += cx * cx * ws;
-        Myy += cy * cy * ws;
-        Mzz += cz * cz * ws;
-        Mxy += cx * cy * ws;
-        Mxz += cx * cz * ws;
-        Myz += cy * cz * ws;
+        mx += signed_sum<cx, 0, 0>(wd, R(0), R(0));
+        my += signed_sum<cy, 0, 0>(wd, R(0), R(0));
+        mz += signed_sum<cz, 0, 0>(wd, R(0), R(0));
+        if constexpr (cx != 0) Mxx += ws;
+        if constexpr (cy != 0) Myy += ws;
+        if constexpr (cz != 0) Mzz += ws;
+        Mxy += signed_sum<cx * cy, 0, 0>(ws, R(0), R(0));
+        Mxz += signed_sum<cx * cz, 0, 0>(ws, R(0), R(0));
+        Myz += signed_sum<cy * cz, 0, 0>(ws, R(0), R(0));
         // forward pair quantities for dC/dn_s and dC/dtau
         const R s = x[i] + x[j], d = x[i] - x[j];
-        const R cu = cx * ux + cy * uy + cz * uz;
-        const R cF = cx * Fx + cy * Fy + cz * Fz;
+        const R cu = cdot<L, i>(ux, uy, uz);
+        const R cF = cdot<L, i>(Fx, Fy, Fz);
         const R sneq = s - R(2) * w * c.rho * (base + R(4.5) * cu * cu);
         const R dneq = d - R(6) * w * c.rho * cu;
         const R sF = R(2) * w * (R(9) * cu * cF - R(3) * uF);
@@ -155,7 +167,7 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
         gns += R(0.5) * (sg * (s - sst) - dl * (d + dst));
         gtp += R(0.5) * sg * (-sneq - R(0.5) * sF);
         gtm += R(0.5) * dl * (-dneq - R(0.5) * dF);
-    }
+    });
     g_ns = double(gns);
     g_tau = double((R(1) - ns) * (dwp * gtp + dwm * gtm));
 
@@ -178,17 +190,15 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
     const R keep = R(1) - ns;
     nout[0] = keep * (mu0 * (R(1) - wp) + P - Vu) + ns * mu0;
     const R even0 = R(2) * (P - Vu);
-#pragma unroll
-    for (int p = 0; p < L::PAIRS; ++p) {
-        const int i = 2 * p + 1, j = i + 1;
+    static_for<0, L::PAIRS>([&](auto PP) {
+        constexpr int p = decltype(PP)::value;
+        constexpr int i = 2 * p + 1, j = i + 1;
         const R ls = keep * (ms[p] * (R(1) - wp) + even0) + ns * ms[p];
-        const R ld = keep * (md[p] * (R(1) - wm) +
-                             R(2) * (R(L::cx(i)) * Vx + R(L::cy(i)) * Vy + R(L::cz(i)) * Vz)) -
-                     ns * md[p];
+        const R ld = keep * (md[p] * (R(1) - wm) + R(2) * cdot<L, i>(Vx, Vy, Vz)) - ns * md[p];
         // lambda_i = (ls + ld) / 2 is stored in slot j (flipped), lambda_j in slot i
         nout[i] = R(0.5) * (ls - ld);
         nout[j] = R(0.5) * (ls + ld);
-    }
+    });
 }
 
 // Deterministic FP64 block sum of v added to partials[block] (every thread of
@@ -273,13 +283,12 @@ __global__ void __launch_bounds__(128) k_adjoint_seed(const __grid_constant__ Ad
     const R g0 = gr - (gx * c.utx + gy * c.uty + gz * c.utz);
     R nout[L::Q];
     nout[0] = g0;
-#pragma unroll
-    for (int p = 0; p < L::PAIRS; ++p) {
-        const int i = 2 * p + 1, j = i + 1;
-        const R cg = R(L::cx(i)) * gx + R(L::cy(i)) * gy + R(L::cz(i)) * gz;
+    static_for<0, L::PAIRS>([&](auto PP) {
+        constexpr int i = 2 * decltype(PP)::value + 1, j = i + 1;
+        const R cg = cdot<L, i>(gx, gy, gz);
         nout[i] = g0 - cg; // lambda_j, stored flipped in slot i
         nout[j] = g0 + cg; // lambda_i
-    }
+    });
     scatter<L, LS, true, false>(A.l, n, o, nout, 0U);
 }
 

@@ -45,6 +45,10 @@ struct LbmArgs {
     std::uint32_t pa_off[13];
     std::uint32_t pb_off[13];
     const std::uint8_t* flags; // internal flags or nullptr
+    // Per fluid cell next to a wall: bit 2p set when direction 2p+1's source
+    // n + c_{2p+2} is a wall, bit 2p+1 when direction 2p+2's source n + c_{2p+1}
+    // is (computed once with the flags; nullptr without flags).
+    const std::uint32_t* wall_mask;
     const float* ax_field;     // per-cell acceleration components or nullptr
     const float* ay_field;
     const float* az_field;
@@ -58,6 +62,11 @@ struct LbmArgs {
     double trt_magic;
     double les_k;              // Smagorinsky K (0 = off)
     double ax, ay, az;         // uniform acceleration
+    // FP32 copies of the parameters above for the FP32/FP16 kernels (no
+    // double-to-float conversion per thread) and the omega- rule as an int:
+    // 1 fixed (omega_minus), 0 TRT magic, -1 BGK.
+    float tau_f, omega_minus_f, trt_magic_f, les_k_f, ax_f, ay_f, az_f;
+    int minus_mode;
     float wall_u[kMaxWallIds][3];
     float scale[27];           // FP16S per-direction scale
     float inv_scale[27];

@@ -145,6 +145,58 @@ template <class S, class L> __device__ __forceinline__ typename S::R absolute(ty
     }
 }
 
+// ------------------------------------------------ lattice-vector products
+// c_D . (x, y, z) for a direction with components in {-1, 0, 1}, written as
+// the signed sum of its nonzero terms (positive terms first).  The generic
+// form c_x * x + c_y * y + c_z * z costs a multiply-add per zero component:
+// IEEE semantics (NaN, signed zero) forbid folding x * 0 away.
+template <int A, int B, int C, class R> __device__ __forceinline__ R signed_sum(R x, R y, R z) {
+    if constexpr (A > 0) {
+        R r = x;
+        if constexpr (B > 0) r = r + y;
+        if constexpr (C > 0) r = r + z;
+        if constexpr (B < 0) r = r - y;
+        if constexpr (C < 0) r = r - z;
+        return r;
+    } else if constexpr (B > 0) {
+        R r = y;
+        if constexpr (C > 0) r = r + z;
+        if constexpr (A < 0) r = r - x;
+        if constexpr (C < 0) r = r - z;
+        return r;
+    } else if constexpr (C > 0) {
+        R r = z;
+        if constexpr (A < 0) r = r - x;
+        if constexpr (B < 0) r = r - y;
+        return r;
+    } else if constexpr (A < 0) {
+        R r = -x;
+        if constexpr (B < 0) r = r - y;
+        if constexpr (C < 0) r = r - z;
+        return r;
+    } else if constexpr (B < 0) {
+        R r = -y;
+        if constexpr (C < 0) r = r - z;
+        return r;
+    } else if constexpr (C < 0) {
+        return -z;
+    } else {
+        return R(0);
+    }
+}
+
+template <class L, int D, class R> __device__ __forceinline__ R cdot(R x, R y, R z) {
+    return signed_sum<L::cx(D), L::cy(D), L::cz(D), R>(x, y, z);
+}
+
+// Compile-time loop over the opposite pairs: f(std::integral_constant<int, p>).
+template <class L, int P = 0, class F> __device__ __forceinline__ void static_for_pairs(F&& f) {
+    if constexpr (P < L::PAIRS) {
+        f(std::integral_constant<int, P>{});
+        static_for_pairs<L, P + 1>(f);
+    }
+}
+
 // ------------------------------------------------------- periodic neighbours
 // Offsets of the x-1/x/x+1, y-1/y/y+1, z-1/z/z+1 neighbours with periodic wrap
 // (reference esoteric_pull.hpp:40-46), indexed by c + 1.  Unsigned wrap-around
@@ -229,16 +281,6 @@ __device__ __forceinline__ void gather_walls(const LbmArgs& a, u32 n, const Nbr&
     }
 }
 
-template <class L, int P = 0> __device__ __forceinline__ unsigned wall_links(const LbmArgs& a, u32 n, const Nbr& o) {
-    if constexpr (P < L::PAIRS) {
-        constexpr int i = 2 * P + 1, j = i + 1;
-        const unsigned b = (a.flags[n + nbr_off<L, j>(o)] & kFlagTypeMask) != 0 ? 1U : 0U;
-        const unsigned fw = (a.flags[n + nbr_off<L, i>(o)] & kFlagTypeMask) != 0 ? 1U : 0U;
-        return (b << (2 * P)) | (fw << (2 * P + 1)) | wall_links<L, P + 1>(a, n, o);
-    } else {
-        return 0U;
-    }
-}
 
 template <class L, class R, int P = 0>
 __device__ __forceinline__ void moving_wall_pairs(const LbmArgs& a, u32 n, const Nbr& o, R rw, R* fin) {
@@ -246,14 +288,12 @@ __device__ __forceinline__ void moving_wall_pairs(const LbmArgs& a, u32 n, const
         constexpr int i = 2 * P + 1, j = i + 1;
         const int idb = a.flags[n + nbr_off<L, j>(o)] & kFlagTypeMask;
         if (idb >= 2) {
-            const R cu = R(L::cx(i)) * R(a.wall_u[idb][0]) + R(L::cy(i)) * R(a.wall_u[idb][1]) +
-                         R(L::cz(i)) * R(a.wall_u[idb][2]);
+            const R cu = cdot<L, i, R>(R(a.wall_u[idb][0]), R(a.wall_u[idb][1]), R(a.wall_u[idb][2]));
             fin[i] += R(6.0) * R(L::w(i)) * rw * cu;
         }
         const int idf = a.flags[n + nbr_off<L, i>(o)] & kFlagTypeMask;
         if (idf >= 2) {
-            const R cu = R(L::cx(j)) * R(a.wall_u[idf][0]) + R(L::cy(j)) * R(a.wall_u[idf][1]) +
-                         R(L::cz(j)) * R(a.wall_u[idf][2]);
+            const R cu = cdot<L, j, R>(R(a.wall_u[idf][0]), R(a.wall_u[idf][1]), R(a.wall_u[idf][2]));
             fin[j] += R(6.0) * R(L::w(j)) * rw * cu;
         }
         moving_wall_pairs<L, R, P + 1>(a, n, o, rw, fin);
@@ -266,11 +306,24 @@ __device__ __forceinline__ void gather_loads(const LbmArgs& a, u32 n, const Nbr&
     fin[0] = ld<S, L, 0, RAW>(Slots<S, NARROW>::rest(a, n), a);
     if constexpr (FLAGS) {
         if (flag & kFlagNearWall) {
-            gather_walls<L, S, NARROW, RAW>(a, n, o, wall_links<L>(a, n, o), fin);
+            gather_walls<L, S, NARROW, RAW>(a, n, o, a.wall_mask[n], fin);
             return;
         }
     }
     gather_plain<L, S, NARROW, RAW>(a, n, o, fin);
+}
+
+// Bounce-back fix-up of one near-wall cell whose values were gathered as if
+// it had no walls (the paired kernels): wall links reload the partner slot.
+template <class L, class S, int P = 0>
+__device__ __forceinline__ void bounce_fixup(const LbmArgs& a, const typename S::T* base, u32 n, const Nbr& o,
+                                             unsigned walls, typename S::R* f) {
+    if constexpr (P < L::PAIRS) {
+        constexpr int i = 2 * P + 1, j = i + 1;
+        if ((walls >> (2 * P)) & 1U) f[i] = ld<S, L, i, S::scaled>(base + (a.pb_off[P] + (n + nbr_off<L, j>(o))), a);
+        if ((walls >> (2 * P + 1)) & 1U) f[j] = ld<S, L, j, S::scaled>(base + (a.pa_off[P] + n), a);
+        bounce_fixup<L, S, P + 1>(a, base, n, o, walls, f);
+    }
 }
 
 // Moving-wall correction for values held in FP16 storage units: the
@@ -281,14 +334,12 @@ __device__ __forceinline__ void moving_wall_pairs_scaled(const LbmArgs& a, u32 n
         constexpr int i = 2 * P + 1, j = i + 1;
         const int idb = a.flags[n + nbr_off<L, j>(o)] & kFlagTypeMask;
         if (idb >= 2) {
-            const float cu = float(L::cx(i)) * a.wall_u[idb][0] + float(L::cy(i)) * a.wall_u[idb][1] +
-                             float(L::cz(i)) * a.wall_u[idb][2];
+            const float cu = cdot<L, i, float>(a.wall_u[idb][0], a.wall_u[idb][1], a.wall_u[idb][2]);
             h[i] += a.scale[i] * (6.0F * float(L::w(i)) * rw * cu);
         }
         const int idf = a.flags[n + nbr_off<L, i>(o)] & kFlagTypeMask;
         if (idf >= 2) {
-            const float cu = float(L::cx(j)) * a.wall_u[idf][0] + float(L::cy(j)) * a.wall_u[idf][1] +
-                             float(L::cz(j)) * a.wall_u[idf][2];
+            const float cu = cdot<L, j, float>(a.wall_u[idf][0], a.wall_u[idf][1], a.wall_u[idf][2]);
             h[j] += a.scale[j] * (6.0F * float(L::w(j)) * rw * cu);
         }
         moving_wall_pairs_scaled<L, P + 1>(a, n, o, rw, h);
@@ -430,10 +481,24 @@ __device__ __forceinline__ void moments(const R* fin, R& rho, R& ux, R& uy, R& u
     uz = jz * inv;
 }
 
+// Scalar parameters in the arithmetic type (FP32 kernels read the float copies).
+template <class R> __device__ __forceinline__ R p_tau(const LbmArgs& a) {
+    if constexpr (sizeof(R) == 8) return a.tau; else return a.tau_f;
+}
+template <class R> __device__ __forceinline__ R p_les_k(const LbmArgs& a) {
+    if constexpr (sizeof(R) == 8) return a.les_k; else return a.les_k_f;
+}
+
 template <class R> __device__ __forceinline__ void cell_acceleration(const LbmArgs& a, u32 n, R& ax, R& ay, R& az) {
-    ax = R(a.ax);
-    ay = R(a.ay);
-    az = R(a.az);
+    if constexpr (sizeof(R) == 8) {
+        ax = a.ax;
+        ay = a.ay;
+        az = a.az;
+    } else {
+        ax = a.ax_f;
+        ay = a.ay_f;
+        az = a.az_f;
+    }
     if (a.ax_field) {
         ax += R(a.ax_field[n]);
         ay += R(a.ay_field[n]);
@@ -520,13 +585,13 @@ __device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, cons
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
         const ClassCoef<R>& k = cc[weight_class<L>(i)];
-        const R cu3 = R(L::cx(i)) * ux3 + R(L::cy(i)) * uy3 + R(L::cz(i)) * uz3;     // 3 c.u
-        const R cu15 = R(L::cx(i)) * ux15 + R(L::cy(i)) * uy15 + R(L::cz(i)) * uz15; // 1.5 c.u
+        const R cu3 = cdot<L, i>(ux3, uy3, uz3);     // 3 c.u
+        const R cu15 = cdot<L, i>(ux15, uy15, uz15); // 1.5 c.u
         const R t = cu3 * cu15 + base;
         R sp = DELTA ? k.a * t + (a1 * s[P] - k.a0) : k.a * t + a1 * s[P];
         R dp = k.c * cu3 + b1 * d[P];
         if constexpr (FORCE) {
-            const R cf = R(L::cx(i)) * fx + R(L::cy(i)) * fy + R(L::cz(i)) * fz;
+            const R cf = cdot<L, i>(fx, fy, fz);
             sp += k.g1 * (cu3 * cf - uf);
             dp += k.g2 * cf;
         }
@@ -548,11 +613,12 @@ __device__ __forceinline__ void collide_pairs(R* f, const R* s, const R* d, cons
 // Relaxation rates of a cell: omega+ from tau (LES-adjusted) and omega- by
 // the configured rule.
 template <class R> __device__ __forceinline__ R omega_minus_of(const LbmArgs& a, R tau, R omega) {
-    if (a.omega_minus > 0.0) return R(a.omega_minus); // fixed TRT antisymmetric rate
-    if (a.omega_minus < 0.0) return omega;           // BGK
+    if (a.minus_mode > 0) return sizeof(R) == 8 ? R(a.omega_minus) : R(a.omega_minus_f); // fixed TRT rate
+    if (a.minus_mode < 0) return omega;                                                  // BGK
     // TRT magic: tau- = 1/2 + Lambda / (tau+ - 1/2)
     const R sp = tau - R(0.5);
-    return sp * rcp(R(a.trt_magic) + R(0.5) * sp);
+    const R lam = sizeof(R) == 8 ? R(a.trt_magic) : R(a.trt_magic_f);
+    return sp * rcp(lam + R(0.5) * sp);
 }
 
 // Per weight class coefficients; `scale` multiplies every term (FP16 storage
@@ -588,8 +654,8 @@ __device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
         uy += R(0.5) * ay;
         uz += R(0.5) * az;
     }
-    R tau = R(a.tau);
-    if constexpr (LES) tau = les_tau<L, R, DELTA>(s, rho, inv, ux, uy, uz, tau, R(a.les_k));
+    R tau = p_tau<R>(a);
+    if constexpr (LES) tau = les_tau<L, R, DELTA>(s, rho, inv, ux, uy, uz, tau, p_les_k<R>(a));
     const R omega = rcp(tau);
     const R omega_m = omega_minus_of<R>(a, tau, omega);
     const R base = R(1) - R(1.5) * (ux * ux + uy * uy + uz * uz);
@@ -624,116 +690,273 @@ __device__ __forceinline__ void collide(const LbmArgs& a, u32 n, R* f) {
 // The same TRT/Guo/gray update as collide, for values held in FP16 storage
 // units h = (f - w) s_k, with s_k constant within each weight class k.
 // Pair sums stay in storage units: the moments scale each class's partial
-// sums once, and the scales are folded into the per-class coefficients
-// (ClassCoef scaled by s_k), so decoding and encoding cost only the
-// half <-> float conversions.
-template <class L, bool LES, bool GRAY, bool FORCE>
-__device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, float* h) {
-    float sh[L::PAIRS], dh[L::PAIRS];
-    pair_sums<L, float>(h, sh, dh);
-    // Per weight class partial sums (classes 1..3), scaled once each.
-    float S[4] = {0, 0, 0, 0}, JX[4] = {0, 0, 0, 0}, JY[4] = {0, 0, 0, 0}, JZ[4] = {0, 0, 0, 0};
-    float XX[4] = {0, 0, 0, 0}, YY[4] = {0, 0, 0, 0}, ZZ[4] = {0, 0, 0, 0};
-    float XY[4] = {0, 0, 0, 0}, XZ[4] = {0, 0, 0, 0}, YZ[4] = {0, 0, 0, 0};
+// sums once, and the scales are folded into the per-class coefficients, so
+// decoding and encoding cost only the half <-> float conversions.
+//
+// Written once for V = float (one cell) and V = float2 (two cells, sm_100a
+// packed f32x2 instructions: one issue slot for both cells).  Every operation
+// is an explicitly rounded intrinsic, so the compiler cannot contract the two
+// forms differently and the one-cell and two-cell kernels stay bitwise equal.
+
+__device__ __forceinline__ float v_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float v_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float v_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float v_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float2 v_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 v_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b = RN(b * (-1) + a), the same rounding as the scalar subtraction
+__device__ __forceinline__ float2 v_sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0F, -1.0F), a); }
+__device__ __forceinline__ float2 v_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
+template <class V> __device__ __forceinline__ V v_splat(float c) {
+    if constexpr (sizeof(V) == 8) return make_float2(c, c); else return c;
+}
+template <class V> constexpr int v_lanes() { return sizeof(V) / sizeof(float); }
+__device__ __forceinline__ float v_lane(float v, int) { return v; }
+__device__ __forceinline__ float v_lane(float2 v, int k) { return k ? v.y : v.x; }
+__device__ __forceinline__ void v_set(float& v, int, float x) { v = x; }
+__device__ __forceinline__ void v_set(float2& v, int k, float x) { if (k) v.y = x; else v.x = x; }
+// Applies a scalar function lane by lane.
+template <class V, class F> __device__ __forceinline__ V v_map(V v, F f) {
+    V r = v;
+#pragma unroll
+    for (int k = 0; k < v_lanes<V>(); ++k) v_set(r, k, f(v_lane(v, k), k));
+    return r;
+}
+
+// Signed sum of lattice-vector components, V form (see signed_sum).
+template <int A, int B, int C, class V> __device__ __forceinline__ V v_signed_sum(V x, V y, V z) {
+    static_assert(A > 0 || B > 0 || C > 0, "the pair's first direction has a positive component");
+    if constexpr (A > 0) {
+        V r = x;
+        if constexpr (B > 0) r = v_add(r, y);
+        if constexpr (C > 0) r = v_add(r, z);
+        if constexpr (B < 0) r = v_sub(r, y);
+        if constexpr (C < 0) r = v_sub(r, z);
+        return r;
+    } else if constexpr (B > 0) {
+        V r = y;
+        if constexpr (C > 0) r = v_add(r, z);
+        if constexpr (A < 0) r = v_sub(r, x);
+        if constexpr (C < 0) r = v_sub(r, z);
+        return r;
+    } else {
+        V r = z;
+        if constexpr (A < 0) r = v_sub(r, x);
+        if constexpr (B < 0) r = v_sub(r, y);
+        return r;
+    }
+}
+template <class L, int D, class V> __device__ __forceinline__ V v_cdot(V x, V y, V z) {
+    return v_signed_sum<L::cx(D), L::cy(D), L::cz(D), V>(x, y, z);
+}
+
+// Sum over pairs p in [P, PAIRS) of coef(p) * val[p], coef(p) in {-1, 0, 1}
+// given by Coef::at(p); started from the first nonzero term, so no
+// instruction is spent adding to zero.
+template <class Coef, int P, int E, class V> __device__ __forceinline__ V v_csum_from(V acc, const V* val) {
+    if constexpr (P < E) {
+        constexpr int c = Coef::at(P);
+        if constexpr (c > 0) acc = v_add(acc, val[P]);
+        if constexpr (c < 0) acc = v_sub(acc, val[P]);
+        return v_csum_from<Coef, P + 1, E>(acc, val);
+    } else {
+        return acc;
+    }
+}
+template <class Coef, int P, int E, class V> __device__ __forceinline__ V v_csum(const V* val) {
+    if constexpr (P >= E) {
+        return v_splat<V>(0.0F);
+    } else {
+        constexpr int c = Coef::at(P);
+        if constexpr (c > 0) return v_csum_from<Coef, P + 1, E>(val[P], val);
+        else if constexpr (c < 0) return v_csum_from<Coef, P + 1, E>(v_sub(v_splat<V>(0.0F), val[P]), val);
+        else return v_csum<Coef, P + 1, E>(val);
+    }
+}
+// Coefficients of pair p (first direction i = 2p+1) in the class-k sums:
+// component moments (c_a, 0 = all ones) and second moments (c_a c_b).
+template <class L, int K, int A> struct CoefFirst {
+    static constexpr int at(int p) {
+        const int i = 2 * p + 1;
+        if (weight_class<L>(i) != K) return 0;
+        return A == 0 ? 1 : (A == 1 ? L::cx(i) : (A == 2 ? L::cy(i) : L::cz(i)));
+    }
+};
+template <class L, int K, int A, int B> struct CoefSecond {
+    static constexpr int comp(int i, int c) { return c == 1 ? L::cx(i) : (c == 2 ? L::cy(i) : L::cz(i)); }
+    static constexpr int at(int p) {
+        const int i = 2 * p + 1;
+        return weight_class<L>(i) != K ? 0 : comp(i, A) * comp(i, B);
+    }
+};
+template <class L, int K, int A, class V> __device__ __forceinline__ V class_sum(const V* v) {
+    return v_csum<CoefFirst<L, K, A>, 0, L::PAIRS>(v);
+}
+template <class L, int K, int A, int B, class V> __device__ __forceinline__ V class_sum2(const V* v) {
+    return v_csum<CoefSecond<L, K, A, B>, 0, L::PAIRS>(v);
+}
+// sum_k sum_k-class(v) / s_k over the weight classes 1..K, as a multiply-add chain.
+template <class L, int A, class V> __device__ __forceinline__ V scaled_moment(const V* v, const float* inv, V init) {
+    V r = v_fma(class_sum<L, 1, A>(v), v_splat<V>(inv[1]), init);
+    r = v_fma(class_sum<L, 2, A>(v), v_splat<V>(inv[2]), r);
+    if constexpr (L::Q == 27) r = v_fma(class_sum<L, 3, A>(v), v_splat<V>(inv[3]), r);
+    return r;
+}
+template <class L, int A, int B, class V>
+__device__ __forceinline__ V scaled_moment2(const V* v, const float* inv, V init) {
+    V r = v_fma(class_sum2<L, 1, A, B>(v), v_splat<V>(inv[1]), init);
+    r = v_fma(class_sum2<L, 2, A, B>(v), v_splat<V>(inv[2]), r);
+    if constexpr (L::Q == 27) r = v_fma(class_sum2<L, 3, A, B>(v), v_splat<V>(inv[3]), r);
+    return r;
+}
+
+// sqrt for the Smagorinsky rate: hardware reciprocal square root (2 ulp);
+// the eddy viscosity needs no correctly rounded square root, and FP16
+// storage rounding is far larger.  x >= 0; x = 0 gives 0.
+__device__ __forceinline__ float les_sqrt(float x) { return x * rsqrtf(fmaxf(x, 1.0e-30F)); }
+
+// n: the first cell of V's lanes (lane k is cell n + k).
+template <class L, bool LES, bool GRAY, bool FORCE, class V>
+__device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, V* h) {
+    constexpr int K = L::Q == 27 ? 3 : 2;
+    const V one = v_splat<V>(1.0F);
+    V sh[L::PAIRS], dh[L::PAIRS];
 #pragma unroll
     for (int p = 0; p < L::PAIRS; ++p) {
-        const int i = 2 * p + 1;
-        const int k = weight_class<L>(i);
-        S[k] += sh[p];
-        if (L::cx(i) > 0) JX[k] += dh[p];
-        if (L::cx(i) < 0) JX[k] -= dh[p];
-        if (L::cy(i) > 0) JY[k] += dh[p];
-        if (L::cy(i) < 0) JY[k] -= dh[p];
-        if (L::cz(i) > 0) JZ[k] += dh[p];
-        if (L::cz(i) < 0) JZ[k] -= dh[p];
-        if constexpr (LES) {
-            if (L::cx(i) != 0) XX[k] += sh[p];
-            if (L::cy(i) != 0) YY[k] += sh[p];
-            if (L::cz(i) != 0) ZZ[k] += sh[p];
-            if (L::cx(i) * L::cy(i) > 0) XY[k] += sh[p];
-            if (L::cx(i) * L::cy(i) < 0) XY[k] -= sh[p];
-            if (L::cx(i) * L::cz(i) > 0) XZ[k] += sh[p];
-            if (L::cx(i) * L::cz(i) < 0) XZ[k] -= sh[p];
-            if (L::cy(i) * L::cz(i) > 0) YZ[k] += sh[p];
-            if (L::cy(i) * L::cz(i) < 0) YZ[k] -= sh[p];
-        }
+        sh[p] = v_add(h[2 * p + 1], h[2 * p + 2]);
+        dh[p] = v_sub(h[2 * p + 1], h[2 * p + 2]);
     }
-    constexpr int K = L::Q == 27 ? 3 : 2;
-    float inv[4];
+    float inv[4], scl[4];
 #pragma unroll
-    for (int k = 0; k <= K; ++k) inv[k] = a.inv_scale[class_rep(k)];
-    float rho = h[0] * inv[0], jx = 0.0F, jy = 0.0F, jz = 0.0F;
-#pragma unroll
-    for (int k = 1; k <= K; ++k) {
-        rho += S[k] * inv[k];
-        jx += JX[k] * inv[k];
-        jy += JY[k] * inv[k];
-        jz += JZ[k] * inv[k];
+    for (int k = 0; k <= K; ++k) {
+        inv[k] = a.inv_scale[class_rep(k)];
+        scl[k] = a.scale[class_rep(k)];
     }
-    rho += 1.0F;
-    const float irho = rho > 0.0F ? rcp_unbiased(rho) : 0.0F;
-    float ux = jx * irho, uy = jy * irho, uz = jz * irho;
-    float ax = 0.0F, ay = 0.0F, az = 0.0F;
+    const V rho = v_add(scaled_moment<L, 0>(sh, inv, v_mul(h[0], v_splat<V>(inv[0]))), one);
+    const V zero = v_splat<V>(-0.0F); // x + (-0) == x for every x
+    const V jx = scaled_moment<L, 1>(dh, inv, zero);
+    const V jy = scaled_moment<L, 2>(dh, inv, zero);
+    const V jz = scaled_moment<L, 3>(dh, inv, zero);
+    const V irho = v_map(rho, [](float r, int) { return r > 0.0F ? rcp_unbiased(r) : 0.0F; });
+    V ux = v_mul(jx, irho), uy = v_mul(jy, irho), uz = v_mul(jz, irho);
+    V ax = zero, ay = zero, az = zero;
     if constexpr (FORCE) {
-        cell_acceleration<float>(a, n, ax, ay, az);
-        ux += 0.5F * ax;
-        uy += 0.5F * ay;
-        uz += 0.5F * az;
+        ax = v_map(ax, [&](float, int k) { float x, y, z; cell_acceleration<float>(a, n + k, x, y, z); return x; });
+        ay = v_map(ay, [&](float, int k) { float x, y, z; cell_acceleration<float>(a, n + k, x, y, z); return y; });
+        az = v_map(az, [&](float, int k) { float x, y, z; cell_acceleration<float>(a, n + k, x, y, z); return z; });
+        const V half = v_splat<V>(0.5F);
+        ux = v_fma(ax, half, ux);
+        uy = v_fma(ay, half, uy);
+        uz = v_fma(az, half, uz);
     }
-    float tau = float(a.tau);
+    V omega, omega_m;
     if constexpr (LES) {
-        if (rho > 0.0F) {
-            const float third = 1.0F / 3.0F;
-            float sxx = third, syy = third, szz = third, sxy = 0.0F, sxz = 0.0F, syz = 0.0F;
-#pragma unroll
-            for (int k = 1; k <= K; ++k) {
-                sxx += XX[k] * inv[k];
-                syy += YY[k] * inv[k];
-                szz += ZZ[k] * inv[k];
-                sxy += XY[k] * inv[k];
-                sxz += XZ[k] * inv[k];
-                syz += YZ[k] * inv[k];
-            }
-            const float pxx = sxx - rho * (third + ux * ux);
-            const float pyy = syy - rho * (third + uy * uy);
-            const float pzz = szz - rho * (third + uz * uz);
-            const float pxy = sxy - rho * ux * uy;
-            const float pxz = sxz - rho * ux * uz;
-            const float pyz = syz - rho * uy * uz;
-            const float q = pxx * pxx + pyy * pyy + pzz * pzz + 2.0F * (pxy * pxy + pxz * pxz + pyz * pyz);
-            tau = 0.5F * (tau + sqrtf(tau * tau + float(a.les_k) * sqrtf(q) * irho));
-        }
+        const V third = v_splat<V>(1.0F / 3.0F);
+        const V sxx = scaled_moment2<L, 1, 1>(sh, inv, third);
+        const V syy = scaled_moment2<L, 2, 2>(sh, inv, third);
+        const V szz = scaled_moment2<L, 3, 3>(sh, inv, third);
+        const V sxy = scaled_moment2<L, 1, 2>(sh, inv, zero);
+        const V sxz = scaled_moment2<L, 1, 3>(sh, inv, zero);
+        const V syz = scaled_moment2<L, 2, 3>(sh, inv, zero);
+        const V nrho = v_mul(rho, v_splat<V>(-1.0F));
+        const V pxx = v_fma(nrho, v_fma(ux, ux, third), sxx);
+        const V pyy = v_fma(nrho, v_fma(uy, uy, third), syy);
+        const V pzz = v_fma(nrho, v_fma(uz, uz, third), szz);
+        const V nrux = v_mul(nrho, ux), nruy = v_mul(nrho, uy);
+        const V pxy = v_fma(nrux, uy, sxy);
+        const V pxz = v_fma(nrux, uz, sxz);
+        const V pyz = v_fma(nruy, uz, syz);
+        V off = v_mul(pxy, pxy);
+        off = v_fma(pxz, pxz, off);
+        off = v_fma(pyz, pyz, off);
+        V q = v_fma(pxx, pxx, v_add(off, off));
+        q = v_fma(pyy, pyy, q);
+        q = v_fma(pzz, pzz, q);
+        const float tau0 = a.tau_f, kles = a.les_k_f;
+        V tau = v_map(q, [&](float qq, int k) {
+            const float r = v_lane(rho, k);
+            return r > 0.0F ? 0.5F * (tau0 + les_sqrt(tau0 * tau0 + kles * les_sqrt(qq) * v_lane(irho, k))) : tau0;
+        });
+        omega = v_map(tau, [](float t, int) { return rcp(t); });
+        omega_m = v_map(tau, [&](float t, int k) { return omega_minus_of<float>(a, t, v_lane(omega, k)); });
+    } else {
+        const float w = rcp(a.tau_f);
+        omega = v_splat<V>(w);
+        omega_m = v_splat<V>(omega_minus_of<float>(a, a.tau_f, w));
     }
-    const float omega = rcp(tau);
-    const float omega_m = omega_minus_of<float>(a, tau, omega);
-    const float base = 1.0F - 1.5F * (ux * ux + uy * uy + uz * uz);
-    float fx = 0.0F, fy = 0.0F, fz = 0.0F, uf = 0.0F;
+    V base = v_mul(ux, ux);
+    base = v_fma(uy, uy, base);
+    base = v_fma(uz, uz, base);
+    base = v_fma(base, v_splat<V>(-1.5F), one);
+    V fx = zero, fy = zero, fz = zero, nuf = zero;
     if constexpr (FORCE) {
-        fx = rho * ax;
-        fy = rho * ay;
-        fz = rho * az;
-        uf = ux * fx + uy * fy + uz * fz;
+        fx = v_mul(rho, ax);
+        fy = v_mul(rho, ay);
+        fz = v_mul(rho, az);
+        V uf = v_mul(ux, fx);
+        uf = v_fma(uy, fy, uf);
+        uf = v_fma(uz, fz, uf);
+        nuf = v_mul(uf, v_splat<V>(-1.0F));
     }
-    const float gp = 1.0F - 0.5F * omega;
-    const float gm = 1.0F - 0.5F * omega_m;
-    float ns = 0.0F;
-    if constexpr (GRAY) ns = a.ns[n];
+    const V nhalf = v_splat<V>(-0.5F);
+    const V gp = v_fma(omega, nhalf, one), gm = v_fma(omega_m, nhalf, one);
+    V ns = zero, keep = one;
+    if constexpr (GRAY) {
+        ns = v_map(ns, [&](float, int k) { return a.ns[n + k]; });
+        keep = v_sub(one, ns);
+    }
     {
-        constexpr float w0 = float(L::w(0));
-        const float h0 = h[0];
-        float o0 = (1.0F - omega) * h0 + a.scale[0] * (omega * w0 * (rho * base - 1.0F));
-        if constexpr (FORCE) o0 -= a.scale[0] * (gp * w0 * (3.0F * uf));
-        if constexpr (GRAY) o0 = (1.0F - ns) * o0 + ns * h0;
+        const float w0 = float(L::w(0)) * scl[0];
+        const V h0 = h[0];
+        // (1 - omega) h0 + s0 omega w0 (rho base - 1)  [- s0 (1 - omega/2) w0 3 u.F]
+        V o0 = v_fma(v_sub(one, omega), h0, v_mul(v_mul(omega, v_splat<V>(w0)), v_fma(rho, base, v_splat<V>(-1.0F))));
+        if constexpr (FORCE) o0 = v_fma(v_mul(gp, v_splat<V>(3.0F * w0)), nuf, o0);
+        if constexpr (GRAY) o0 = v_fma(keep, o0, v_mul(ns, h0));
         h[0] = o0;
     }
-    ClassCoef<float> cc[4];
-    float scl[4];
+    // per weight class: a = omega w rho, a0 = omega w, c = omega- w rho (w includes the storage scale)
+    V ka[4], nka0[4], kc[4], g1[4], g2[4];
 #pragma unroll
-    for (int k = 0; k <= K; ++k) scl[k] = a.scale[class_rep(k)];
-    class_coefficients<L, float>(cc, rho, omega, omega_m, gp, gm, scl);
-    collide_pairs<L, float, FORCE, GRAY, true>(h, sh, dh, cc, 3.0F * ux, 3.0F * uy, 3.0F * uz, 1.5F * ux, 1.5F * uy,
-                                               1.5F * uz, fx, fy, fz, base, uf, 0.5F * (1.0F - omega),
-                                               0.5F * (1.0F - omega_m), ns);
+    for (int k = 1; k <= K; ++k) {
+        const float w = float(L::w(class_rep(k))) * scl[k];
+        const V wr = v_mul(rho, v_splat<V>(w));
+        ka[k] = v_mul(omega, wr);
+        kc[k] = v_mul(omega_m, wr);
+        nka0[k] = v_mul(omega, v_splat<V>(-w));
+        if constexpr (FORCE) {
+            g1[k] = v_mul(gp, v_splat<V>(3.0F * w));
+            g2[k] = v_mul(gm, v_splat<V>(3.0F * w));
+        }
+    }
+    const V a1 = v_mul(v_sub(one, omega), v_splat<V>(0.5F));
+    const V b1 = v_mul(v_sub(one, omega_m), v_splat<V>(0.5F));
+    const V ux3 = v_mul(ux, v_splat<V>(3.0F)), uy3 = v_mul(uy, v_splat<V>(3.0F)), uz3 = v_mul(uz, v_splat<V>(3.0F));
+    const V ux15 = v_mul(ux, v_splat<V>(1.5F)), uy15 = v_mul(uy, v_splat<V>(1.5F)), uz15 = v_mul(uz, v_splat<V>(1.5F));
+    static_for_pairs<L>([&](auto PP) {
+        constexpr int p = decltype(PP)::value;
+        constexpr int i = 2 * p + 1, j = i + 1;
+        constexpr int k = weight_class<L>(i);
+        const V cu3 = v_cdot<L, i>(ux3, uy3, uz3);
+        const V cu15 = v_cdot<L, i>(ux15, uy15, uz15);
+        const V t = v_fma(cu3, cu15, base);
+        V sp = v_fma(ka[k], t, v_fma(a1, sh[p], nka0[k]));
+        V dp = v_fma(kc[k], cu3, v_mul(b1, dh[p]));
+        if constexpr (FORCE) {
+            const V cf = v_cdot<L, i>(fx, fy, fz);
+            sp = v_fma(g1[k], v_fma(cu3, cf, nuf), sp);
+            dp = v_fma(g2[k], cf, dp);
+        }
+        V oi = v_add(sp, dp);
+        V oj = v_sub(sp, dp);
+        if constexpr (GRAY) {
+            const V hi = h[i], hj = h[j];
+            oi = v_fma(keep, oi, v_mul(ns, hj));
+            oj = v_fma(keep, oj, v_mul(ns, hi));
+        }
+        h[i] = oi;
+        h[j] = oj;
+    });
 }
 
 // ---------------------------------------------------------------- the step
@@ -827,7 +1050,7 @@ __device__ __forceinline__ void init_pairs(const LbmArgs& a, u32 n, const Nbr& o
     using R = typename S::R;
     if constexpr (P < L::PAIRS) {
         constexpr int i = 2 * P + 1, j = i + 1;
-        const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
+        const R cu = cdot<L, i>(ux, uy, uz);
         const R wr = R(L::w(i)) * rho;
         const R fi = wr * (R(1) + R(3) * cu + R(4.5) * cu * cu - usq15);
         const R fj = wr * (R(1) - R(3) * cu + R(4.5) * cu * cu - usq15);
@@ -856,7 +1079,7 @@ __global__ void __launch_bounds__(128) k_init(const __grid_constant__ LbmArgs a,
     if constexpr (FLAGS) {
         const std::uint8_t flag = a.flags[n];
         if (flag & kFlagTypeMask) return;
-        if (flag & kFlagNearWall) walls = wall_links<L>(a, n, o);
+        if (flag & kFlagNearWall) walls = a.wall_mask[n];
     }
     R rho, ux, uy, uz;
     if (s.kind == 0) {
@@ -1040,7 +1263,7 @@ static __global__ void __launch_bounds__(kReduceThreads) k_reduce_final(const do
 // flags.  Near-wall bits let interior cells skip all neighbour-flag loads.
 template <class L>
 __global__ void __launch_bounds__(128) k_prepare_flags(const __grid_constant__ LbmArgs a, const std::uint8_t* user,
-                                                       std::uint8_t* out) {
+                                                       std::uint8_t* out, std::uint32_t* mask) {
     const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
     const u32 z = blockIdx.z;
@@ -1049,18 +1272,26 @@ __global__ void __launch_bounds__(128) k_prepare_flags(const __grid_constant__ L
     const std::uint8_t t = user[n] & kFlagTypeMask;
     if (t != 0) {
         out[n] = t;
+        mask[n] = 0U;
         return;
     }
     const Nbr o = make_nbr(a, x, y, z);
     std::uint8_t b = 0;
+    std::uint32_t links = 0U;
 #pragma unroll
-    for (int d = 1; d < L::Q; ++d) {
-        const u32 m = n + o.ox[L::cx(d) + 1] + o.oy[L::cy(d) + 1] + o.oz[L::cz(d) + 1];
-        const std::uint8_t u = user[m] & kFlagTypeMask;
-        if (u != 0) b |= kFlagNearWall;
-        if (u >= 2) b |= kFlagNearMoving;
+    for (int p = 0; p < L::PAIRS; ++p) {
+        const int i = 2 * p + 1, j = i + 1;
+        // source of direction i is n + c_j, source of direction j is n + c_i
+        const u32 mb = n + o.ox[L::cx(j) + 1] + o.oy[L::cy(j) + 1] + o.oz[L::cz(j) + 1];
+        const u32 mf = n + o.ox[L::cx(i) + 1] + o.oy[L::cy(i) + 1] + o.oz[L::cz(i) + 1];
+        const std::uint8_t ub = user[mb] & kFlagTypeMask, uf = user[mf] & kFlagTypeMask;
+        if (ub != 0) links |= 1U << (2 * p);
+        if (uf != 0) links |= 1U << (2 * p + 1);
+        if (ub >= 2 || uf >= 2) b |= kFlagNearMoving;
     }
+    if (links != 0U) b |= kFlagNearWall;
     out[n] = b;
+    mask[n] = links;
 }
 
 } // namespace cfdx

@@ -15,12 +15,12 @@ cudaError_t launch_sum_partials(const double* partials, std::size_t count, doubl
 }
 
 // Flag preparation does not depend on the storage type; it lives here once.
-cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out, dim3 g, dim3 b,
-                                 cudaStream_t s) {
+cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out,
+                                 std::uint32_t* mask, dim3 g, dim3 b, cudaStream_t s) {
     if (q == 19)
-        k_prepare_flags<D3Q19><<<g, b, 0, s>>>(a, user, out);
+        k_prepare_flags<D3Q19><<<g, b, 0, s>>>(a, user, out, mask);
     else if (q == 27)
-        k_prepare_flags<D3Q27><<<g, b, 0, s>>>(a, user, out);
+        k_prepare_flags<D3Q27><<<g, b, 0, s>>>(a, user, out, mask);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();

@@ -61,7 +61,7 @@ cudaError_t launch_step_oop(const KernelKey& k, const LbmArgs& src, const LbmArg
 cudaError_t launch_adjoint_seed(const KernelKey& k, const AdjointArgs& a, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t launch_adjoint_step(const KernelKey& k, const AdjointArgs& a, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t launch_sum_partials(const double* partials, std::size_t count, double* out, cudaStream_t s);
-cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out, dim3 grid,
-                                 dim3 block, cudaStream_t s);
+cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out,
+                                 std::uint32_t* mask, dim3 grid, dim3 block, cudaStream_t s);
 
 } // namespace cfdx

@@ -5,6 +5,7 @@
 #include "lbm_adjoint.cuh"
 #include "lbm_device.cuh"
 #include "lbm_launch.h"
+#include "lbm_step_h2.cuh"
 #include "lbm_step_x2.cuh"
 
 namespace cfdx {
@@ -36,7 +37,8 @@ cudaError_t step_single(bool narrow, const LbmArgs& a, dim3 g, dim3 b, cudaStrea
     return cudaGetLastError();
 }
 
-// Paired-cell kernel (FP32 / FP16 storage): a thread owns x0 = 2t and x0 + 1.
+// Paired-cell kernels: a thread owns x0 = 2t and x0 + 1 (FP16: k_step_h2,
+// packed f32x2 collision; FP32: k_step_x2).
 template <class L, class S, bool LES, bool FL, bool GR>
 cudaError_t step_paired(const LbmArgs& a, dim3 b, cudaStream_t s) {
     if constexpr (sizeof(typename S::T) == 8) {
@@ -44,7 +46,10 @@ cudaError_t step_paired(const LbmArgs& a, dim3 b, cudaStream_t s) {
     } else {
         const unsigned pairs = (a.nx + 1U) / 2U;
         dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, a.nz);
-        k_step_x2<L, S, LES, FL, GR><<<g, b, 0, s>>>(a);
+        if constexpr (sizeof(typename S::T) == 2)
+            k_step_h2<L, LES, FL, GR><<<g, b, 0, s>>>(a);
+        else
+            k_step_x2<L, S, LES, FL, GR><<<g, b, 0, s>>>(a);
         return cudaGetLastError();
     }
 }

@@ -204,18 +204,6 @@ __device__ __forceinline__ void pair_stores(const LbmArgs& a, typename S::T* bas
     }
 }
 
-// Bounce-back fix-up of one near-wall cell: wall links reload the partner slot.
-template <class L, class S, int P = 0>
-__device__ __forceinline__ void bounce_fixup(const LbmArgs& a, const typename S::T* base, u32 n, const Nbr& o,
-                                             unsigned walls, typename S::R* f) {
-    if constexpr (P < L::PAIRS) {
-        constexpr int i = 2 * P + 1, j = i + 1;
-        if ((walls >> (2 * P)) & 1U) f[i] = ld<S, L, i, S::scaled>(base + (a.pb_off[P] + (n + nbr_off<L, j>(o))), a);
-        if ((walls >> (2 * P + 1)) & 1U) f[j] = ld<S, L, j, S::scaled>(base + (a.pa_off[P] + n), a);
-        bounce_fixup<L, S, P + 1>(a, base, n, o, walls, f);
-    }
-}
-
 template <class L, class S, bool LES, bool FLAGS, bool GRAY>
 __global__ void __launch_bounds__(128, pair_min_blocks<S>()) k_step_x2(const __grid_constant__ LbmArgs a) {
     using R = typename S::R;
@@ -261,7 +249,7 @@ __global__ void __launch_bounds__(128, pair_min_blocks<S>()) k_step_x2(const __g
     if constexpr (FLAGS) {
         if (c.live0 && (fl0 & (kFlagNearWall | kFlagNearMoving))) {
             const Nbr o = make_nbr(a, c.x0, y, z);
-            if (fl0 & kFlagNearWall) bounce_fixup<L, S>(a, base, c.n0, o, wall_links<L>(a, c.n0, o), f0);
+            if (fl0 & kFlagNearWall) bounce_fixup<L, S>(a, base, c.n0, o, a.wall_mask[c.n0], f0);
             if constexpr (S::scaled)
                 gather_fixup_scaled<L>(a, c.n0, o, fl0, f0);
             else
@@ -269,7 +257,7 @@ __global__ void __launch_bounds__(128, pair_min_blocks<S>()) k_step_x2(const __g
         }
         if (c.live1 && (fl1 & (kFlagNearWall | kFlagNearMoving))) {
             const Nbr o = make_nbr(a, c.x0 + 1U, y, z);
-            if (fl1 & kFlagNearWall) bounce_fixup<L, S>(a, base, c.n0 + 1U, o, wall_links<L>(a, c.n0 + 1U, o), f1);
+            if (fl1 & kFlagNearWall) bounce_fixup<L, S>(a, base, c.n0 + 1U, o, a.wall_mask[c.n0 + 1U], f1);
             if constexpr (S::scaled)
                 gather_fixup_scaled<L>(a, c.n0 + 1U, o, fl1, f1);
             else
