@@ -6,7 +6,7 @@ front end that mirrors the reference's ``cfd::lbm`` solver API.  There is no
 CPU fallback: without the built library or a CUDA device every solver call
 raises.
 """
-from .bindings import CfdxError, CudaError, NonFiniteError, SolverLibrary, load
+from .bindings import CfdxError, CheckpointError, CudaError, NonFiniteError, SolverLibrary, load
 from .lbm import (
     DeviceAccelerationView,
     DeviceMacroscopicView,
@@ -21,6 +21,7 @@ from .lbm import (
 
 __all__ = [
     "CfdxError",
+    "CheckpointError",
     "CudaError",
     "NonFiniteError",
     "SolverLibrary",

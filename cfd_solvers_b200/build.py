@@ -3,7 +3,7 @@
 Compiles every ``csrc/*.cu`` with nvcc (``-gencode arch=compute_100a,code=sm_100a``)
 in parallel into ``_build/`` at the repository root and links the shared
 library next to this file, where ``cfd_solvers_b200.bindings`` loads it.  The
-C++ front end (``apps/cfd_bench.cpp``, ``include/cfd/solvers/lbm/esoteric_pull_cuda.hpp``)
+C++ front end (``cfd_solvers_b200/apps/cfd_bench.cpp``, ``include/cfd/solvers/lbm/esoteric_pull_cuda.hpp``)
 links against the same library.
 
 Usage: ``python -m cfd_solvers_b200.build [--force] [--jobs N]``.
@@ -24,8 +24,8 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 BUILD = ROOT / "_build"
 LIB = PKG / "libcfdx_lbm.so"
-APPS = ROOT / "apps"
-BENCH_BIN = ROOT / "apps" / "cfd-bench-cuda"
+APPS = PKG / "apps"
+BENCH_BIN = PKG / "cfd-bench-cuda"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr",
@@ -90,7 +90,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     if bench_src.exists() and (force or _stale(BENCH_BIN, [bench_src, LIB] + _headers() +
                                                list((INCLUDE / "cfd" / "solvers" / "lbm").glob("*.hpp")))):
         cmd = [host_cxx(), "-std=c++20", "-O2", f"-I{INCLUDE}", str(bench_src), "-o", str(BENCH_BIN),
-               f"-L{PKG}", "-lcfdx_lbm", f"-Wl,-rpath,$ORIGIN/../cfd_solvers_b200"]
+               f"-L{PKG}", "-lcfdx_lbm", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -18,6 +18,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "handle_access.h"
 #include "lbm_launch.h"
@@ -474,6 +475,16 @@ cudaError_t launch_adjoint_seed(const KernelKey& k, const AdjointArgs& a, dim3 g
     case kStoreF32: return Launcher<kStoreF32>::adjoint_seed(k, a, g, b, s);
     case kStoreF64: return Launcher<kStoreF64>::adjoint_seed(k, a, g, b, s);
     case kStoreF16S: return Launcher<kStoreF16S>::adjoint_seed(k, a, g, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_slot_io(const KernelKey& k, const LbmArgs& a, int d, float* buf, bool in, dim3 g, dim3 b,
+                           cudaStream_t s) {
+    switch (k.storage) {
+    case kStoreF32: return Launcher<kStoreF32>::slot_io(k, a, d, buf, in, g, b, s);
+    case kStoreF64: return Launcher<kStoreF64>::slot_io(k, a, d, buf, in, g, b, s);
+    case kStoreF16S: return Launcher<kStoreF16S>::slot_io(k, a, d, buf, in, g, b, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -978,6 +989,138 @@ CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int variant)
                     "the paired-cell kernel needs FP32/FP16 storage, an even nx, q*cells < 2^32 and block_x a "
                     "multiple of 32");
         h->choose_variant();
+    });
+}
+
+// ---------------------------------------------------------- checkpoints
+// CFDCHK3 version 1, the layout of the reference's distributed two-grid
+// checkpoint (include/cfd/solvers/lbm/distributed_pull.hpp:176-245): 8-byte
+// magic "CFDCHK3\0", u32 version 1, u32 endian marker 0x01020304, u32 q, the
+// global extent, brick begin and brick extent as 3 x u64 each (one brick:
+// begin 0, extent = global), u64 time step, f32 tau and ax/ay/az, then q*N
+// f32 populations in [d][z][y][x] order.  The populations are what each fluid
+// cell gathers at the stored time step (before any moving-wall correction),
+// 0 on walls; the time step's parity places them back into the in-place
+// slots, so a restart continues bit for bit (FP32 storage; FP16 restarts
+// re-encode the decoded values, FP64 ones keep FP32 precision).
+extern "C++" {
+namespace {
+
+constexpr char kCheckpointMagic[8] = {'C', 'F', 'D', 'C', 'H', 'K', '3', '\0'};
+
+struct File {
+    std::FILE* f = nullptr;
+    ~File() {
+        if (f) std::fclose(f);
+    }
+};
+
+template <class T> void put(std::FILE* f, T v, const char* path) {
+    if (std::fwrite(&v, sizeof v, 1, f) != 1) fail(CFDX_ERR_IO, std::string("checkpoint write failed: ") + path);
+}
+template <class T> T get(std::FILE* f, const char* path) {
+    T v{};
+    if (std::fread(&v, sizeof v, 1, f) != 1) fail(CFDX_ERR_IO, std::string("truncated checkpoint: ") + path);
+    return v;
+}
+
+float* checkpoint_scratch(cfdx_lbm* h) {
+    if (!h->macro_scratch)
+        h->macro_scratch = static_cast<float*>(device_alloc(4U * h->N * sizeof(float), "macroscopic scratch"));
+    return h->macro_scratch;
+}
+
+} // namespace
+} // extern "C++"
+
+CFDX_API int cfdx_lbm_checkpoint_save(cfdx_lbm* h, const char* path) {
+    return guarded([&] {
+        checked(h);
+        require(path != nullptr, "null checkpoint path");
+        File file;
+        file.f = std::fopen(path, "wb");
+        if (!file.f) fail(CFDX_ERR_IO, std::string("cannot open checkpoint for writing: ") + path);
+        std::FILE* f = file.f;
+        if (std::fwrite(kCheckpointMagic, 1, 8, f) != 8) fail(CFDX_ERR_IO, std::string("checkpoint write failed: ") + path);
+        put<std::uint32_t>(f, 1U, path);
+        put<std::uint32_t>(f, 0x01020304U, path);
+        put<std::uint32_t>(f, static_cast<std::uint32_t>(h->key.q), path);
+        const std::uint64_t ext[3] = {h->cfg.nx, h->cfg.ny, h->cfg.nz};
+        for (int r = 0; r < 3; ++r) {
+            const std::uint64_t begin[3] = {0, 0, 0};
+            const std::uint64_t* v = r == 1 ? begin : ext;
+            for (int k = 0; k < 3; ++k) put<std::uint64_t>(f, v[k], path);
+        }
+        put<std::uint64_t>(f, h->t, path);
+        put<float>(f, h->cfg.tau, path);
+        put<float>(f, h->cfg.acceleration_x, path);
+        put<float>(f, h->cfg.acceleration_y, path);
+        put<float>(f, h->cfg.acceleration_z, path);
+        float* dev = checkpoint_scratch(h);
+        std::vector<float> host(h->N);
+        for (int d = 0; d < h->key.q; ++d) {
+            check_cuda(launch_slot_io(h->key, h->args(), d, dev, false, h->grid(), h->block(), h->stream),
+                       "checkpoint read kernel");
+            check_cuda(cudaMemcpyAsync(host.data(), dev, h->N * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+                       "cudaMemcpyAsync (checkpoint)");
+            h->sync();
+            h->d2h += h->N * sizeof(float);
+            if (std::fwrite(host.data(), sizeof(float), h->N, f) != h->N)
+                fail(CFDX_ERR_IO, std::string("checkpoint write failed: ") + path);
+        }
+        if (std::fflush(f) != 0) fail(CFDX_ERR_IO, std::string("checkpoint write failed: ") + path);
+    });
+}
+
+CFDX_API int cfdx_lbm_checkpoint_load(cfdx_lbm* h, const char* path) {
+    return guarded([&] {
+        checked(h);
+        require(path != nullptr, "null checkpoint path");
+        File file;
+        file.f = std::fopen(path, "rb");
+        if (!file.f) fail(CFDX_ERR_IO, std::string("cannot open checkpoint for reading: ") + path);
+        std::FILE* f = file.f;
+        char magic[8] = {0};
+        if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCheckpointMagic, 8) != 0)
+            fail(CFDX_ERR_IO, "invalid checkpoint magic");
+        const auto version = get<std::uint32_t>(f, path);
+        const auto endian = get<std::uint32_t>(f, path);
+        const auto q = get<std::uint32_t>(f, path);
+        if (version != 1U || endian != 0x01020304U || q != static_cast<std::uint32_t>(h->key.q))
+            fail(CFDX_ERR_IO, "unsupported checkpoint format/descriptor");
+        const std::uint64_t ext[3] = {h->cfg.nx, h->cfg.ny, h->cfg.nz};
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 3; ++k) {
+                const auto v = get<std::uint64_t>(f, path);
+                if (v != (r == 1 ? 0U : ext[k])) fail(CFDX_ERR_IO, "checkpoint decomposition does not match the lattice");
+            }
+        const auto t = get<std::uint64_t>(f, path);
+        const float tau = get<float>(f, path), ax = get<float>(f, path), ay = get<float>(f, path),
+                    az = get<float>(f, path);
+        if (tau != h->cfg.tau || ax != h->cfg.acceleration_x || ay != h->cfg.acceleration_y ||
+            az != h->cfg.acceleration_z)
+            fail(CFDX_ERR_IO, "checkpoint LBM configuration mismatch");
+        // The whole payload must be present before the lattice is touched.
+        const long header = std::ftell(f);
+        if (header < 0 || std::fseek(f, 0, SEEK_END) != 0) fail(CFDX_ERR_IO, std::string("cannot size checkpoint: ") + path);
+        const long total = std::ftell(f);
+        const unsigned long long payload = static_cast<unsigned long long>(h->key.q) * h->N * sizeof(float);
+        if (total < 0 || static_cast<unsigned long long>(total - header) != payload)
+            fail(CFDX_ERR_IO, std::string("checkpoint payload size mismatch (truncated or trailing data): ") + path);
+        if (std::fseek(f, header, SEEK_SET) != 0) fail(CFDX_ERR_IO, std::string("cannot read checkpoint: ") + path);
+        float* dev = checkpoint_scratch(h);
+        std::vector<float> host(h->N);
+        h->adj.ready = false;
+        h->t = t;
+        const LbmArgs a = h->args(); // slot tables of the stored time step's parity
+        for (int d = 0; d < h->key.q; ++d) {
+            if (std::fread(host.data(), sizeof(float), h->N, f) != h->N)
+                fail(CFDX_ERR_IO, std::string("truncated checkpoint: ") + path);
+            upload(h, dev, host.data(), h->N * sizeof(float), CFDX_HOST);
+            check_cuda(launch_slot_io(h->key, a, d, dev, true, h->grid(), h->block(), h->stream),
+                       "checkpoint write kernel");
+        }
+        h->sync();
     });
 }
 

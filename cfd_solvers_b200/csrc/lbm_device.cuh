@@ -1168,6 +1168,83 @@ __global__ void __launch_bounds__(128) k_logical(const __grid_constant__ LbmArgs
         out[static_cast<std::size_t>(d) * a.N + n] = wall ? OutT(0) : OutT(absolute<S, L>(fin[d], d));
 }
 
+// Checkpoint I/O of one direction d: the value a fluid cell gathers for d at
+// the current parity, before any moving-wall correction (so that writing it
+// back with k_slot_in restores the lattice exactly).  Walls: 0 / untouched.
+template <class L, class S, bool FLAGS, int P = 0>
+__device__ __forceinline__ typename S::T* slot_of(const LbmArgs& a, u32 n, const Nbr& o, unsigned walls, int d) {
+    if constexpr (P < L::PAIRS) {
+        constexpr int i = 2 * P + 1, j = i + 1;
+        if (d == i) {
+            const bool sb = ((walls >> (2 * P)) & 1U) != 0U;
+            return Slots<S, false>::at(a, !sb, P, n + nbr_off<L, j>(o));
+        }
+        if (d == j) {
+            const bool sf = ((walls >> (2 * P + 1)) & 1U) != 0U;
+            return Slots<S, false>::at(a, sf, P, n);
+        }
+        return slot_of<L, S, FLAGS, P + 1>(a, n, o, walls, d);
+    } else {
+        return Slots<S, false>::rest(a, n);
+    }
+}
+
+template <class L, class S, bool FLAGS>
+__global__ void __launch_bounds__(128) k_slot_out(const __grid_constant__ LbmArgs a, int d, float* out) {
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
+    const u32 n = (z * a.ny + y) * a.nx + x;
+    unsigned walls = 0U;
+    if constexpr (FLAGS) {
+        const std::uint8_t flag = a.flags[n];
+        if (flag & kFlagTypeMask) {
+            out[n] = 0.0F;
+            return;
+        }
+        if (flag & kFlagNearWall) walls = a.wall_mask[n];
+    }
+    const typename S::T* p = slot_of<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), walls, d);
+    if constexpr (sizeof(typename S::T) == 2) {
+        // FP16: deviation h / s_d plus the weight of direction d
+        float w = d == 0 ? float(L::w(0)) : 0.0F;
+        static_for_pairs<L>([&](auto PP) {
+            constexpr int i = 2 * decltype(PP)::value + 1;
+            if (d == i || d == i + 1) w = float(L::w(i));
+        });
+        out[n] = __half2float(*p) * a.inv_scale[d] + w;
+    } else {
+        out[n] = float(*p);
+    }
+}
+
+template <class L, class S, bool FLAGS>
+__global__ void __launch_bounds__(128) k_slot_in(const __grid_constant__ LbmArgs a, int d, const float* in) {
+    const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    const u32 z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
+    const u32 n = (z * a.ny + y) * a.nx + x;
+    unsigned walls = 0U;
+    if constexpr (FLAGS) {
+        const std::uint8_t flag = a.flags[n];
+        if (flag & kFlagTypeMask) return;
+        if (flag & kFlagNearWall) walls = a.wall_mask[n];
+    }
+    typename S::T* p = slot_of<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), walls, d);
+    if constexpr (sizeof(typename S::T) == 2) {
+        float w = d == 0 ? float(L::w(0)) : 0.0F;
+        static_for_pairs<L>([&](auto PP) {
+            constexpr int i = 2 * decltype(PP)::value + 1;
+            if (d == i || d == i + 1) w = float(L::w(i));
+        });
+        *p = __float2half_rn((in[n] - w) * a.scale[d]);
+    } else {
+        *p = typename S::T(in[n]);
+    }
+}
+
 // Fluid-cell reduction with FP64 accumulation (reference
 // esoteric_pull.hpp:211-255 accumulates per-cell FP32 sums in FP64; the
 // reference's SYCL total_mass, esoteric_pull_sycl.hpp:327-339, used FP32).

@@ -41,6 +41,9 @@ template <int STORAGE> struct Launcher {
                                cudaStream_t s);
     static cudaError_t reduce(const KernelKey& k, const LbmArgs& a, double* partials, int blocks, double* out,
                               cudaStream_t s);
+    // Checkpoint I/O of direction d (k_slot_out / k_slot_in).
+    static cudaError_t slot_io(const KernelKey& k, const LbmArgs& a, int d, float* buffer, bool in, dim3 grid,
+                               dim3 block, cudaStream_t s);
     // Adjoint (lbm_adjoint.cuh); all three need 32-bit slot offsets.
     static cudaError_t step_oop(const KernelKey& k, const LbmArgs& src, const LbmArgs& dst, dim3 grid, dim3 block,
                                 cudaStream_t s);
@@ -60,6 +63,8 @@ cudaError_t launch_step_oop(const KernelKey& k, const LbmArgs& src, const LbmArg
                             cudaStream_t s);
 cudaError_t launch_adjoint_seed(const KernelKey& k, const AdjointArgs& a, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t launch_adjoint_step(const KernelKey& k, const AdjointArgs& a, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t launch_slot_io(const KernelKey& k, const LbmArgs& a, int d, float* buffer, bool in, dim3 grid,
+                           dim3 block, cudaStream_t s);
 cudaError_t launch_sum_partials(const double* partials, std::size_t count, double* out, cudaStream_t s);
 cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out,
                                  std::uint32_t* mask, dim3 grid, dim3 block, cudaStream_t s);

@@ -191,4 +191,25 @@ cudaError_t Launcher<STORAGE>::adjoint_step(const KernelKey& k, const AdjointArg
     });
 }
 
+template <int STORAGE>
+cudaError_t Launcher<STORAGE>::slot_io(const KernelKey& k, const LbmArgs& a, int d, float* buf, bool in, dim3 g,
+                                       dim3 b, cudaStream_t s) {
+    using S = typename StorageOf<STORAGE>::type;
+    return with_lattice(k.q, [&](auto lat) {
+        using L = decltype(lat);
+        if (in) {
+            if (k.flags)
+                k_slot_in<L, S, true><<<g, b, 0, s>>>(a, d, buf);
+            else
+                k_slot_in<L, S, false><<<g, b, 0, s>>>(a, d, buf);
+        } else {
+            if (k.flags)
+                k_slot_out<L, S, true><<<g, b, 0, s>>>(a, d, buf);
+            else
+                k_slot_out<L, S, false><<<g, b, 0, s>>>(a, d, buf);
+        }
+        return cudaGetLastError();
+    });
+}
+
 } // namespace cfdx

@@ -371,6 +371,14 @@ class EsotericPullCudaSolver:
         """Threads per block and step-kernel variant (0 auto, 1 one cell, 2 paired cells)."""
         self._call("cfdx_lbm_set_launch_shape", int(block_x), int(block_y), int(variant))
 
+    def save_checkpoint(self, path):
+        """CFDCHK3 checkpoint of the current state (reference DistributedPullSolver::save_checkpoint)."""
+        self._call("cfdx_lbm_checkpoint_save", str(path).encode())
+
+    def load_checkpoint(self, path):
+        """Restores a CFDCHK3 checkpoint written for this configuration (time step and populations)."""
+        self._call("cfdx_lbm_checkpoint_load", str(path).encode())
+
     def set_tau(self, tau: float):
         """Symmetric relaxation time of the following steps (the adjoint's dJ/dtau variable)."""
         self._call("cfdx_lbm_set_tau", float(tau))

@@ -1,0 +1,261 @@
+// C++20 front end of the B200 in-place Esoteric-Pull engine.
+//
+// cfd::lbm::EsotericPullCudaSolver<Descriptor> has the interface of the
+// reference's CPU solver cfd::lbm::EsotericPullSolver<Descriptor>
+// (include/cfd/solvers/lbm/esoteric_pull.hpp:104-515) and of its SYCL twin
+// (esoteric_pull_sycl.hpp:18-475): same constructor argument, method names,
+// argument meaning and exception types, so a driver switches by changing the
+// class name.  Every call goes through the C ABI of libcfdx_lbm.so
+// (include/cfdx_lbm.h); the step runs as sm_100a CUDA kernels, with no CPU
+// fallback.
+//
+// Descriptor: any type with `static constexpr int q` equal to 19 or 27 --
+// the reference's D3Q19Descriptor / D3Q27Descriptor, or the tags
+// cfd::lbm::cuda::D3Q19 / D3Q27 below when the reference headers are absent.
+// Config: any type with the members of the reference's InPlaceLbmConfig
+// (nx, ny, nz, tau, acceleration_x/y/z, smagorinsky_les), e.g.
+// cfd::lbm::cuda::InPlaceLbmConfig, which adds the engine's extensions.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <new>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "cfdx_lbm.h"
+
+namespace cfd::lbm {
+
+namespace cuda {
+
+struct D3Q19 {
+    static constexpr int q = 19;
+};
+struct D3Q27 {
+    static constexpr int q = 27;
+};
+
+enum class Collision { bgk = CFDX_BGK, trt = CFDX_TRT };
+enum class Storage { fp32 = CFDX_STORE_F32, fp16s = CFDX_STORE_F16S, fp64 = CFDX_STORE_F64 };
+enum class Fp16Rounding { nearest = CFDX_ROUND_NEAREST, stochastic = CFDX_ROUND_STOCHASTIC };
+
+// The reference's InPlaceLbmConfig (esoteric_pull.hpp:20-29) plus the engine's extensions.
+struct InPlaceLbmConfig {
+    std::size_t nx{128};
+    std::size_t ny{128};
+    std::size_t nz{128};
+    float tau{0.6F};
+    float acceleration_x{0.0F};
+    float acceleration_y{0.0F};
+    float acceleration_z{0.0F};
+    bool smagorinsky_les{false};
+    // extensions
+    Collision collision{Collision::bgk};
+    Storage storage{Storage::fp32};
+    float smagorinsky_cs{0.0F}; // <= 0: the reference's fixed coefficient
+    float trt_magic{3.0F / 16.0F};
+    float trt_tau_minus{0.0F}; // > 0: fixed antisymmetric relaxation time
+    int device{0};
+    Fp16Rounding fp16_rounding{Fp16Rounding::stochastic};
+    std::uint32_t rounding_seed{0};
+};
+
+// rho and u + a/2 per cell (reference MacroscopicFields, esoteric_pull.hpp:31-36).
+struct MacroscopicFields {
+    std::vector<float> rho;
+    std::vector<float> ux;
+    std::vector<float> uy;
+    std::vector<float> uz;
+};
+
+// Converts a C ABI status into the reference's exception types.
+inline void check(int status, const char* what) {
+    if (status == CFDX_OK) return;
+    char buffer[1024] = {0};
+    cfdx_last_error(buffer, sizeof buffer);
+    const std::string message = std::string(what) + ": " + buffer;
+    switch (status) {
+    case CFDX_ERR_INVALID: throw std::invalid_argument(message);
+    case CFDX_ERR_RANGE: throw std::out_of_range(message);
+    case CFDX_ERR_OOM: throw std::bad_alloc();
+    default: throw std::runtime_error(message);
+    }
+}
+
+template <class C, class = void> struct has_extensions : std::false_type {};
+template <class C> struct has_extensions<C, std::void_t<decltype(std::declval<C>().storage)>> : std::true_type {};
+
+} // namespace cuda
+
+template <class Descriptor> class EsotericPullCudaSolver {
+public:
+    static constexpr int q = Descriptor::q;
+    static constexpr std::size_t pair_count = static_cast<std::size_t>((q - 1) / 2);
+    static_assert(q == 19 || q == 27, "the B200 engine implements D3Q19 and D3Q27");
+
+    template <class Config = cuda::InPlaceLbmConfig>
+    explicit EsotericPullCudaSolver(const Config& config = Config{}) {
+        cfdx_lbm_config c;
+        cuda::check(cfdx_lbm_config_default(&c), "cfdx_lbm_config_default");
+        c.nx = config.nx;
+        c.ny = config.ny;
+        c.nz = config.nz;
+        c.tau = config.tau;
+        c.acceleration_x = config.acceleration_x;
+        c.acceleration_y = config.acceleration_y;
+        c.acceleration_z = config.acceleration_z;
+        c.smagorinsky_les = config.smagorinsky_les ? 1 : 0;
+        c.lattice = q;
+        if constexpr (cuda::has_extensions<Config>::value) {
+            c.collision = static_cast<int>(config.collision);
+            c.storage = static_cast<int>(config.storage);
+            c.smagorinsky_cs = config.smagorinsky_cs;
+            c.trt_magic = config.trt_magic;
+            c.trt_tau_minus = config.trt_tau_minus;
+            c.device = config.device;
+            c.fp16_rounding = static_cast<int>(config.fp16_rounding);
+            c.rounding_seed = config.rounding_seed;
+        }
+        char error[1024] = {0};
+        const int status = cfdx_lbm_create(&c, &handle_, error, sizeof error);
+        if (status != CFDX_OK) {
+            handle_ = nullptr;
+            cuda::check(status, "cfdx_lbm_create");
+        }
+        config_ = c;
+        cells_ = c.nx * c.ny * c.nz;
+    }
+
+    ~EsotericPullCudaSolver() {
+        if (handle_) cfdx_lbm_destroy(handle_);
+    }
+    EsotericPullCudaSolver(const EsotericPullCudaSolver&) = delete;
+    EsotericPullCudaSolver& operator=(const EsotericPullCudaSolver&) = delete;
+    EsotericPullCudaSolver(EsotericPullCudaSolver&& other) noexcept
+        : handle_(std::exchange(other.handle_, nullptr)), config_(other.config_), cells_(other.cells_),
+          mask_(std::move(other.mask_)), local_(other.local_) {}
+
+    // ------------------------------------------------ reference API (CPU class)
+    void initialize_uniform(float rho = 1.0F, float ux = 0.0F, float uy = 0.0F, float uz = 0.0F) {
+        cuda::check(cfdx_lbm_init_uniform(handle_, rho, ux, uy, uz), "initialize_uniform");
+    }
+    void initialize_taylor_green(float amplitude = 0.03F) {
+        cuda::check(cfdx_lbm_init_taylor_green(handle_, amplitude), "initialize_taylor_green");
+    }
+    void step(std::size_t count = 1) { cuda::check(cfdx_lbm_step(handle_, count), "step"); }
+
+    void set_local_body_acceleration(std::span<const float> ax, std::span<const float> ay, std::span<const float> az) {
+        if (ax.size() != cells_ || ay.size() != cells_ || az.size() != cells_)
+            throw std::invalid_argument("local body acceleration size mismatch");
+        std::vector<float> packed;
+        packed.reserve(3 * cells_);
+        packed.insert(packed.end(), ax.begin(), ax.end());
+        packed.insert(packed.end(), ay.begin(), ay.end());
+        packed.insert(packed.end(), az.begin(), az.end());
+        cuda::check(cfdx_lbm_set_local_acceleration(handle_, packed.data(), CFDX_HOST), "set_local_body_acceleration");
+        local_ = true;
+    }
+    void clear_local_body_acceleration() noexcept {
+        cfdx_lbm_set_local_acceleration(handle_, nullptr, CFDX_HOST);
+        local_ = false;
+    }
+    [[nodiscard]] bool has_local_body_acceleration() const noexcept { return local_; }
+
+    // mask != 0 => solid (stationary half-way bounce-back wall)
+    void set_solid_mask(std::span<const std::uint8_t> mask) {
+        if (mask.size() != cells_) throw std::invalid_argument("LBM solid mask size mismatch");
+        std::vector<std::uint8_t> flags(mask.size());
+        for (std::size_t n = 0; n < mask.size(); ++n) flags[n] = mask[n] != 0U ? 1U : 0U;
+        cuda::check(cfdx_lbm_set_flags(handle_, flags.data(), CFDX_HOST), "set_solid_mask");
+        mask_ = std::move(flags);
+    }
+    void clear_solid_mask() noexcept {
+        cfdx_lbm_set_flags(handle_, nullptr, CFDX_HOST);
+        mask_.clear();
+    }
+    [[nodiscard]] bool has_solid_mask() const noexcept { return !mask_.empty(); }
+    [[nodiscard]] const std::vector<std::uint8_t>& solid_mask() const noexcept { return mask_; }
+
+    [[nodiscard]] cuda::MacroscopicFields compute_macroscopic() const {
+        cuda::MacroscopicFields f;
+        f.rho.resize(cells_);
+        f.ux.resize(cells_);
+        f.uy.resize(cells_);
+        f.uz.resize(cells_);
+        cuda::check(cfdx_lbm_macroscopic(handle_, f.rho.data(), f.ux.data(), f.uy.data(), f.uz.data(), CFDX_HOST),
+                    "compute_macroscopic");
+        return f;
+    }
+    [[nodiscard]] double mass() const { return reduce()[0]; }
+    [[nodiscard]] double kinetic_energy() const { return reduce()[4]; }
+    [[nodiscard]] float max_speed() const { return static_cast<float>(reduce()[5]); }
+    [[nodiscard]] std::vector<float> logical_populations() const {
+        std::vector<float> out(static_cast<std::size_t>(q) * cells_);
+        cuda::check(cfdx_lbm_logical_populations(handle_, out.data(), CFDX_HOST), "logical_populations");
+        return out;
+    }
+    [[nodiscard]] const cfdx_lbm_config& config() const noexcept { return config_; }
+    [[nodiscard]] std::size_t cells() const noexcept { return cells_; }
+    [[nodiscard]] std::uint64_t time_step() const { return info().time_step; }
+    [[nodiscard]] std::size_t population_bytes() const { return info().population_bytes; }
+    [[nodiscard]] std::size_t two_lattice_population_bytes() const noexcept { return 2U * population_bytes(); }
+
+    // ------------------------------------------------ reference API (SYCL class)
+    void wait() { cuda::check(cfdx_lbm_synchronize(handle_), "wait"); }
+    [[nodiscard]] double total_mass() const { return mass(); }
+    [[nodiscard]] std::size_t resident_bytes() const { return info().resident_bytes; }
+    [[nodiscard]] std::string device_name() const { return "CUDA device " + std::to_string(config_.device); }
+
+    // ------------------------------------------------------------ extensions
+    // Cell flags: 0 fluid, 1 wall, 2..15 moving wall (velocity from set_wall_velocity).
+    void set_flags(std::span<const std::uint8_t> flags) {
+        if (flags.size() != cells_) throw std::invalid_argument("LBM flag field size mismatch");
+        cuda::check(cfdx_lbm_set_flags(handle_, flags.data(), CFDX_HOST), "set_flags");
+        mask_.assign(flags.begin(), flags.end());
+    }
+    void set_wall_velocity(int wall_id, float ux, float uy, float uz) {
+        cuda::check(cfdx_lbm_set_wall_velocity(handle_, wall_id, ux, uy, uz), "set_wall_velocity");
+    }
+    void set_solid_fraction(std::span<const float> ns) {
+        if (ns.size() != cells_) throw std::invalid_argument("solid fraction size mismatch");
+        cuda::check(cfdx_lbm_set_solid_fraction(handle_, ns.data(), CFDX_HOST), "set_solid_fraction");
+    }
+    // mass, momentum xyz, kinetic energy, max |u|, non-finite cells (FP64 sums)
+    [[nodiscard]] std::vector<double> reduce() const {
+        std::vector<double> out(CFDX_REDUCE_COUNT);
+        cuda::check(cfdx_lbm_reduce(handle_, out.data()), "reduce");
+        return out;
+    }
+    [[nodiscard]] double checksum() const {
+        double c = 0.0;
+        cuda::check(cfdx_lbm_checksum(handle_, &c), "checksum");
+        return c;
+    }
+    void save_checkpoint(const std::string& path) const {
+        cuda::check(cfdx_lbm_checkpoint_save(handle_, path.c_str()), "save_checkpoint");
+    }
+    void load_checkpoint(const std::string& path) {
+        cuda::check(cfdx_lbm_checkpoint_load(handle_, path.c_str()), "load_checkpoint");
+    }
+    [[nodiscard]] cfdx_lbm* native_handle() const noexcept { return handle_; }
+
+private:
+    [[nodiscard]] cfdx_lbm_info info() const {
+        cfdx_lbm_info i{};
+        cuda::check(cfdx_lbm_get_info(handle_, &i), "get_info");
+        return i;
+    }
+
+    cfdx_lbm* handle_{nullptr};
+    cfdx_lbm_config config_{};
+    std::size_t cells_{0};
+    std::vector<std::uint8_t> mask_;
+    bool local_{false};
+};
+
+} // namespace cfd::lbm

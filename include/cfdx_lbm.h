@@ -250,6 +250,18 @@ CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, 
  * serialised by the caller. */
 CFDX_API int cfdx_lbm_reduce_noalloc(cfdx_lbm* lbm, double* out);
 
+/* Checkpoint files in the reference's CFDCHK3 version-1 layout
+ * (include/cfd/solvers/lbm/distributed_pull.hpp:176-245, one brick covering
+ * the lattice): header, time step, tau and acceleration, then q*N float
+ * populations [d][z][y][x] -- what each fluid cell gathers at the stored
+ * time step (before moving-wall corrections), 0 on walls.  Load restores the
+ * time step and the lattice so that stepping continues bit for bit (FP32
+ * storage); the header must match the handle (q, extents, tau, acceleration)
+ * and the payload must be complete, else CFDX_ERR_IO and nothing changes.
+ * Reference: DistributedPullSolver::save_checkpoint / load_checkpoint. */
+CFDX_API int cfdx_lbm_checkpoint_save(cfdx_lbm* lbm, const char* path);
+CFDX_API int cfdx_lbm_checkpoint_load(cfdx_lbm* lbm, const char* path);
+
 /* Symmetric relaxation time (> 0.5) for the following steps; the adjoint's
  * dJ/dtau is taken with respect to it.  Reference: InPlaceLbmConfig::tau,
  * esoteric_pull.hpp:20-29 (fixed at construction there). */
