@@ -52,6 +52,10 @@ def parse_args(argv=None):
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-differentiation", action="store_true",
                    help="skip the adjoint workloads (128^3 D3Q19 FP32 and 256^3 D3Q27 FP16 gray TRT)")
+    p.add_argument("--case", choices=["cavity", "adjoint", "precision"], default="cavity",
+                   help="cavity: the headline line (default); adjoint / precision: only that workload at --n "
+                        "(adjoint: gray TRT --lattice/--storage, --steps steps; precision: n x n/2 x n/2 sphere "
+                        "pack, --steps steps), one JSON line -- small cases for profiling")
     p.add_argument("--no-precision", action="store_true",
                    help="skip the 512x256x256 sphere-pack FP16/FP32/FP64 precision study (20000 steps)")
     return p.parse_args(argv)
@@ -512,6 +516,16 @@ def main(argv=None):
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device (no CPU fallback)")
     torch.cuda.set_device(local_rank)
+    if args.case != "cavity":
+        if world != 1:
+            raise SystemExit("--case adjoint/precision run on one GPU")
+        if args.case == "adjoint":
+            out, _, _ = adjoint_case(torch, cs, args.lattice, args.n, args.storage, args.steps,
+                                     min(64, args.steps), local_rank)
+        else:
+            out = precision_study(torch, cs, local_rank, shape=(args.n, args.n // 2, args.n // 2), steps=args.steps)
+        print(json.dumps(out), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
