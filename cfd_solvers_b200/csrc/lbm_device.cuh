@@ -1245,6 +1245,28 @@ __global__ void __launch_bounds__(128) k_slot_in(const __grid_constant__ LbmArgs
     }
 }
 
+// Counts fluid cells (out[0]) and fluid cells with a wall neighbour (out[1])
+// of the internal flags; the host uses the ratio to pick the step kernel.
+static __global__ void __launch_bounds__(256) k_count_flags(const std::uint8_t* flags, u32 n, unsigned long long* out) {
+    unsigned long long fluid = 0, near = 0;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const std::uint8_t f = flags[i];
+        if ((f & kFlagTypeMask) == 0) {
+            ++fluid;
+            if (f & kFlagNearWall) ++near;
+        }
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        fluid += __shfl_down_sync(0xffffffffU, fluid, s);
+        near += __shfl_down_sync(0xffffffffU, near, s);
+    }
+    if ((threadIdx.x & 31U) == 0U) {
+        atomicAdd(out, fluid);
+        atomicAdd(out + 1, near);
+    }
+}
+
 // Fluid-cell reduction with FP64 accumulation (reference
 // esoteric_pull.hpp:211-255 accumulates per-cell FP32 sums in FP64; the
 // reference's SYCL total_mass, esoteric_pull_sycl.hpp:327-339, used FP32).

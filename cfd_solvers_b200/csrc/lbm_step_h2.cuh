@@ -241,4 +241,5 @@ __global__ void __launch_bounds__(128, (LES || FLAGS) ? CFDX_H2_MIN_BLOCKS_LES :
     }
 }
 
+
 } // namespace cfdx
