@@ -9,8 +9,10 @@ one fused stream+collide launch over the whole lattice.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0).  ``value`` is whole-job GLUPS (lattice cells x
-steps / device time, max over ranks); with N > 1 every rank runs its own
-independent 512^3 lattice (weak scaling, no data-path collective).
+steps / device time, max over ranks).  With N > 1 the lattice is a
+512 x 512 x (512 N) cavity cut into z-slabs of 512^3 per GPU (weak scaling):
+every step is the step kernel on each slab plus one halo exchange per cut
+(5 plane runs each way for D3Q19, NCCL point-to-point over NVLink).
 """
 from __future__ import annotations
 
@@ -207,6 +209,64 @@ def e2e_job(torch, cs, n, steps, device):
     if red["nonfinite"]:
         raise RuntimeError("e2e job produced non-finite populations")
     return cells * steps / (t1 - t0) / 1e9, stats.host_to_device_bytes, stats.device_to_host_bytes
+
+
+def cavity_slab_flags(n: int, nz: int, planes) -> np.ndarray:
+    """cavity_flags of an n x n x nz cavity restricted to the global z `planes` (a slab's local planes)."""
+    from cfd_solvers_b200 import bindings as B
+
+    planes = np.asarray(planes)
+    fl = np.zeros((len(planes), n, n), np.uint8)
+    fl[:, :, 0] = B.WALL
+    fl[:, :, n - 1] = B.WALL
+    fl[:, 0, :] = B.WALL
+    fl[(planes == 0) | (planes == nz - 1)] = B.WALL
+    fl[:, n - 1, :] = 2
+    return fl.reshape(-1)
+
+
+def cavity_config(cs, n, nz, lattice, storage, device):
+    return cs.InPlaceLbmConfig(nx=n, ny=n, nz=nz, tau=0.51, lattice=lattice, collision="trt",
+                               trt_magic=3.0 / 16.0, smagorinsky_les=True, smagorinsky_cs=0.1, storage=storage,
+                               device=device)
+
+
+def slab_exchange_overhead(torch, cs, n, steps, device, whole_ms, slabs=2):
+    """The 512^3 cavity as `slabs` z-slabs on this one GPU, exchanged after every step.
+
+    Both slabs run the same kernels as the whole lattice; the difference in
+    device time per step is the cost of the halo copies (one copy kernel per
+    cut, both directions) and of running the slabs' steps as separate launches.
+    """
+    from cfd_solvers_b200 import slabs as S
+
+    cfg = cavity_config(cs, n, n, "d3q19", "fp32", device)
+    ss = S.virtual_slabs(cfg, slabs)
+    try:
+        for s in ss:
+            s.set_flags(cavity_slab_flags(n, n, s.slab.local_planes))
+            s.set_wall_velocity(2, 0.1, 0.0, 0.0)
+            s.initialize_uniform()
+        S.virtual_step(ss, 3)
+        torch.cuda.synchronize()
+        # the last cut's exchange makes slab 0's stream wait for every slab's work
+        stream = torch.cuda.ExternalStream(ss[0].stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        S.virtual_step(ss, steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        red = S.virtual_reduce(ss)
+        msg = ss[0].halo_bytes()
+    finally:
+        for s in ss:
+            s.close()
+    return {"slabs": slabs, "glups": n ** 3 / (ms / 1e3) / 1e9, "ms_per_step": ms,
+            "whole_lattice_ms_per_step": whole_ms, "overhead_frac": ms / whole_ms - 1.0,
+            "message_bytes": msg, "exchange_bytes_per_step": 2 * slabs * msg,
+            "launches_per_step": 2 * slabs, "nonfinite": red["nonfinite"]}
 
 
 def measure_variant(torch, cs, n, lattice, storage, steps, device):
@@ -498,6 +558,121 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+# ------------------------------------------------------------- N > 1: slabs
+def slab_main(args, torch, cs, rank, world, local_rank):
+    """Weak scaling over z-slabs: rank r owns planes [r n, (r+1) n) of an n x n x (n world) cavity."""
+    import ctypes
+    import datetime
+
+    import torch.distributed as dist
+
+    from cfd_solvers_b200.slabs import DistributedEsotericPullSolver
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device(f"cuda:{local_rank}"))
+    n = args.n
+    q = 19 if args.lattice == "d3q19" else 27
+    nz = n * world
+    cfg = cavity_config(cs, n, nz, args.lattice, args.storage, local_rank)
+
+    def build():
+        d = DistributedEsotericPullSolver(cfg)
+        return d
+
+    d = build()
+    g = d.slab
+    local_flags = cavity_slab_flags(n, nz, g.local_planes)
+    d.set_flags(local_flags, local=True)
+    d.set_wall_velocity(2, 0.1, 0.0, 0.0)
+    d.initialize_uniform()
+    d.step(args.warmup)
+    stream = d.solver.torch_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local_rank)
+    dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    e0.record(stream)
+    d.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    dist.barrier()
+    red = d.reduce()  # FP64 sums all-reduced over the ranks
+    halo = d.solver.halo_bytes()
+    d.close()
+
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    cells = n * n * nz
+    value = cells * args.steps / (ms_max / 1e3) / 1e9
+
+    # end to end: local flags from pinned host memory, init, steps, own-plane rho/u download, reductions
+    e2e = None
+    if not args.no_e2e:
+        flags_host = torch.from_numpy(local_flags).pin_memory()
+        dist.barrier()
+        t0 = time.perf_counter()
+        d = build()
+        try:
+            d.solver.library.check(d.solver.library.raw.cfdx_lbm_set_flags(
+                d.solver.handle, ctypes.c_void_p(flags_host.data_ptr()), cs.bindings.HOST))
+            d.set_wall_velocity(2, 0.1, 0.0, 0.0)
+            d.initialize_uniform()
+            d.step(args.steps)
+            d.compute_macroscopic()
+            d.reduce()
+            t1 = time.perf_counter()
+            stats = d.solver.transfer_stats()
+        finally:
+            d.close()
+        w = torch.tensor([t1 - t0], device="cuda", dtype=torch.float64)
+        dist.all_reduce(w, op=dist.ReduceOp.MAX)
+        e2e = {"value": cells * args.steps / float(w.item()) / 1e9, "unit": "GLUPS",
+               "h2d_bytes_per_step": stats.host_to_device_bytes / args.steps,
+               "d2h_bytes_per_step": stats.device_to_host_bytes / args.steps,
+               "job": f"per rank: slab flags upload (pinned) + init + {args.steps} steps with halo exchange + "
+                      "own-plane rho/u download + all-reduced FP64 reductions; host wall clock, max over ranks; "
+                      "bytes per step = rank 0's job bytes / steps"}
+
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        fluid = (n - 2) * (n - 2) * (n - 1)  # rank 0: its z = 0 plane is a wall
+        alg = fluid * bytes_per_update(q, args.storage) + n * n * (n + 2)
+        achieved = alg / (ms / args.steps / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.storage == "fp32" else "f16 storage / f32 arithmetic", "data": "synthetic",
+            "config": {
+                "workload": f"{args.lattice.upper()} lid-driven cavity {n}x{n}x{nz} in {world} z-slabs of {n}^3, "
+                            f"TRT magic 3/16 + Smagorinsky Cs 0.1, tau 0.51, lid u=(0.1,0,0), "
+                            f"{args.storage.upper()} populations, from rest",
+                "lattice": args.lattice, "n": n, "storage": args.storage, "collision": "trt+les",
+                "parallelism": f"z-slabs x{world}, halo exchange {halo} B per cut and direction per step "
+                               "(NCCL send/recv over NVLink)",
+                "l2": "populations per GPU > 126 MB L2 (no flush needed)",
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic": None, "algorithmic_bytes_per_launch": alg,
+                         "kernel": "cfdx::k_step per slab; achieved over the whole step incl. the exchange"},
+            "clocks": clocks,
+            "gpu_launches": 5 * args.steps,
+            "checks": {"nonfinite_cells": red["nonfinite"], "mass": red["mass"]},
+            "e2e": e2e,
+        }
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 # --------------------------------------------------------------------- main
 def main(argv=None):
     args = parse_args(argv)
@@ -526,13 +701,9 @@ def main(argv=None):
             out = precision_study(torch, cs, local_rank, shape=(args.n, args.n // 2, args.n // 2), steps=args.steps)
         print(json.dumps(out), flush=True)
         return 0
-    dist = None
     if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        return slab_main(args, torch, cs, rank, world, local_rank)
+    dist = None
 
     def barrier():
         if dist is not None:
@@ -577,7 +748,7 @@ def main(argv=None):
                 "workload": f"{args.lattice.upper()} lid-driven cavity {n}^3, TRT magic 3/16 + Smagorinsky Cs 0.1, "
                             f"tau 0.51, lid u=(0.1,0,0), {args.storage.upper()} populations, from rest",
                 "lattice": args.lattice, "n": n, "storage": args.storage, "collision": "trt+les",
-                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "parallelism": "single GPU",
                 "l2": f"populations {cells * q * (4 if args.storage == 'fp32' else 2) / 1e9:.1f} GB > 126 MB L2 "
                       "(no flush needed)",
                 "fluid_cells": cavity_fluid_cells(n),
@@ -616,6 +787,7 @@ def main(argv=None):
             d27 = measure_variant(torch, cs, n, "d3q27", "fp32", vs, local_rank)
             d27["roofline_frac"] = d27["achieved_gbs"] / hbm_peak()[0]
             variants["d3q27_fp32"] = d27
+            variants["z_slabs_one_gpu"] = slab_exchange_overhead(torch, cs, n, vs, local_rank, ms / args.steps)
         if not args.no_differentiation:
             variants["differentiation"] = differentiation_variants(torch, cs, local_rank)
         if not args.no_precision:

@@ -41,6 +41,8 @@ FLUID = 0
 WALL = 1
 MAX_WALL_IDS = 16
 REDUCE_COUNT = 7
+SIDE_LOWER = 0
+SIDE_UPPER = 1
 
 
 class CfdxError(RuntimeError):
@@ -100,6 +102,10 @@ class cfdx_lbm_info(ctypes.Structure):
     ]
 
 
+class cfdx_halo_entry(ctypes.Structure):
+    _fields_ = [("plane", ctypes.c_uint32), ("direction", ctypes.c_uint32)]
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _f = ctypes.c_float
@@ -142,6 +148,15 @@ SIGNATURES = {
     "cfdx_lbm_adjoint_backward": (_i, [_H, _vp, _vp, _vp, _vp, _i, _vp, _i, ctypes.POINTER(ctypes.c_double)]),
     "cfdx_lbm_adjoint_memory": (_i, [_H, ctypes.POINTER(_sz)]),
     "cfdx_lbm_adjoint_release": (_i, [_H]),
+    "cfdx_lbm_create_slab": (_i, [ctypes.POINTER(cfdx_lbm_config), ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_H),
+                                  ctypes.c_char_p, _sz]),
+    "cfdx_lbm_slab_info": (_i, [_H] + [ctypes.POINTER(ctypes.c_uint32)] * 3),
+    "cfdx_halo_plan": (_i, [_i, _i, _i, ctypes.c_uint32, ctypes.POINTER(cfdx_halo_entry),
+                            ctypes.POINTER(cfdx_halo_entry), _i, ctypes.POINTER(_i)]),
+    "cfdx_lbm_halo_bytes": (_i, [_H, ctypes.POINTER(_sz)]),
+    "cfdx_lbm_halo_pack": (_i, [_H, _i, _vp]),
+    "cfdx_lbm_halo_unpack": (_i, [_H, _i, _vp]),
+    "cfdx_lbm_halo_exchange": (_i, [_H, _H]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

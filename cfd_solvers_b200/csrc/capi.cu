@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "halo.h"
 #include "handle_access.h"
 #include "lbm_launch.h"
 
@@ -164,6 +165,18 @@ struct cfdx_lbm {
     std::uint64_t h2d = 0, d2h = 0, syncs = 0;
     bool moving_walls = false; // some flag is a moving-wall id (2..15)
 
+    // z-slab of a decomposed lattice (cfdx_lbm_create_slab): nz = z_extent + 2
+    // local planes, planes 0 and nz-1 being ghost copies of the neighbours'
+    // edge planes.  Off for a plain handle.
+    struct Slab {
+        bool on = false;
+        std::uint32_t z_begin = 0, z_extent = 0, nz_global = 0;
+        std::uint8_t due = 0; // sides (bit 0 lower, bit 1 upper) whose message of the last step is not yet in
+        bool fresh = false;   // a step ran since the last initialisation or checkpoint load
+        bool whole_ring() const { return on && z_extent == nz_global; }
+    } slab;
+    cudaEvent_t event = nullptr; // ordering point between two slabs' streams (cfdx_lbm_halo_exchange)
+
     // Discrete adjoint (cfdx_lbm_adjoint_*): forward checkpoints every
     // `interval` steps, recompute frames for one segment, the adjoint lattice
     // and the gradient accumulators.  Buffers are kept for reuse until
@@ -248,6 +261,8 @@ struct cfdx_lbm {
         a.round_mask = stochastic ? 0xffffffffU : 0U;
         a.round_add = stochastic ? 0U : 0x10001000U; // nearest: half a step in both 13-bit fields
         a.round_seed = 0U;
+        // global index of local cell n: n + (z_begin - 1) * nx * ny (mod 2^32)
+        a.hash_base = slab.on ? (slab.z_begin - 1U) * static_cast<std::uint32_t>(cfg.nx * cfg.ny) : 0U;
         for (int d = 0; d < 27; ++d) {
             a.scale[d] = scale[d] == 0.0F ? 1.0F : scale[d];
             a.inv_scale[d] = 1.0F / a.scale[d];
@@ -351,13 +366,24 @@ void download(cfdx_lbm* h, void* dst, const void* src, std::size_t bytes, int wh
     h->sync();
 }
 
-void init_state(cfdx_lbm* h, const InitSpec& spec) {
+void init_state(cfdx_lbm* h, const InitSpec& in) {
+    InitSpec spec = in;
+    if (h->slab.on) {
+        spec.nz_total = h->slab.nz_global;
+        spec.z_origin = (h->slab.z_begin + h->slab.nz_global - 1U) % h->slab.nz_global;
+    } else {
+        spec.nz_total = static_cast<std::uint32_t>(h->cfg.nz);
+        spec.z_origin = 0U;
+    }
     // Zero first: wall cells and wall-only slots are never written by the init
     // kernel and must not hold stale or non-finite data.
     check_cuda(cudaMemsetAsync(h->f, 0, h->f_bytes, h->stream), "cudaMemsetAsync");
     check_cuda(launch_init(h->key, h->args(), spec, h->grid(), h->block(), h->stream), "init kernel");
     h->t = 0;
     h->adj.ready = false;
+    // Every slot a step reads now holds its own cell's state: no message is due.
+    h->slab.due = 0;
+    h->slab.fresh = false;
 }
 
 void ensure_reduce(cfdx_lbm* h) {
@@ -398,6 +424,7 @@ void release(cfdx_lbm* h) {
     device_free(h->reduce_out);
     release_adjoint(h);
     if (h->host_reduce) cudaFreeHost(h->host_reduce);
+    if (h->event) cudaEventDestroy(h->event);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -557,52 +584,98 @@ CFDX_API int cfdx_lbm_config_default(cfdx_lbm_config* c) {
     });
 }
 
+namespace {
+
+void validate_config(const cfdx_lbm_config& c) {
+    // reference esoteric_pull.hpp:111-113,292-301
+    require(c.nx >= 2 && c.ny >= 2, "LBM grid requires nx, ny >= 2");
+    require(c.nz >= 2, "3-D LBM grid requires nz >= 2");
+    require(c.tau > 0.5F && std::isfinite(c.tau), "LBM tau must be > 0.5 for positive viscosity");
+    require(c.lattice == CFDX_D3Q19 || c.lattice == CFDX_D3Q27, "lattice must be CFDX_D3Q19 or CFDX_D3Q27");
+    require(c.collision == CFDX_BGK || c.collision == CFDX_TRT, "collision must be CFDX_BGK or CFDX_TRT");
+    require(c.storage == CFDX_STORE_F32 || c.storage == CFDX_STORE_F64 || c.storage == CFDX_STORE_F16S,
+            "unknown storage");
+    require(c.fp16_rounding == CFDX_ROUND_NEAREST || c.fp16_rounding == CFDX_ROUND_STOCHASTIC,
+            "fp16_rounding must be CFDX_ROUND_NEAREST or CFDX_ROUND_STOCHASTIC");
+    require(std::isfinite(c.acceleration_x) && std::isfinite(c.acceleration_y) && std::isfinite(c.acceleration_z),
+            "acceleration must be finite");
+    if (c.collision == CFDX_TRT)
+        require(c.trt_tau_minus > 0.5F || (c.trt_tau_minus <= 0.0F && c.trt_magic > 0.0F),
+                "TRT needs trt_tau_minus > 0.5 or trt_magic > 0");
+    require(c.nx <= (1U << 30) && c.ny <= 65535U && c.nz <= 65535U, "grid extent exceeds launch limits");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        fail(CFDX_ERR_CUDA, "no CUDA device is available (the B200 engine has no CPU fallback)");
+    require(c.device >= 0 && c.device < count, "device ordinal out of range");
+}
+
+void apply_flags(cfdx_lbm* h, const std::uint8_t* flags, int where);
+
+// Sets up a new handle for the validated local configuration c.
+void build_handle(cfdx_lbm* h, const cfdx_lbm_config& c, const cfdx_lbm::Slab& slab) {
+    h->cfg = c;
+    h->slab = slab;
+    h->set_device();
+    h->N = c.nx * c.ny * c.nz;
+    require(h->N <= 0xffffffffULL, "lattice exceeds 2^32 - 1 cells");
+    h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false, 0, false, false};
+    h->choose_variant();
+    h->les_k = c.smagorinsky_les ? (c.smagorinsky_cs > 0.0F
+                                        ? 18.0 * std::sqrt(2.0) * double(c.smagorinsky_cs) * double(c.smagorinsky_cs)
+                                        : double(reference_les_k()))
+                                 : 0.0;
+    default_scales(h);
+    check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaEventCreateWithFlags(&h->event, cudaEventDisableTiming), "cudaEventCreate");
+    h->f_bytes = static_cast<std::size_t>(c.lattice) * h->N * static_cast<std::size_t>(storage_bytes(c.storage));
+    h->f = device_alloc(h->f_bytes, "population lattice");
+    InitSpec spec{};
+    spec.kind = 0;
+    spec.rho = 1.0F;
+    init_state(h, spec); // reference constructor calls initialize_uniform()
+    // A slab always carries flags: they keep its ghost planes out of every kernel.
+    if (slab.on) apply_flags(h, nullptr, CFDX_HOST);
+    h->sync();
+}
+
+} // namespace
+
 CFDX_API int cfdx_lbm_create(const cfdx_lbm_config* config, cfdx_lbm** out, char* error, std::size_t cap) {
     cfdx_lbm* h = nullptr;
     const int rc = guarded([&] {
         require(config != nullptr && out != nullptr, "null config or output handle");
         *out = nullptr;
-        const cfdx_lbm_config& c = *config;
-        // reference esoteric_pull.hpp:111-113,292-301
-        require(c.nx >= 2 && c.ny >= 2, "LBM grid requires nx, ny >= 2");
-        require(c.nz >= 2, "3-D LBM grid requires nz >= 2");
-        require(c.tau > 0.5F && std::isfinite(c.tau), "LBM tau must be > 0.5 for positive viscosity");
-        require(c.lattice == CFDX_D3Q19 || c.lattice == CFDX_D3Q27, "lattice must be CFDX_D3Q19 or CFDX_D3Q27");
-        require(c.collision == CFDX_BGK || c.collision == CFDX_TRT, "collision must be CFDX_BGK or CFDX_TRT");
-        require(c.storage == CFDX_STORE_F32 || c.storage == CFDX_STORE_F64 || c.storage == CFDX_STORE_F16S,
-                "unknown storage");
-        require(c.fp16_rounding == CFDX_ROUND_NEAREST || c.fp16_rounding == CFDX_ROUND_STOCHASTIC,
-                "fp16_rounding must be CFDX_ROUND_NEAREST or CFDX_ROUND_STOCHASTIC");
-        require(std::isfinite(c.acceleration_x) && std::isfinite(c.acceleration_y) && std::isfinite(c.acceleration_z),
-                "acceleration must be finite");
-        if (c.collision == CFDX_TRT)
-            require(c.trt_tau_minus > 0.5F || (c.trt_tau_minus <= 0.0F && c.trt_magic > 0.0F),
-                    "TRT needs trt_tau_minus > 0.5 or trt_magic > 0");
-        require(c.nx <= (1U << 30) && c.ny <= 65535U && c.nz <= 65535U, "grid extent exceeds launch limits");
-        int count = 0;
-        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
-            fail(CFDX_ERR_CUDA, "no CUDA device is available (the B200 engine has no CPU fallback)");
-        require(c.device >= 0 && c.device < count, "device ordinal out of range");
+        validate_config(*config);
         h = new cfdx_lbm();
-        h->cfg = c;
-        h->set_device();
-        h->N = c.nx * c.ny * c.nz;
-        require(h->N <= 0xffffffffULL, "lattice exceeds 2^32 - 1 cells");
-        h->key = KernelKey{c.storage, c.lattice, c.collision, c.smagorinsky_les != 0, false, false, 0, false, false};
-        h->choose_variant();
-        h->les_k = c.smagorinsky_les ? (c.smagorinsky_cs > 0.0F
-                                            ? 18.0 * std::sqrt(2.0) * double(c.smagorinsky_cs) * double(c.smagorinsky_cs)
-                                            : double(reference_les_k()))
-                                     : 0.0;
-        default_scales(h);
-        check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-        h->f_bytes = static_cast<std::size_t>(c.lattice) * h->N * static_cast<std::size_t>(storage_bytes(c.storage));
-        h->f = device_alloc(h->f_bytes, "population lattice");
-        InitSpec spec{};
-        spec.kind = 0;
-        spec.rho = 1.0F;
-        init_state(h, spec); // reference constructor calls initialize_uniform()
-        h->sync();
+        build_handle(h, *config, cfdx_lbm::Slab{});
+        *out = h;
+    });
+    if (rc != CFDX_OK) {
+        release(h);
+        copy_error(error, cap, g_error);
+    }
+    return rc;
+}
+
+CFDX_API int cfdx_lbm_create_slab(const cfdx_lbm_config* global, std::uint32_t z_begin, std::uint32_t z_extent,
+                                  cfdx_lbm** out, char* error, std::size_t cap) {
+    cfdx_lbm* h = nullptr;
+    const int rc = guarded([&] {
+        require(global != nullptr && out != nullptr, "null config or output handle");
+        *out = nullptr;
+        validate_config(*global);
+        require(z_extent >= 1U, "a slab needs at least one plane");
+        require(static_cast<std::uint64_t>(z_begin) + z_extent <= global->nz, "slab exceeds the lattice's z extent");
+        cfdx_lbm_config local = *global;
+        local.nz = static_cast<std::size_t>(z_extent) + 2U;
+        require(local.nz <= 65535U, "grid extent exceeds launch limits");
+        cfdx_lbm::Slab slab;
+        slab.on = true;
+        slab.z_begin = z_begin;
+        slab.z_extent = z_extent;
+        slab.nz_global = static_cast<std::uint32_t>(global->nz);
+        h = new cfdx_lbm();
+        build_handle(h, local, slab);
         *out = h;
     });
     if (rc != CFDX_OK) {
@@ -663,22 +736,25 @@ CFDX_API int cfdx_lbm_init_fields(cfdx_lbm* h, const float* fields, int where) {
     });
 }
 
-CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
-    return guarded([&] {
-        checked(h);
-        h->adj.ready = false;
-        if (!flags) {
-            h->key.flags = false;
-            h->moving_walls = false;
-            h->near_wall_fraction = 0.0;
-            h->choose_variant();
-            return;
-        }
-        if (!h->flags) h->flags = static_cast<std::uint8_t*>(device_alloc(h->N, "flag field"));
-        if (!h->wall_mask)
-            h->wall_mask = static_cast<std::uint32_t*>(device_alloc(h->N * sizeof(std::uint32_t), "wall-link masks"));
-        std::uint8_t* user = static_cast<std::uint8_t*>(device_alloc(h->N, "flag staging"));
-        try {
+namespace {
+
+// Internal flags and wall-link masks from the caller's flags (nullptr: none;
+// on a slab, all own cells fluid -- its ghost planes stay marked).
+void apply_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
+    h->adj.ready = false;
+    if (!flags && !h->slab.on) {
+        h->key.flags = false;
+        h->moving_walls = false;
+        h->near_wall_fraction = 0.0;
+        h->choose_variant();
+        return;
+    }
+    if (!h->flags) h->flags = static_cast<std::uint8_t*>(device_alloc(h->N, "flag field"));
+    if (!h->wall_mask)
+        h->wall_mask = static_cast<std::uint32_t*>(device_alloc(h->N * sizeof(std::uint32_t), "wall-link masks"));
+    std::uint8_t* user = static_cast<std::uint8_t*>(device_alloc(h->N, "flag staging"));
+    try {
+        if (flags) {
             upload(h, user, flags, h->N, where);
             // Record whether any cell is a moving wall (the adjoint does not cover them).
             std::string host_copy;
@@ -690,36 +766,49 @@ CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int wher
                 h->sync();
                 scan = reinterpret_cast<const std::uint8_t*>(host_copy.data());
             }
-            h->moving_walls = std::any_of(scan, scan + h->N, [](std::uint8_t v) { return v >= CFDX_MOVING_WALL_MIN; });
-            check_cuda(launch_prepare_flags(h->key.q, h->args(), user, h->flags, h->wall_mask, h->grid(), h->block(),
-                                            h->stream),
-                       "flag preparation kernel");
-            // count fluid cells and near-wall fluid cells (for the kernel choice)
-            unsigned long long* counts =
-                static_cast<unsigned long long*>(device_alloc(2 * sizeof(unsigned long long), "flag counters"));
-            unsigned long long host_counts[2] = {0, 0};
-            try {
-                check_cuda(cudaMemsetAsync(counts, 0, sizeof host_counts, h->stream), "cudaMemsetAsync");
-                check_cuda(launch_count_flags(h->flags, static_cast<std::uint32_t>(h->N), counts, h->stream),
-                           "flag count kernel");
-                check_cuda(cudaMemcpyAsync(host_counts, counts, sizeof host_counts, cudaMemcpyDeviceToHost, h->stream),
-                           "cudaMemcpyAsync (flag counts)");
-                h->sync();
-            } catch (...) {
-                device_free(counts);
-                throw;
-            }
-            device_free(counts);
-            h->near_wall_fraction =
-                host_counts[0] ? static_cast<double>(host_counts[1]) / static_cast<double>(host_counts[0]) : 0.0;
+            h->moving_walls =
+                std::any_of(scan, scan + h->N, [](std::uint8_t v) { return v >= CFDX_MOVING_WALL_MIN; });
+        } else {
+            check_cuda(cudaMemsetAsync(user, 0, h->N, h->stream), "cudaMemsetAsync");
+            h->moving_walls = false;
+        }
+        check_cuda(launch_prepare_flags(h->key.q, h->args(), user, h->flags, h->wall_mask, h->slab.on, h->grid(),
+                                        h->block(), h->stream),
+                   "flag preparation kernel");
+        // count fluid cells and near-wall fluid cells (for the kernel choice)
+        unsigned long long* counts =
+            static_cast<unsigned long long*>(device_alloc(2 * sizeof(unsigned long long), "flag counters"));
+        unsigned long long host_counts[2] = {0, 0};
+        try {
+            check_cuda(cudaMemsetAsync(counts, 0, sizeof host_counts, h->stream), "cudaMemsetAsync");
+            check_cuda(launch_count_flags(h->flags, static_cast<std::uint32_t>(h->N), counts, h->stream),
+                       "flag count kernel");
+            check_cuda(cudaMemcpyAsync(host_counts, counts, sizeof host_counts, cudaMemcpyDeviceToHost, h->stream),
+                       "cudaMemcpyAsync (flag counts)");
             h->sync();
         } catch (...) {
-            device_free(user);
+            device_free(counts);
             throw;
         }
+        device_free(counts);
+        h->near_wall_fraction =
+            host_counts[0] ? static_cast<double>(host_counts[1]) / static_cast<double>(host_counts[0]) : 0.0;
+        h->sync();
+    } catch (...) {
         device_free(user);
-        h->key.flags = true;
-        h->choose_variant();
+        throw;
+    }
+    device_free(user);
+    h->key.flags = true;
+    h->choose_variant();
+}
+
+} // namespace
+
+CFDX_API int cfdx_lbm_set_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
+    return guarded([&] {
+        checked(h);
+        apply_flags(h, flags, where);
     });
 }
 
@@ -804,9 +893,74 @@ CFDX_API int cfdx_lbm_set_storage_scale(cfdx_lbm* h, const float* scale) {
     });
 }
 
+// ------------------------------------------------------------ slab halos
+namespace {
+
+std::size_t plane_cells(const cfdx_lbm* h) { return h->cfg.nx * h->cfg.ny; }
+
+std::size_t halo_chunk_bytes(const cfdx_lbm* h) {
+    return plane_cells(h) * static_cast<std::size_t>(storage_bytes(h->key.storage));
+}
+
+// Start of the run of direction e.direction over local plane e.plane.
+char* plane_run(const cfdx_lbm* h, const HaloEntry& e) {
+    const std::size_t element = static_cast<std::size_t>(e.direction) * h->N + static_cast<std::size_t>(e.plane) * plane_cells(h);
+    return static_cast<char*>(h->f) + element * static_cast<std::size_t>(storage_bytes(h->key.storage));
+}
+
+// Message layout of `side` after the step the slab has just taken.
+int last_step_plan(const cfdx_lbm* h, int side, HaloEntry* send, HaloEntry* recv) {
+    return halo_plan(h->key.q, static_cast<int>((h->t - 1U) & 1U), side, h->slab.z_extent, send, recv);
+}
+
+cfdx_lbm* checked_slab(cfdx_lbm* h) {
+    checked(h);
+    require(h->slab.on, "not a slab handle (cfdx_lbm_create_slab)");
+    return h;
+}
+
+// Both messages of the cut between lo's upper side and up's lower side:
+// one copy launch on lo's stream, after both slabs' steps and before their
+// next ones (lo == up: the ring of one slab).
+void exchange_cut(cfdx_lbm* lo, cfdx_lbm* up) {
+    HaloEntry ls[kMaxHaloChunks], lr[kMaxHaloChunks], us[kMaxHaloChunks], ur[kMaxHaloChunks];
+    const int k = last_step_plan(lo, 1, ls, lr);
+    last_step_plan(up, 0, us, ur);
+    HaloCopy c{};
+    for (int i = 0; i < k; ++i) {
+        c.src[i] = plane_run(lo, ls[i]);
+        c.dst[i] = plane_run(up, ur[i]);
+        c.src[k + i] = plane_run(up, us[i]);
+        c.dst[k + i] = plane_run(lo, lr[i]);
+    }
+    c.chunks = 2 * k;
+    if (lo != up) {
+        check_cuda(cudaSetDevice(up->cfg.device), "cudaSetDevice");
+        check_cuda(cudaEventRecord(up->event, up->stream), "cudaEventRecord");
+        lo->set_device();
+        check_cuda(cudaStreamWaitEvent(lo->stream, up->event, 0), "cudaStreamWaitEvent");
+    }
+    check_cuda(launch_halo_copy(c, halo_chunk_bytes(lo), lo->stream), "halo copy kernel");
+    if (lo != up) {
+        check_cuda(cudaEventRecord(lo->event, lo->stream), "cudaEventRecord");
+        check_cuda(cudaSetDevice(up->cfg.device), "cudaSetDevice");
+        check_cuda(cudaStreamWaitEvent(up->stream, lo->event, 0), "cudaStreamWaitEvent");
+        lo->set_device();
+    }
+    lo->slab.due = static_cast<std::uint8_t>(lo->slab.due & ~2U);
+    up->slab.due = static_cast<std::uint8_t>(up->slab.due & ~1U);
+}
+
+} // namespace
+
 CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
     return guarded([&] {
         checked(h);
+        if (count == 0) return;
+        if (h->slab.on) {
+            require(h->slab.due == 0, "the halo messages of the slab's previous step have not all been received");
+            require(count == 1 || h->slab.whole_ring(), "a slab takes one step between halo exchanges");
+        }
         h->adj.ready = false;
         const dim3 g = h->grid(), b = h->step_block();
         LbmArgs a = h->args();
@@ -814,7 +968,116 @@ CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
             h->set_step(a, h->t);
             check_cuda(launch_step(h->key, a, g, b, h->stream), "step kernel");
             ++h->t;
+            if (h->slab.on) {
+                h->slab.due = 3;
+                h->slab.fresh = true;
+                if (h->slab.whole_ring()) exchange_cut(h, h);
+            }
         }
+    });
+}
+
+CFDX_API int cfdx_lbm_slab_info(cfdx_lbm* h, std::uint32_t* z_begin, std::uint32_t* z_extent, std::uint32_t* nz_global) {
+    return guarded([&] {
+        require(h != nullptr && z_begin != nullptr && z_extent != nullptr && nz_global != nullptr,
+                "null handle or output");
+        const auto nz = static_cast<std::uint32_t>(h->cfg.nz);
+        *z_begin = h->slab.on ? h->slab.z_begin : 0U;
+        *z_extent = h->slab.on ? h->slab.z_extent : nz;
+        *nz_global = h->slab.on ? h->slab.nz_global : nz;
+    });
+}
+
+CFDX_API int cfdx_halo_plan(int lattice, int odd, int side, std::uint32_t z_extent, cfdx_halo_entry* send,
+                            cfdx_halo_entry* recv, int capacity, int* count) {
+    return guarded([&] {
+        require(lattice == CFDX_D3Q19 || lattice == CFDX_D3Q27, "lattice must be CFDX_D3Q19 or CFDX_D3Q27");
+        require(odd == 0 || odd == 1, "odd must be 0 or 1");
+        require(side == CFDX_SIDE_LOWER || side == CFDX_SIDE_UPPER, "side must be CFDX_SIDE_LOWER or CFDX_SIDE_UPPER");
+        require(z_extent >= 1U, "a slab needs at least one plane");
+        require(send != nullptr && recv != nullptr && count != nullptr, "null output");
+        HaloEntry hs[kMaxHaloChunks], hr[kMaxHaloChunks];
+        const int k = halo_plan(lattice, odd, side, z_extent, hs, hr);
+        require(capacity >= k, "capacity below the chunk count");
+        for (int i = 0; i < k; ++i) {
+            send[i] = cfdx_halo_entry{hs[i].plane, hs[i].direction};
+            recv[i] = cfdx_halo_entry{hr[i].plane, hr[i].direction};
+        }
+        *count = k;
+    });
+}
+
+CFDX_API int cfdx_lbm_halo_bytes(cfdx_lbm* h, std::size_t* bytes) {
+    return guarded([&] {
+        require(h != nullptr && bytes != nullptr, "null handle or output");
+        require(h->slab.on, "not a slab handle (cfdx_lbm_create_slab)");
+        HaloEntry hs[kMaxHaloChunks], hr[kMaxHaloChunks];
+        *bytes = static_cast<std::size_t>(halo_plan(h->key.q, 0, 0, h->slab.z_extent, hs, hr)) * halo_chunk_bytes(h);
+    });
+}
+
+CFDX_API int cfdx_lbm_halo_pack(cfdx_lbm* h, int side, void* buffer) {
+    return guarded([&] {
+        checked_slab(h);
+        require(side == CFDX_SIDE_LOWER || side == CFDX_SIDE_UPPER, "side must be CFDX_SIDE_LOWER or CFDX_SIDE_UPPER");
+        require(buffer != nullptr, "null message buffer");
+        require(h->slab.fresh, "no step since the slab was initialised or loaded: there is no message to send");
+        HaloEntry hs[kMaxHaloChunks], hr[kMaxHaloChunks];
+        const int k = last_step_plan(h, side, hs, hr);
+        const std::size_t chunk = halo_chunk_bytes(h);
+        HaloCopy c{};
+        for (int i = 0; i < k; ++i) {
+            c.src[i] = plane_run(h, hs[i]);
+            c.dst[i] = static_cast<char*>(buffer) + static_cast<std::size_t>(i) * chunk;
+        }
+        c.chunks = k;
+        check_cuda(launch_halo_copy(c, chunk, h->stream), "halo pack kernel");
+    });
+}
+
+CFDX_API int cfdx_lbm_halo_unpack(cfdx_lbm* h, int side, const void* buffer) {
+    return guarded([&] {
+        checked_slab(h);
+        require(side == CFDX_SIDE_LOWER || side == CFDX_SIDE_UPPER, "side must be CFDX_SIDE_LOWER or CFDX_SIDE_UPPER");
+        require(buffer != nullptr, "null message buffer");
+        require((h->slab.due >> side) & 1U, "no message is due through this side (unpacked already, or no step yet)");
+        HaloEntry hs[kMaxHaloChunks], hr[kMaxHaloChunks];
+        const int k = last_step_plan(h, side, hs, hr);
+        const std::size_t chunk = halo_chunk_bytes(h);
+        HaloCopy c{};
+        for (int i = 0; i < k; ++i) {
+            c.src[i] = static_cast<const char*>(buffer) + static_cast<std::size_t>(i) * chunk;
+            c.dst[i] = plane_run(h, hr[i]);
+        }
+        c.chunks = k;
+        check_cuda(launch_halo_copy(c, chunk, h->stream), "halo unpack kernel");
+        h->slab.due = static_cast<std::uint8_t>(h->slab.due & ~(1U << side));
+    });
+}
+
+CFDX_API int cfdx_lbm_halo_exchange(cfdx_lbm* lower, cfdx_lbm* upper) {
+    return guarded([&] {
+        checked_slab(upper);
+        checked_slab(lower);
+        const auto& a = lower->slab;
+        const auto& b = upper->slab;
+        require(lower->key.q == upper->key.q && lower->key.storage == upper->key.storage &&
+                    lower->cfg.nx == upper->cfg.nx && lower->cfg.ny == upper->cfg.ny && a.nz_global == b.nz_global,
+                "slabs of different lattices");
+        require((a.z_begin + a.z_extent) % a.nz_global == b.z_begin, "upper is not the slab above lower");
+        require(lower->t == upper->t, "slabs at different time steps");
+        require(a.fresh && b.fresh && (a.due & 2U) && (b.due & 1U), "no message of this cut is due");
+        if (lower->cfg.device != upper->cfg.device) {
+            int ok = 0;
+            check_cuda(cudaDeviceCanAccessPeer(&ok, lower->cfg.device, upper->cfg.device), "cudaDeviceCanAccessPeer");
+            require(ok != 0, "the slabs' devices have no peer access");
+            const cudaError_t e = cudaDeviceEnablePeerAccess(upper->cfg.device, 0);
+            if (e == cudaErrorPeerAccessAlreadyEnabled)
+                (void)cudaGetLastError();
+            else
+                check_cuda(e, "cudaDeviceEnablePeerAccess");
+        }
+        exchange_cut(lower, upper);
     });
 }
 
@@ -1052,6 +1315,26 @@ template <class T> T get(std::FILE* f, const char* path) {
     return v;
 }
 
+// The CFDCHK3 brick of a handle: global extent, begin and extent (rows of
+// v), and the local cells it covers (a slab's own planes).
+struct Brick {
+    std::uint64_t v[3][3];
+    std::size_t first_cell, cells;
+};
+
+Brick brick_of(const cfdx_lbm* h) {
+    Brick b{};
+    const std::uint64_t nz = h->slab.on ? h->slab.nz_global : h->cfg.nz;
+    const std::uint64_t z0 = h->slab.on ? h->slab.z_begin : 0U;
+    const std::uint64_t ze = h->slab.on ? h->slab.z_extent : h->cfg.nz;
+    const std::uint64_t rows[3][3] = {{h->cfg.nx, h->cfg.ny, nz}, {0U, 0U, z0}, {h->cfg.nx, h->cfg.ny, ze}};
+    std::memcpy(b.v, rows, sizeof rows);
+    const std::size_t plane = h->cfg.nx * h->cfg.ny;
+    b.first_cell = h->slab.on ? plane : 0U;
+    b.cells = plane * static_cast<std::size_t>(ze);
+    return b;
+}
+
 float* checkpoint_scratch(cfdx_lbm* h) {
     if (!h->macro_scratch)
         h->macro_scratch = static_cast<float*>(device_alloc(4U * h->N * sizeof(float), "macroscopic scratch"));
@@ -1073,27 +1356,26 @@ CFDX_API int cfdx_lbm_checkpoint_save(cfdx_lbm* h, const char* path) {
         put<std::uint32_t>(f, 1U, path);
         put<std::uint32_t>(f, 0x01020304U, path);
         put<std::uint32_t>(f, static_cast<std::uint32_t>(h->key.q), path);
-        const std::uint64_t ext[3] = {h->cfg.nx, h->cfg.ny, h->cfg.nz};
-        for (int r = 0; r < 3; ++r) {
-            const std::uint64_t begin[3] = {0, 0, 0};
-            const std::uint64_t* v = r == 1 ? begin : ext;
-            for (int k = 0; k < 3; ++k) put<std::uint64_t>(f, v[k], path);
-        }
+        const Brick brick = brick_of(h);
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 3; ++k) put<std::uint64_t>(f, brick.v[r][k], path);
         put<std::uint64_t>(f, h->t, path);
         put<float>(f, h->cfg.tau, path);
         put<float>(f, h->cfg.acceleration_x, path);
         put<float>(f, h->cfg.acceleration_y, path);
         put<float>(f, h->cfg.acceleration_z, path);
         float* dev = checkpoint_scratch(h);
-        std::vector<float> host(h->N);
+        const std::size_t first = brick.first_cell, cells = brick.cells;
+        std::vector<float> host(cells);
         for (int d = 0; d < h->key.q; ++d) {
             check_cuda(launch_slot_io(h->key, h->args(), d, dev, false, h->grid(), h->block(), h->stream),
                        "checkpoint read kernel");
-            check_cuda(cudaMemcpyAsync(host.data(), dev, h->N * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+            check_cuda(cudaMemcpyAsync(host.data(), dev + first, cells * sizeof(float), cudaMemcpyDeviceToHost,
+                                       h->stream),
                        "cudaMemcpyAsync (checkpoint)");
             h->sync();
-            h->d2h += h->N * sizeof(float);
-            if (std::fwrite(host.data(), sizeof(float), h->N, f) != h->N)
+            h->d2h += cells * sizeof(float);
+            if (std::fwrite(host.data(), sizeof(float), cells, f) != cells)
                 fail(CFDX_ERR_IO, std::string("checkpoint write failed: ") + path);
         }
         if (std::fflush(f) != 0) fail(CFDX_ERR_IO, std::string("checkpoint write failed: ") + path);
@@ -1116,11 +1398,11 @@ CFDX_API int cfdx_lbm_checkpoint_load(cfdx_lbm* h, const char* path) {
         const auto q = get<std::uint32_t>(f, path);
         if (version != 1U || endian != 0x01020304U || q != static_cast<std::uint32_t>(h->key.q))
             fail(CFDX_ERR_IO, "unsupported checkpoint format/descriptor");
-        const std::uint64_t ext[3] = {h->cfg.nx, h->cfg.ny, h->cfg.nz};
+        const Brick brick = brick_of(h);
         for (int r = 0; r < 3; ++r)
             for (int k = 0; k < 3; ++k) {
                 const auto v = get<std::uint64_t>(f, path);
-                if (v != (r == 1 ? 0U : ext[k])) fail(CFDX_ERR_IO, "checkpoint decomposition does not match the lattice");
+                if (v != brick.v[r][k]) fail(CFDX_ERR_IO, "checkpoint decomposition does not match the lattice");
             }
         const auto t = get<std::uint64_t>(f, path);
         const float tau = get<float>(f, path), ax = get<float>(f, path), ay = get<float>(f, path),
@@ -1132,23 +1414,29 @@ CFDX_API int cfdx_lbm_checkpoint_load(cfdx_lbm* h, const char* path) {
         const long header = std::ftell(f);
         if (header < 0 || std::fseek(f, 0, SEEK_END) != 0) fail(CFDX_ERR_IO, std::string("cannot size checkpoint: ") + path);
         const long total = std::ftell(f);
-        const unsigned long long payload = static_cast<unsigned long long>(h->key.q) * h->N * sizeof(float);
+        const unsigned long long payload = static_cast<unsigned long long>(h->key.q) * brick.cells * sizeof(float);
         if (total < 0 || static_cast<unsigned long long>(total - header) != payload)
             fail(CFDX_ERR_IO, std::string("checkpoint payload size mismatch (truncated or trailing data): ") + path);
         if (std::fseek(f, header, SEEK_SET) != 0) fail(CFDX_ERR_IO, std::string("cannot read checkpoint: ") + path);
         float* dev = checkpoint_scratch(h);
-        std::vector<float> host(h->N);
+        // ghost planes of a slab stay 0: their cells are walls, which the write kernel skips
+        std::vector<float> host(h->N, 0.0F);
+        float* own = host.data() + brick.first_cell;
         h->adj.ready = false;
         h->t = t;
         const LbmArgs a = h->args(); // slot tables of the stored time step's parity
         for (int d = 0; d < h->key.q; ++d) {
-            if (std::fread(host.data(), sizeof(float), h->N, f) != h->N)
+            if (std::fread(own, sizeof(float), brick.cells, f) != brick.cells)
                 fail(CFDX_ERR_IO, std::string("truncated checkpoint: ") + path);
             upload(h, dev, host.data(), h->N * sizeof(float), CFDX_HOST);
             check_cuda(launch_slot_io(h->key, a, d, dev, true, h->grid(), h->block(), h->stream),
                        "checkpoint write kernel");
         }
         h->sync();
+        // Each own cell's populations now sit where its next step reads them,
+        // ghost-plane slots included: no message is due.
+        h->slab.due = 0;
+        h->slab.fresh = false;
     });
 }
 
@@ -1215,6 +1503,7 @@ CFDX_API int cfdx_lbm_adjoint_forward(cfdx_lbm* h, std::uint64_t steps, std::uin
     return guarded([&] {
         checked(h);
         require(steps >= 1U && interval >= 1U, "adjoint forward needs steps >= 1 and a checkpoint interval >= 1");
+        require(!h->slab.on, "the adjoint covers whole lattices, not slabs");
         require(!h->key.les, "the adjoint does not cover Smagorinsky LES (its tau depends on the populations)");
         require(!h->moving_walls, "the adjoint does not cover moving walls");
         require(h->key.narrow, "the adjoint needs q * cells < 2^32");

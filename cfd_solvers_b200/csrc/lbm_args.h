@@ -76,6 +76,9 @@ struct LbmArgs {
     std::uint32_t round_seed;
     std::uint32_t round_mask;
     std::uint32_t round_add;
+    // Added to the local cell index before hashing: a z-slab hashes the
+    // global index, so a decomposed lattice rounds like the whole one.
+    std::uint32_t hash_base;
 };
 
 // Parameters of the adjoint kernels (lbm_adjoint.cuh).
@@ -96,6 +99,9 @@ struct InitSpec {
     int kind; // 0 uniform, 1 Taylor-Green, 2 per-cell fields
     float rho, ux, uy, uz, amplitude;
     const float* fields; // 4*N (rho|ux|uy|uz), device
+    // Global z of local plane z: (z + z_origin) mod nz_total (a z-slab's
+    // Taylor-Green field is the whole lattice's); 0 and nz for a whole lattice.
+    std::uint32_t z_origin, nz_total;
 };
 
 // Output of the fluid-cell reduction, accumulated in FP64.

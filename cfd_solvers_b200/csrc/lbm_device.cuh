@@ -99,7 +99,7 @@ __device__ __forceinline__ void st(typename S::T* p, typename S::R v, const LbmA
 
 // lowbias32 integer hash (C. Wellons, "hash-prospector", public domain).
 __device__ __forceinline__ u32 round_hash(const LbmArgs& a, u32 n) {
-    u32 x = n ^ a.round_seed;
+    u32 x = (n + a.hash_base) ^ a.round_seed;
     x ^= x >> 16;
     x *= 0x7feb352dU;
     x ^= x >> 15;
@@ -1093,7 +1093,7 @@ __global__ void __launch_bounds__(128) k_init(const __grid_constant__ LbmArgs a,
         const R two_pi = R(2) * R(3.14159265358979323846);
         const R xf = (R(x) + R(0.5)) / R(a.nx);
         const R yf = (R(y) + R(0.5)) / R(a.ny);
-        const R zf = (R(z) + R(0.5)) / R(a.nz);
+        const R zf = (R((z + s.z_origin) % s.nz_total) + R(0.5)) / R(s.nz_total);
         const R sx = sin(two_pi * xf), cx = cos(two_pi * xf);
         const R sy = sin(two_pi * yf), cy = cos(two_pi * yf);
         const R cz = cos(two_pi * zf);
@@ -1360,17 +1360,21 @@ static __global__ void __launch_bounds__(kReduceThreads) k_reduce_final(const do
 
 // Derives the internal flag byte (wall id, near-wall bits) from the caller's
 // flags.  Near-wall bits let interior cells skip all neighbour-flag loads.
+// With `ghost`, planes 0 and nz-1 are a z-slab's copies of its neighbours'
+// edge planes: their flags still set the links of the cells next to them,
+// but the cells themselves are marked as walls (id 1 unless a moving wall),
+// so that no kernel steps, initialises, reduces or reports them.
 template <class L>
 __global__ void __launch_bounds__(128) k_prepare_flags(const __grid_constant__ LbmArgs a, const std::uint8_t* user,
-                                                       std::uint8_t* out, std::uint32_t* mask) {
+                                                       std::uint8_t* out, std::uint32_t* mask, int ghost) {
     const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
     const u32 z = blockIdx.z;
     if (x >= a.nx || y >= a.ny) return;
     const u32 n = (z * a.ny + y) * a.nx + x;
     const std::uint8_t t = user[n] & kFlagTypeMask;
-    if (t != 0) {
-        out[n] = t;
+    if (t != 0 || (ghost && (z == 0 || z == a.nz - 1U))) {
+        out[n] = t != 0 ? t : std::uint8_t(1);
         mask[n] = 0U;
         return;
     }

@@ -21,11 +21,11 @@ cudaError_t launch_count_flags(const std::uint8_t* flags, std::uint32_t n, unsig
 
 // Flag preparation does not depend on the storage type; it lives here once.
 cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out,
-                                 std::uint32_t* mask, dim3 g, dim3 b, cudaStream_t s) {
+                                 std::uint32_t* mask, bool ghost, dim3 g, dim3 b, cudaStream_t s) {
     if (q == 19)
-        k_prepare_flags<D3Q19><<<g, b, 0, s>>>(a, user, out, mask);
+        k_prepare_flags<D3Q19><<<g, b, 0, s>>>(a, user, out, mask, ghost ? 1 : 0);
     else if (q == 27)
-        k_prepare_flags<D3Q27><<<g, b, 0, s>>>(a, user, out, mask);
+        k_prepare_flags<D3Q27><<<g, b, 0, s>>>(a, user, out, mask, ghost ? 1 : 0);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();

@@ -67,7 +67,8 @@ cudaError_t launch_slot_io(const KernelKey& k, const LbmArgs& a, int d, float* b
                            dim3 block, cudaStream_t s);
 cudaError_t launch_count_flags(const std::uint8_t* flags, std::uint32_t n, unsigned long long* out, cudaStream_t s);
 cudaError_t launch_sum_partials(const double* partials, std::size_t count, double* out, cudaStream_t s);
+// ghost: planes 0 and nz-1 are a z-slab's ghost planes (k_prepare_flags).
 cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out,
-                                 std::uint32_t* mask, dim3 grid, dim3 block, cudaStream_t s);
+                                 std::uint32_t* mask, bool ghost, dim3 grid, dim3 block, cudaStream_t s);
 
 } // namespace cfdx

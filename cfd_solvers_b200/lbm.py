@@ -143,17 +143,23 @@ class EsotericPullCudaSolver:
             raise ValueError("fp16_rounding must be stochastic or nearest")
         c.fp16_rounding = B.ROUND_STOCHASTIC if config.fp16_rounding == "stochastic" else B.ROUND_NEAREST
         c.rounding_seed = int(config.rounding_seed) & 0xFFFFFFFF
-        handle = ctypes.c_void_p()
-        err = ctypes.create_string_buffer(1024)
-        status = self._lib.raw.cfdx_lbm_create(ctypes.byref(c), ctypes.byref(handle), err, len(err))
         self._h = None
-        self._lib.check(status, "cfdx_lbm_create")
-        self._h = handle
+        self._h = self._create(c)
         self._q = c.lattice
-        self._cells = c.nx * c.ny * c.nz
+        self._cells = self._local_cells(c)
         self._has_mask = False
         self._has_local = False
         self._mask = None
+
+    def _create(self, c: B.cfdx_lbm_config):
+        handle = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(1024)
+        self._lib.check(self._lib.raw.cfdx_lbm_create(ctypes.byref(c), ctypes.byref(handle), err, len(err)),
+                        "cfdx_lbm_create")
+        return handle
+
+    def _local_cells(self, c: B.cfdx_lbm_config) -> int:
+        return c.nx * c.ny * c.nz
 
     # ------------------------------------------------------------ lifecycle
     def close(self):

@@ -303,6 +303,77 @@ CFDX_API int cfdx_lbm_adjoint_memory(cfdx_lbm* lbm, size_t* bytes);
 /* Frees the adjoint's buffers (checkpoints, frames, adjoint lattice). */
 CFDX_API int cfdx_lbm_adjoint_release(cfdx_lbm* lbm);
 
+/* ---- z-slab decomposition (multi-GPU).  The reference cuts its distributed
+ * two-grid solver into bricks (DistributedPullBlock, distributed_pull.hpp:35-60;
+ * make_brick / partition_axis, distributed/cartesian.hpp:132-159) and sends
+ * only the populations that cross a face (selective_halo.hpp:24-62).  Here the
+ * in-place lattice is cut along z only, one slab per rank, by the same
+ * partition rule (the first nz % parts slabs get one extra plane); the slabs
+ * form a periodic ring, as the lattice is periodic in z.
+ *
+ * A slab handle holds nx*ny*(z_extent + 2) cells: local plane k is global
+ * plane (z_begin - 1 + k) mod nz, so planes 0 and z_extent + 1 ("ghost
+ * planes") hold copies of the neighbours' edge planes.  Every per-cell array
+ * the other entry points take or return (flags, fields, accelerations, n_s,
+ * macroscopic fields, logical populations) covers the local planes.  Ghost
+ * plane flags must be the neighbours' flags (they set the bounce-back links of
+ * the edge planes); the other ghost-plane inputs are ignored and ghost-plane
+ * outputs are 0.  Reductions, checksums and checkpoints cover the slab's own
+ * planes; checkpoints record the slab as a CFDCHK3 brick
+ * (begin = (0, 0, z_begin), extent = (nx, ny, z_extent)).
+ *
+ * After each step every cut carries one message each way (5 chunks for D3Q19,
+ * 9 for D3Q27, of nx*ny populations in the storage type): the ghost slots this
+ * slab's edge cells wrote, and the edge slots the neighbour's edge cells read
+ * next.  A slab steps once, exchanges through both sides (pack -> transport ->
+ * unpack, or cfdx_lbm_halo_exchange between two handles of one process), then
+ * steps again; cfdx_lbm_step refuses to start a step while a side of the
+ * previous one has not been received.  A slab that is the whole ring
+ * (z_extent == nz) exchanges with itself inside cfdx_lbm_step.  The discrete
+ * adjoint is not available on slab handles. */
+typedef struct cfdx_halo_entry {
+    uint32_t plane;     /* local plane, 0 .. z_extent + 1 */
+    uint32_t direction; /* lattice direction (storage slot) */
+} cfdx_halo_entry;
+
+#define CFDX_SIDE_LOWER 0 /* towards global plane z_begin - 1 */
+#define CFDX_SIDE_UPPER 1 /* towards global plane z_begin + z_extent */
+
+/* Creates the slab [z_begin, z_begin + z_extent) of the lattice `global`
+ * describes (global->nz is the whole lattice's extent); z_extent >= 1. */
+CFDX_API int cfdx_lbm_create_slab(const cfdx_lbm_config* global, uint32_t z_begin, uint32_t z_extent,
+                                  cfdx_lbm** out, char* error, size_t error_capacity);
+
+/* Slab geometry of a handle (a plain handle reports 0, nz, nz). */
+CFDX_API int cfdx_lbm_slab_info(cfdx_lbm* lbm, uint32_t* z_begin, uint32_t* z_extent, uint32_t* nz_global);
+
+/* Message layout of one side, host-only (no device needed): after a step of
+ * parity `odd` on a slab of z_extent planes, chunk k of the message sent
+ * through `side` is local (send[k].plane, send[k].direction), and chunk k of
+ * the message arriving through `side` is written to (recv[k].plane,
+ * recv[k].direction).  *count = 5 (D3Q19) or 9 (D3Q27); capacity >= *count. */
+CFDX_API int cfdx_halo_plan(int lattice, int odd, int side, uint32_t z_extent, cfdx_halo_entry* send,
+                            cfdx_halo_entry* recv, int capacity, int* count);
+
+/* Bytes of one message (chunks * nx * ny * storage bytes). */
+CFDX_API int cfdx_lbm_halo_bytes(cfdx_lbm* lbm, size_t* bytes);
+
+/* Copies the message for `side` of the step just taken into device memory
+ * `buffer` (this device's or a peer's), stream-ordered after the step. */
+CFDX_API int cfdx_lbm_halo_pack(cfdx_lbm* lbm, int side, void* device_buffer);
+
+/* Writes the message that arrived through `side` (device memory) into the
+ * slab, stream-ordered; the buffer must stay valid until the slab's stream
+ * has passed this point. */
+CFDX_API int cfdx_lbm_halo_unpack(cfdx_lbm* lbm, int side, const void* device_buffer);
+
+/* Both messages of the cut between `lower` (its upper side) and `upper` (its
+ * lower side), two slab handles of this process on one device or on devices
+ * with peer access: one copy kernel, slot to slot, ordered after both
+ * handles' steps and before their next ones.  lower == upper is the ring of
+ * one slab. */
+CFDX_API int cfdx_lbm_halo_exchange(cfdx_lbm* lower, cfdx_lbm* upper);
+
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */

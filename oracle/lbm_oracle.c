@@ -226,15 +226,18 @@ int ora_init(const ora_cfg* c, void* f, int kind, const float* p, const float* f
     return 0;
 }
 
-int ora_step(const ora_cfg* c, void* f, uint64_t t) {
+int ora_step(const ora_cfg* c, void* f, uint64_t t) { return ora_step_planes(c, f, t, 0, c ? c->nz : 0); }
+
+int ora_step_planes(const ora_cfg* c, void* f, uint64_t t, size_t z_begin, size_t z_end) {
     ora_lattice L;
     if (ora_setup(c, &L)) return 1;
+    if (z_begin > z_end || z_end > c->nz) return 1;
     if (c->storage == ORA_STORE_F32)
-        step_f32(&L, c, (float*)f, t);
+        step_f32(&L, c, (float*)f, t, z_begin, z_end);
     else if (c->storage == ORA_STORE_F64)
-        step_f64(&L, c, (double*)f, t);
+        step_f64(&L, c, (double*)f, t, z_begin, z_end);
     else
-        step_h16(&L, c, (uint16_t*)f, t);
+        step_h16(&L, c, (uint16_t*)f, t, z_begin, z_end);
     return 0;
 }
 

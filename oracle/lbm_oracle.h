@@ -74,6 +74,11 @@ int ora_init(const ora_cfg* c, void* f, int kind, const float* p, const float* f
 /* One fused stream+collide step at parity (t & 1).  Reference: esoteric_pull.hpp:494-515. */
 int ora_step(const ora_cfg* c, void* f, uint64_t t);
 
+/* The same step for the cells of planes [z_begin, z_end) only: the other
+ * planes are read and written by those cells' streaming but not updated
+ * themselves (a z-slab with ghost planes in the decomposition tests). */
+int ora_step_planes(const ora_cfg* c, void* f, uint64_t t, size_t z_begin, size_t z_end);
+
 /* Macroscopic fields of the state at time t (rho, u + a/2); non-fluid cells
  * report rho = 0, u = 0.  Outputs are float for F32/F16S and double for F64.
  * Reference: esoteric_pull.hpp:180-209. */

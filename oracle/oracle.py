@@ -71,6 +71,7 @@ def oracle_lib():
         P = ctypes.POINTER(_OraCfg)
         lib.ora_init.argtypes = [P, ctypes.c_void_p, ctypes.c_int, _f, _f]
         lib.ora_step.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64]
+        lib.ora_step_planes.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_size_t]
         lib.ora_macroscopic.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64] + [ctypes.c_void_p] * 4
         lib.ora_reduce.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64, _d]
         lib.ora_logical.argtypes = [P, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
@@ -81,7 +82,7 @@ def oracle_lib():
         lib.ora_reference_les_k.restype = ctypes.c_float
         lib.ora_adjoint_forward.argtypes = [P, _d, ctypes.c_uint64, _d]
         lib.ora_adjoint.argtypes = [P, _d, ctypes.c_uint64, _d, _d, _d, _d]
-        for name in ("ora_init", "ora_step", "ora_macroscopic", "ora_reduce", "ora_logical", "ora_adjoint_forward",
+        for name in ("ora_init", "ora_step", "ora_step_planes", "ora_macroscopic", "ora_reduce", "ora_logical", "ora_adjoint_forward",
                      "ora_adjoint"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
@@ -184,6 +185,12 @@ class OracleLattice:
         for _ in range(count):
             self._call(lib.ora_step(ctypes.byref(self._cfg), self.f.ctypes.data, self.t))
             self.t += 1
+
+    def step_planes(self, z_begin: int, z_end: int):
+        """One step of the cells of planes [z_begin, z_end) only (ora_step_planes)."""
+        self._refresh()
+        self._call(oracle_lib().ora_step_planes(ctypes.byref(self._cfg), self.f.ctypes.data, self.t, z_begin, z_end))
+        self.t += 1
 
     def macroscopic(self):
         self._refresh()
