@@ -50,6 +50,8 @@ def parse_args(argv=None):
     p.add_argument("--lattice", choices=["d3q19", "d3q27"], default="d3q19")
     p.add_argument("--storage", choices=["fp32", "fp16s"], default="fp32")
     p.add_argument("--no-variants", action="store_true", help="skip the FP16S / D3Q27 side measurements")
+    p.add_argument("--slabs", action="store_true",
+                   help="run the z-slab path (used for N > 1) also on one GPU: one slab that is the whole ring")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-differentiation", action="store_true",
@@ -568,6 +570,11 @@ def slab_main(args, torch, cs, rank, world, local_rank):
 
     from cfd_solvers_b200.slabs import DistributedEsotericPullSolver
 
+    if world == 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29531")
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
     dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                             device_id=torch.device(f"cuda:{local_rank}"))
     n = args.n
@@ -641,7 +648,7 @@ def slab_main(args, torch, cs, rank, world, local_rank):
 
     if rank == 0:
         peak, peak_kind = hbm_peak()
-        fluid = (n - 2) * (n - 2) * (n - 1)  # rank 0: its z = 0 plane is a wall
+        fluid = int(np.count_nonzero(g.own(local_flags) == 0))  # rank 0's own fluid cells
         alg = fluid * bytes_per_update(q, args.storage) + n * n * (n + 2)
         achieved = alg / (ms / args.steps / 1e3) / 1e9
         line = {
@@ -663,7 +670,7 @@ def slab_main(args, torch, cs, rank, world, local_rank):
                          "traffic": None, "algorithmic_bytes_per_launch": alg,
                          "kernel": "cfdx::k_step per slab; achieved over the whole step incl. the exchange"},
             "clocks": clocks,
-            "gpu_launches": 5 * args.steps,
+            "gpu_launches": (5 if world > 1 else 2) * args.steps,
             "checks": {"nonfinite_cells": red["nonfinite"], "mass": red["mass"]},
             "e2e": e2e,
         }
@@ -701,7 +708,7 @@ def main(argv=None):
             out = precision_study(torch, cs, local_rank, shape=(args.n, args.n // 2, args.n // 2), steps=args.steps)
         print(json.dumps(out), flush=True)
         return 0
-    if world > 1:
+    if world > 1 or args.slabs:
         return slab_main(args, torch, cs, rank, world, local_rank)
     dist = None
 

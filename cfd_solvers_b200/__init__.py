@@ -18,6 +18,7 @@ from .lbm import (
     smagorinsky_k,
     trt_tau_minus,
 )
+from .slabs import DistributedEsotericPullSolver, SlabSolver
 
 __all__ = [
     "CfdxError",
@@ -35,4 +36,6 @@ __all__ = [
     "cavity_flags",
     "smagorinsky_k",
     "trt_tau_minus",
+    "DistributedEsotericPullSolver",
+    "SlabSolver",
 ]
