@@ -530,6 +530,49 @@ def cpu_reference_sample(n, warmup, steps, threads=0):
     return mlups, seconds, O.ref_threads()
 
 
+def voxelizer_measure(torch, device, n=512, subdivisions=7, cpu_sample=True):
+    """The device voxelizer on a closed sphere of 20*4^s triangles over an n^3 grid.
+
+    Device time of one whole cfdx_voxelize call (triangle upload, row lists,
+    cells; output in device memory), host wall clock around it after a warm-up
+    call.  The reference's voxelize_surface (single-threaded, every cell against
+    every triangle) is timed on a bounded sample (48^3 cells x 1280 triangles) and
+    reported as ray-triangle tests per second.
+    """
+    from cfd_solvers_b200 import geometry as G
+
+    tris = G.transform_surface(G.icosphere((0.0, 0.0, 0.0), 0.35, subdivisions), (0.5, 0.5, 0.5), (0.3, 1.0, 0.2),
+                               0.7)
+    grid = G.VoxelGrid3D(n, n, n)
+    out = torch.empty(n ** 3, dtype=torch.uint8, device=f"cuda:{device}")
+    G.voxelize_surface(tris, grid, out=out)
+    times = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        G.voxelize_surface(tris, grid, out=out)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    sec = min(times)
+    res = {"triangles": len(tris), "grid": f"{n}^3", "ms": sec * 1e3, "gcells_per_s": n ** 3 / sec / 1e9,
+           "solid_fraction": float(out.float().mean().item()),
+           "note": "one cfdx_voxelize call incl. triangle upload and scratch; best of 3 after a warm-up"}
+    if cpu_sample:
+        from oracle import oracle as O
+
+        if O.reference_available():
+            small = G.transform_surface(G.icosphere((0.0, 0.0, 0.0), 0.35, 3), (0.5, 0.5, 0.5), (0.3, 1.0, 0.2), 0.7)
+            m = 48
+            t0 = time.perf_counter()
+            O.ref_voxelize(small, m, m, m, (0, 0, 0), (1, 1, 1))
+            cpu = time.perf_counter() - t0
+            rate = m ** 3 * len(small) / cpu
+            res["cpu_reference"] = {"sample": f"{m}^3 cells x {len(small)} triangles", "seconds": cpu, "cores": 1,
+                                    "ray_triangle_tests_per_s": rate,
+                                    "projected_seconds_for_this_case": n ** 3 * len(tris) / rate}
+    return res
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -795,6 +838,7 @@ def main(argv=None):
             d27["roofline_frac"] = d27["achieved_gbs"] / hbm_peak()[0]
             variants["d3q27_fp32"] = d27
             variants["z_slabs_one_gpu"] = slab_exchange_overhead(torch, cs, n, vs, local_rank, ms / args.steps)
+            variants["voxelizer"] = voxelizer_measure(torch, local_rank, n, cpu_sample=not args.no_cpu_baseline)
         if not args.no_differentiation:
             variants["differentiation"] = differentiation_variants(torch, cs, local_rank)
         if not args.no_precision:

@@ -106,6 +106,11 @@ class cfdx_halo_entry(ctypes.Structure):
     _fields_ = [("plane", ctypes.c_uint32), ("direction", ctypes.c_uint32)]
 
 
+class cfdx_voxel_grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_size_t), ("ny", ctypes.c_size_t), ("nz", ctypes.c_size_t),
+                ("minimum", ctypes.c_double * 3), ("maximum", ctypes.c_double * 3)]
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _f = ctypes.c_float
@@ -157,6 +162,9 @@ SIGNATURES = {
     "cfdx_lbm_halo_pack": (_i, [_H, _i, _vp]),
     "cfdx_lbm_halo_unpack": (_i, [_H, _i, _vp]),
     "cfdx_lbm_halo_exchange": (_i, [_H, _H]),
+    "cfdx_voxelize": (_i, [_vp, _sz, ctypes.POINTER(cfdx_voxel_grid), ctypes.c_uint32, ctypes.c_uint32,
+                           ctypes.c_uint8, _vp, _i, _i]),
+    "cfdx_lbm_set_flags_surface": (_i, [_H, _vp, _sz, _vp, _vp, ctypes.c_uint8, _vp, _i]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

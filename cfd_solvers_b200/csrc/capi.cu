@@ -23,6 +23,7 @@
 #include "halo.h"
 #include "handle_access.h"
 #include "lbm_launch.h"
+#include "voxelize.h"
 
 namespace {
 
@@ -1659,6 +1660,97 @@ CFDX_API int cfdx_lbm_adjoint_release(cfdx_lbm* h) {
         checked(h);
         if (h->stream) h->sync();
         release_adjoint(h);
+    });
+}
+
+// ---------------------------------------------------------------- voxelizer
+namespace {
+
+void check_voxel_inputs(const double* tris, std::size_t count, std::size_t nx, std::size_t ny, std::size_t nz,
+                        const double* lo, const double* hi, std::uint32_t z_count) {
+    require(tris != nullptr && lo != nullptr && hi != nullptr, "null voxelization argument");
+    // reference voxelize.cpp:5 ("invalid voxelization inputs")
+    require(count > 0 && nx > 0 && ny > 0 && nz > 0 && hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2],
+            "invalid voxelization inputs");
+    for (int k = 0; k < 3; ++k) require(std::isfinite(lo[k]) && std::isfinite(hi[k]), "voxel grid bounds must be finite");
+    for (std::size_t i = 0; i < 9 * count; ++i) require(std::isfinite(tris[i]), "triangle coordinates must be finite");
+    require(nx <= (1ULL << 30) && ny <= 65535U && nz <= 0xffffffffULL && z_count >= 1U && z_count <= 65535U,
+            "voxel grid exceeds launch limits");
+    require(static_cast<unsigned long long>(ny) * z_count < (1ULL << 31), "voxel grid has too many rows");
+    require(count <= (1ULL << 26), "too many triangles (at most 2^26 per call)");
+}
+
+void run_voxelizer(const double* tris, std::size_t count, const VoxelRequest& q, std::uint8_t* out, cudaStream_t s) {
+    const char* what = "voxelizer";
+    const cudaError_t e = voxelize_device(tris, count, q, out, s, &what);
+    check_cuda(e, what);
+}
+
+} // namespace
+
+CFDX_API int cfdx_voxelize(const double* triangles, std::size_t count, const cfdx_voxel_grid* grid,
+                           std::uint32_t z_first, std::uint32_t z_count, std::uint8_t solid_value, std::uint8_t* out,
+                           int where, int device) {
+    return guarded([&] {
+        require(grid != nullptr && out != nullptr, "null grid or output");
+        const cfdx_voxel_grid& g = *grid;
+        check_voxel_inputs(triangles, count, g.nx, g.ny, g.nz, g.minimum, g.maximum, z_count);
+        require(z_first < g.nz, "z_first outside the grid");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        int devices = 0;
+        if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+            fail(CFDX_ERR_CUDA, "no CUDA device is available (the B200 engine has no CPU fallback)");
+        require(device >= 0 && device < devices, "device ordinal out of range");
+        check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        VoxelRequest q{g.nx, g.ny, g.nz, {g.minimum[0], g.minimum[1], g.minimum[2]},
+                       {g.maximum[0], g.maximum[1], g.maximum[2]}, z_first, z_count, solid_value, nullptr};
+        const std::size_t bytes = g.nx * g.ny * static_cast<std::size_t>(z_count);
+        cudaStream_t s = nullptr;
+        check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+        std::uint8_t* dev = where == CFDX_DEVICE ? out : nullptr;
+        try {
+            if (!dev) dev = static_cast<std::uint8_t*>(device_alloc(bytes, "voxel mask"));
+            run_voxelizer(triangles, count, q, dev, s);
+            if (where == CFDX_HOST) {
+                check_cuda(cudaMemcpyAsync(out, dev, bytes, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync (mask)");
+                check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+            }
+        } catch (...) {
+            if (where == CFDX_HOST) device_free(dev);
+            cudaStreamDestroy(s);
+            throw;
+        }
+        if (where == CFDX_HOST) device_free(dev);
+        cudaStreamDestroy(s);
+    });
+}
+
+CFDX_API int cfdx_lbm_set_flags_surface(cfdx_lbm* h, const double* triangles, std::size_t count,
+                                        const double* minimum, const double* maximum, std::uint8_t solid_value,
+                                        const std::uint8_t* base_flags, int where) {
+    return guarded([&] {
+        checked(h);
+        const std::size_t nz = h->slab.on ? h->slab.nz_global : h->cfg.nz;
+        const auto planes = static_cast<std::uint32_t>(h->cfg.nz);
+        check_voxel_inputs(triangles, count, h->cfg.nx, h->cfg.ny, nz, minimum, maximum, planes);
+        require(solid_value >= 1U && solid_value < CFDX_MAX_WALL_IDS, "solid_value must be a wall id (1..15)");
+        VoxelRequest q{h->cfg.nx, h->cfg.ny, nz, {minimum[0], minimum[1], minimum[2]},
+                       {maximum[0], maximum[1], maximum[2]},
+                       h->slab.on ? (h->slab.z_begin + h->slab.nz_global - 1U) % h->slab.nz_global : 0U, planes,
+                       solid_value, nullptr};
+        std::uint8_t* staging = static_cast<std::uint8_t*>(device_alloc(2 * h->N, "voxel staging"));
+        try {
+            if (base_flags) {
+                upload(h, staging + h->N, base_flags, h->N, where);
+                q.base = staging + h->N;
+            }
+            run_voxelizer(triangles, count, q, staging, h->stream);
+            apply_flags(h, staging, CFDX_DEVICE);
+        } catch (...) {
+            device_free(staging);
+            throw;
+        }
+        device_free(staging);
     });
 }
 

@@ -355,6 +355,29 @@ class EsotericPullCudaSolver:
         self._call("cfdx_lbm_set_flags", ptr, where)
         self._has_mask = True
 
+    def set_solid_surface(self, triangles, minimum=(0.0, 0.0, 0.0), maximum=(1.0, 1.0, 1.0), solid_id: int = 1,
+                          base_flags=None):
+        """Flags from a closed triangle surface voxelized on the GPU over the box [minimum, maximum].
+
+        Cells inside get `solid_id` (1 wall, 2..15 moving wall), the others
+        `base_flags` (e.g. channel walls; host or device array of the handle's
+        cells) or fluid.  Reference: voxelize_surface + set_solid_mask
+        (examples/real_lbm3d_model.cpp:146-150).
+        """
+        from .geometry import as_surface
+
+        t = as_surface(triangles)
+        lo = np.ascontiguousarray(minimum, np.float64)
+        hi = np.ascontiguousarray(maximum, np.float64)
+        if base_flags is None:
+            ptr, where, keep = None, B.HOST, None
+        else:
+            ptr, where, keep = self._pointer(base_flags, np.uint8, self._cells, "base flag field")
+        self._call("cfdx_lbm_set_flags_surface", ctypes.c_void_p(t.ctypes.data), len(t),
+                   ctypes.c_void_p(lo.ctypes.data), ctypes.c_void_p(hi.ctypes.data), int(solid_id), ptr, where)
+        self._has_mask = True
+        del keep
+
     def set_wall_velocity(self, wall_id: int, ux: float, uy: float, uz: float):
         self._call("cfdx_lbm_set_wall_velocity", int(wall_id), ux, uy, uz)
 

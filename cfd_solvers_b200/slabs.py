@@ -319,6 +319,13 @@ class DistributedEsotericPullSolver:
     def set_wall_velocity(self, wall_id: int, ux: float, uy: float, uz: float):
         self.solver.set_wall_velocity(wall_id, ux, uy, uz)
 
+    def set_solid_surface(self, triangles, minimum=(0.0, 0.0, 0.0), maximum=(1.0, 1.0, 1.0), solid_id: int = 1,
+                          base_flags=None, local: bool = False):
+        """Flags from a surface voxelized over the whole lattice's box; each rank voxelizes its own planes."""
+        if base_flags is not None and not local:
+            base_flags = self.slab.local(np.asarray(base_flags, np.uint8))
+        self.solver.set_solid_surface(triangles, minimum, maximum, solid_id, base_flags)
+
     def set_solid_fraction(self, ns):
         self.solver.set_solid_fraction(None if ns is None else self.slab.local(np.asarray(ns, np.float32)))
 

@@ -374,6 +374,39 @@ CFDX_API int cfdx_lbm_halo_unpack(cfdx_lbm* lbm, int side, const void* device_bu
  * one slab. */
 CFDX_API int cfdx_lbm_halo_exchange(cfdx_lbm* lower, cfdx_lbm* upper);
 
+/* ---- Triangle-surface voxelizer (reference cfd::lbm::voxelize_surface,
+ * src/lbm/voxelize.cpp:4-5; SYCL voxelize_surface_sycl, src/sycl/voxelize_sycl.cpp:13-68).
+ * Cell (i, j, k) of the nx*ny*nz grid over [minimum, maximum] is solid when
+ * the ray from (min.x + (i+0.5)dx, min.y + (j+0.5)dy + 1e-10 dx,
+ * min.z + (k+0.5)dz + 2e-10 dx) in direction +x crosses the surface an odd
+ * number of times (Moller-Trumbore hits with |det| >= 1e-12 and distance >
+ * 1e-10), in FP64 with the reference's operation order: the mask equals the
+ * reference CPU voxelizer's bit for bit.  Triangles are 9 doubles each
+ * (a, b, c) in host memory; the surface need not be closed or oriented (a
+ * ray's parity decides).  Non-finite coordinates are rejected. */
+typedef struct cfdx_voxel_grid {
+    size_t nx, ny, nz;
+    double minimum[3];
+    double maximum[3];
+} cfdx_voxel_grid;
+
+/* Voxelizes global planes z_first .. z_first + z_count - 1 (mod nz) into
+ * `out` (nx*ny*z_count bytes, host or device memory of `device`): `solid_value`
+ * inside, 0 outside. */
+CFDX_API int cfdx_voxelize(const double* triangles, size_t count, const cfdx_voxel_grid* grid, uint32_t z_first,
+                           uint32_t z_count, uint8_t solid_value, uint8_t* out, int where, int device);
+
+/* Sets the handle's flags from a surface: the handle's lattice (a slab: its
+ * local planes of the whole lattice) is the voxel grid over [minimum, maximum];
+ * cells inside get `solid_value` (1 wall, 2..15 moving wall), the others
+ * base_flags[n] (the handle's cells, `where` memory) or 0 when base_flags is
+ * NULL.  The same as voxelizing and calling cfdx_lbm_set_flags, without the
+ * host round trip.  Reference use: voxelize_surface + set_solid_mask
+ * (examples/real_lbm3d_model.cpp:146-150). */
+CFDX_API int cfdx_lbm_set_flags_surface(cfdx_lbm* lbm, const double* triangles, size_t count, const double* minimum,
+                                        const double* maximum, uint8_t solid_value, const uint8_t* base_flags,
+                                        int where);
+
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */

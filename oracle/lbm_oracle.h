@@ -105,6 +105,15 @@ int ora_adjoint_forward(const ora_cfg* c, const double* x0, uint64_t steps, doub
 int ora_adjoint(const ora_cfg* c, const double* x0, uint64_t steps, const double* g_rho, const double* g_u,
                 double* grad_ns, double* grad_tau);
 
+/* Triangle-surface voxelizer and rigid transform (voxel_oracle.c; reference
+ * src/lbm/voxelize.cpp:4-6).  Triangles are 9 doubles (a, b, c); mask
+ * [(k*ny + j)*nx + i] is 1 inside.  ora_voxelize returns 1 on the inputs the
+ * reference rejects (no triangles, an empty grid or box). */
+int ora_voxelize(const double* tris, size_t count, size_t nx, size_t ny, size_t nz, const double* lo,
+                 const double* hi, uint8_t* mask);
+int ora_transform_surface(const double* tris, size_t count, const double* translation, const double* axis,
+                          double angle, double* out);
+
 /* IEEE binary16 round-to-nearest-even conversion used by the F16S storage. */
 uint16_t ora_f32_to_f16(float v);
 float ora_f16_to_f32(uint16_t h);

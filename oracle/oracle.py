@@ -82,7 +82,11 @@ def oracle_lib():
         lib.ora_reference_les_k.restype = ctypes.c_float
         lib.ora_adjoint_forward.argtypes = [P, _d, ctypes.c_uint64, _d]
         lib.ora_adjoint.argtypes = [P, _d, ctypes.c_uint64, _d, _d, _d, _d]
-        for name in ("ora_init", "ora_step", "ora_step_planes", "ora_macroscopic", "ora_reduce", "ora_logical", "ora_adjoint_forward",
+        sz = ctypes.c_size_t
+        lib.ora_voxelize.argtypes = [_d, sz, sz, sz, sz, _d, _d, _u8]
+        lib.ora_transform_surface.argtypes = [_d, sz, _d, _d, ctypes.c_double, _d]
+        for name in ("ora_voxelize", "ora_transform_surface", "ora_init", "ora_step", "ora_step_planes",
+                     "ora_macroscopic", "ora_reduce", "ora_logical", "ora_adjoint_forward",
                      "ora_adjoint"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
@@ -249,6 +253,24 @@ def logical_velocity(x: np.ndarray, q: int, cells: int, accel=(0.0, 0.0, 0.0)):
     return rho, np.where(rho > 0, u, 0.0)
 
 
+def voxelize(tris, nx: int, ny: int, nz: int, lo, hi) -> np.ndarray:
+    """Oracle voxel mask (uint8, n = (k*ny + j)*nx + i) of triangles (count x 9 doubles)."""
+    t = np.ascontiguousarray(tris, np.float64).reshape(-1, 9)
+    lo_, hi_ = np.ascontiguousarray(lo, np.float64), np.ascontiguousarray(hi, np.float64)
+    mask = np.zeros(nx * ny * nz, np.uint8)
+    if oracle_lib().ora_voxelize(_ptr(t, _d), len(t), nx, ny, nz, _ptr(lo_, _d), _ptr(hi_, _d), _ptr(mask, _u8)):
+        raise ValueError("invalid voxelization inputs")
+    return mask
+
+
+def transform_surface(tris, translation, axis, angle: float) -> np.ndarray:
+    t = np.ascontiguousarray(tris, np.float64).reshape(-1, 9)
+    tr, ax = np.ascontiguousarray(translation, np.float64), np.ascontiguousarray(axis, np.float64)
+    out = np.empty_like(t)
+    oracle_lib().ora_transform_surface(_ptr(t, _d), len(t), _ptr(tr, _d), _ptr(ax, _d), float(angle), _ptr(out, _d))
+    return out
+
+
 def f32_to_f16_bits(v: float) -> int:
     return int(oracle_lib().ora_f32_to_f16(v))
 
@@ -284,8 +306,30 @@ def ref_lib(fast: bool = False):
         lib.ref_bench.argtypes = [ctypes.c_int, sz, sz, sz, ctypes.c_float, ctypes.c_int, _u8, sz, sz, ctypes.c_uint,
                                   _d, _d]
         lib.ref_bench.restype = ctypes.c_double
+        lib.ref_voxelize.argtypes = [_d, sz, sz, sz, sz, _d, _d, _u8]
+        lib.ref_transform_surface.argtypes = [_d, sz, _d, _d, ctypes.c_double, _d]
         _ref[key] = lib
     return _ref[key]
+
+
+def ref_voxelize(tris, nx: int, ny: int, nz: int, lo, hi) -> np.ndarray:
+    """The reference's voxelize_surface (src/lbm/voxelize.cpp) on the same inputs."""
+    lib = ref_lib()
+    t = np.ascontiguousarray(tris, np.float64).reshape(-1, 9)
+    lo_, hi_ = np.ascontiguousarray(lo, np.float64), np.ascontiguousarray(hi, np.float64)
+    mask = np.zeros(nx * ny * nz, np.uint8)
+    _check(lib, lib.ref_voxelize(_ptr(t, _d), len(t), nx, ny, nz, _ptr(lo_, _d), _ptr(hi_, _d), _ptr(mask, _u8)))
+    return mask
+
+
+def ref_transform_surface(tris, translation, axis, angle: float) -> np.ndarray:
+    lib = ref_lib()
+    t = np.ascontiguousarray(tris, np.float64).reshape(-1, 9)
+    tr, ax = np.ascontiguousarray(translation, np.float64), np.ascontiguousarray(axis, np.float64)
+    out = np.empty_like(t)
+    _check(lib, lib.ref_transform_surface(_ptr(t, _d), len(t), _ptr(tr, _d), _ptr(ax, _d), float(angle),
+                                          _ptr(out, _d)))
+    return out
 
 
 def _init_args(init):

@@ -18,6 +18,7 @@
 #include "cfd/solvers/lbm/esoteric_pull.hpp"
 #include "cfd/solvers/lbm/one_step_pull.hpp"
 #include "cfd/solvers/lbm/precision_pull.hpp"
+#include "cfd/solvers/lbm/voxelize.hpp"
 
 #include <chrono>
 #include <cstdint>
@@ -214,6 +215,41 @@ int ref_compressed_run(int q, std::size_t nx, std::size_t ny, std::size_t nz, fl
             compressed_run<cfd::lbm::D3Q27Descriptor>(nx, ny, nz, tau, init_kind, init_p, steps, rho, ux, uy, uz, mass);
         else
             throw std::invalid_argument("q must be 19 or 27");
+    });
+}
+
+// The reference's triangle-surface voxelizer (src/lbm/voxelize.cpp):
+// triangles are 9 doubles each (a, b, c), the grid spans [lo, hi].
+int ref_voxelize(const double* tris, std::size_t count, std::size_t nx, std::size_t ny, std::size_t nz,
+                 const double* lo, const double* hi, std::uint8_t* mask) {
+    return guarded([&] {
+        cfd::io::TriangleSurface s;
+        for (std::size_t t = 0; t < count; ++t) {
+            const double* v = tris + 9 * t;
+            s.triangles.push_back({{v[0], v[1], v[2]}, {v[3], v[4], v[5]}, {v[6], v[7], v[8]}});
+        }
+        const cfd::lbm::VoxelGrid3D g{nx, ny, nz, {lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}};
+        const auto m = cfd::lbm::voxelize_surface(s, g);
+        std::memcpy(mask, m.data(), m.size());
+    });
+}
+
+// The reference's rigid transform of a surface (rotation about `axis` by `angle`, then translation).
+int ref_transform_surface(const double* tris, std::size_t count, const double* translation, const double* axis,
+                          double angle, double* out) {
+    return guarded([&] {
+        cfd::io::TriangleSurface s;
+        for (std::size_t t = 0; t < count; ++t) {
+            const double* v = tris + 9 * t;
+            s.triangles.push_back({{v[0], v[1], v[2]}, {v[3], v[4], v[5]}, {v[6], v[7], v[8]}});
+        }
+        const auto r = cfd::lbm::transform_surface(s, {translation[0], translation[1], translation[2]},
+                                                   {axis[0], axis[1], axis[2]}, angle);
+        for (std::size_t t = 0; t < count; ++t) {
+            const auto& q = r.triangles[t];
+            const double v[9] = {q.a.x, q.a.y, q.a.z, q.b.x, q.b.y, q.b.z, q.c.x, q.c.y, q.c.z};
+            std::memcpy(out + 9 * t, v, sizeof v);
+        }
     });
 }
 
