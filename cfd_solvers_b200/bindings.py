@@ -165,6 +165,10 @@ SIGNATURES = {
     "cfdx_voxelize": (_i, [_vp, _sz, ctypes.POINTER(cfdx_voxel_grid), ctypes.c_uint32, ctypes.c_uint32,
                            ctypes.c_uint8, _vp, _i, _i]),
     "cfdx_lbm_set_flags_surface": (_i, [_H, _vp, _sz, _vp, _vp, ctypes.c_uint8, _vp, _i]),
+    "cfdx_write_vtk_3d": (_i, [ctypes.c_char_p, _sz, _sz, _sz, _vp, _vp, _vp, ctypes.c_char_p, _i]),
+    "cfdx_write_json_state_3d": (_i, [ctypes.c_char_p, _sz, _sz, _sz, ctypes.c_uint64, _vp, _vp, ctypes.c_char_p]),
+    "cfdx_q_criterion": (_i, [_vp, _sz, _sz, _sz, ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp, _i, _i]),
+    "cfdx_lbm_q_criterion": (_i, [_H, ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp, _i]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

@@ -24,6 +24,7 @@
 #include "handle_access.h"
 #include "lbm_launch.h"
 #include "voxelize.h"
+#include "export.h"
 
 namespace {
 
@@ -1751,6 +1752,123 @@ CFDX_API int cfdx_lbm_set_flags_surface(cfdx_lbm* h, const double* triangles, st
             throw;
         }
         device_free(staging);
+    });
+}
+
+// ------------------------------------------------------------ field export
+extern "C++" {
+namespace {
+
+// Writer failures: size errors stay CFDX_ERR_INVALID, file errors become CFDX_ERR_IO.
+template <class F> void as_io(F&& write) {
+    try {
+        write();
+    } catch (const std::invalid_argument&) {
+        throw;
+    } catch (const std::runtime_error& e) {
+        fail(CFDX_ERR_IO, e.what());
+    }
+}
+
+void check_q_grid(std::size_t nx, std::size_t ny, std::size_t nz, double dx, double dy, double dz) {
+    // reference visualization.cpp:124-125
+    require(nx >= 3 && ny >= 3 && nz >= 3 && dx > 0.0 && dy > 0.0 && dz > 0.0, "invalid LBM Q-criterion grid");
+    require(nx <= (1ULL << 30) && ny <= 65535U && nz <= 65535U, "Q-criterion grid exceeds launch limits");
+}
+
+} // namespace
+} // extern "C++"
+
+CFDX_API int cfdx_write_vtk_3d(const char* path, std::size_t nx, std::size_t ny, std::size_t nz, const double* scalar,
+                               const double* velocity, const std::uint8_t* solid, const char* scalar_name,
+                               int binary) {
+    return guarded([&] {
+        require(path != nullptr && scalar != nullptr, "null path or scalar field");
+        as_io([&] { write_vtk_3d(path, nx, ny, nz, scalar, velocity, solid, scalar_name ? scalar_name : "field",
+                                 binary != 0); });
+    });
+}
+
+CFDX_API int cfdx_write_json_state_3d(const char* path, std::size_t nx, std::size_t ny, std::size_t nz,
+                                      std::uint64_t step, const double* scalar, const std::uint8_t* solid,
+                                      const char* scalar_name) {
+    return guarded([&] {
+        require(path != nullptr && scalar != nullptr, "null path or scalar field");
+        as_io([&] { write_json_state_3d(path, nx, ny, nz, step, scalar, solid, scalar_name ? scalar_name : "field"); });
+    });
+}
+
+CFDX_API int cfdx_q_criterion(const double* velocity, std::size_t nx, std::size_t ny, std::size_t nz, double dx,
+                              double dy, double dz, double* q, int where, int device) {
+    return guarded([&] {
+        require(velocity != nullptr && q != nullptr, "null velocity or output");
+        check_q_grid(nx, ny, nz, dx, dy, dz);
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        int devices = 0;
+        if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+            fail(CFDX_ERR_CUDA, "no CUDA device is available (the B200 engine has no CPU fallback)");
+        require(device >= 0 && device < devices, "device ordinal out of range");
+        check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        const std::size_t n = nx * ny * nz;
+        cudaStream_t s = nullptr;
+        check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+        double* staging = nullptr;
+        try {
+            const double* u = velocity;
+            double* out = q;
+            if (where == CFDX_HOST) {
+                staging = static_cast<double*>(device_alloc(4 * n * sizeof(double), "Q-criterion staging"));
+                check_cuda(cudaMemcpyAsync(staging, velocity, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s),
+                           "cudaMemcpyAsync (velocity)");
+                u = staging;
+                out = staging + 3 * n;
+            }
+            check_cuda(launch_q_criterion(u, u + 1, u + 2, true, 3, nx, ny, nz, dx, dy, dz, out, s),
+                       "Q-criterion kernel");
+            if (where == CFDX_HOST)
+                check_cuda(cudaMemcpyAsync(q, out, n * sizeof(double), cudaMemcpyDeviceToHost, s),
+                           "cudaMemcpyAsync (Q)");
+            check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        } catch (...) {
+            device_free(staging);
+            cudaStreamDestroy(s);
+            throw;
+        }
+        device_free(staging);
+        cudaStreamDestroy(s);
+    });
+}
+
+CFDX_API int cfdx_lbm_q_criterion(cfdx_lbm* h, double dx, double dy, double dz, double* q, int where) {
+    return guarded([&] {
+        checked(h);
+        require(q != nullptr, "null output");
+        require(!h->slab.on, "the Q-criterion of a slab needs its neighbours' velocities: gather the whole lattice");
+        check_q_grid(h->cfg.nx, h->cfg.ny, h->cfg.nz, dx, dy, dz);
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        const std::size_t n = h->N;
+        // rho | ux | uy | uz as cfdx_lbm_macroscopic_f64 reports them, then Q
+        double* s = static_cast<double*>(device_alloc((where == CFDX_HOST ? 5 : 4) * n * sizeof(double),
+                                                      "Q-criterion staging"));
+        try {
+            check_cuda(launch_macro(h->key, h->args(), s, s + n, s + 2 * n, s + 3 * n, true, h->grid(), h->block(),
+                                    h->stream),
+                       "macroscopic kernel");
+            double* out = where == CFDX_HOST ? s + 4 * n : q;
+            check_cuda(launch_q_criterion(s + n, s + 2 * n, s + 3 * n, true, 1, h->cfg.nx, h->cfg.ny, h->cfg.nz, dx,
+                                          dy, dz, out, h->stream),
+                       "Q-criterion kernel");
+            if (where == CFDX_HOST) {
+                check_cuda(cudaMemcpyAsync(q, out, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+                           "cudaMemcpyAsync (Q)");
+                h->d2h += n * sizeof(double);
+            }
+            h->sync();
+        } catch (...) {
+            device_free(s);
+            throw;
+        }
+        device_free(s);
     });
 }
 

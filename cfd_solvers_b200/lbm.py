@@ -378,6 +378,55 @@ class EsotericPullCudaSolver:
         self._has_mask = True
         del keep
 
+    # ------------------------------------------------------------ export
+    def q_criterion(self, dx: float = 1.0, dy: float = 1.0, dz: float = 1.0, out=None):
+        """Q-criterion of the current velocity, computed on the device (reference q_criterion_3d).
+
+        Returns a float64 numpy array, or fills `out` (a float64 CUDA tensor of the cells).
+        """
+        if out is not None:
+            if not _is_device(out) or out.numel() != self._cells:
+                raise ValueError("out must be a CUDA tensor of one float64 per cell")
+            self._call("cfdx_lbm_q_criterion", float(dx), float(dy), float(dz), ctypes.c_void_p(out.data_ptr()),
+                       B.DEVICE)
+            return out
+        q = np.zeros(self._cells, np.float64)
+        self._call("cfdx_lbm_q_criterion", float(dx), float(dy), float(dz), ctypes.c_void_p(q.ctypes.data), B.HOST)
+        return q
+
+    def _export_field(self, field: str):
+        from .export import speed
+
+        f = self.compute_macroscopic()
+        if field == "speed":
+            return speed(f), f
+        if field == "rho":
+            return np.asarray(f.rho, np.float64), f
+        if field == "q_criterion":
+            return self.q_criterion(), f
+        raise ValueError("field must be speed, rho or q_criterion")
+
+    def write_vtk(self, path, field: str = "speed", velocity: bool = True, solid: bool = True, binary: bool = False):
+        """Legacy-VTK file of `field` (speed, rho or q_criterion), the velocity and the wall cells
+        (rho = 0), as the reference's examples write frames (examples/real_lbm3d_model.cpp:120-125)."""
+        from .export import write_vtk_structured_3d
+
+        s, f = self._export_field(field)
+        c = self._config
+        write_vtk_structured_3d(path, c.nx, c.ny, self._cells // (c.nx * c.ny), s,
+                                (f.ux, f.uy, f.uz) if velocity else None,
+                                (np.asarray(f.rho) == 0).astype(np.uint8) if solid else None, field, binary,
+                                library=self._lib)
+
+    def write_json_state(self, path, field: str = "speed", solid: bool = True):
+        """The JSON live state of `field` at the current time step (reference write_json_state_3d)."""
+        from .export import write_json_state_3d
+
+        s, f = self._export_field(field)
+        c = self._config
+        write_json_state_3d(path, c.nx, c.ny, self._cells // (c.nx * c.ny), self.time_step(), s,
+                            (np.asarray(f.rho) == 0).astype(np.uint8) if solid else None, field, library=self._lib)
+
     def set_wall_velocity(self, wall_id: int, ux: float, uy: float, uz: float):
         self._call("cfdx_lbm_set_wall_velocity", int(wall_id), ux, uy, uz)
 

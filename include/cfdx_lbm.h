@@ -407,6 +407,31 @@ CFDX_API int cfdx_lbm_set_flags_surface(cfdx_lbm* lbm, const double* triangles, 
                                         const double* maximum, uint8_t solid_value, const uint8_t* base_flags,
                                         int where);
 
+/* ---- Field export (reference visualization.hpp:17-22, src/lbm/visualization.cpp:39-148).
+ * Host-only writers: legacy-VTK structured points (one scalar, optional
+ * velocity vectors as 3 doubles per cell x,y,z, optional solid bytes) and the
+ * JSON live state (written to "<path>.tmp", then renamed over path).  ASCII
+ * VTK and JSON text equal the reference writers' output byte for byte;
+ * binary = 1 writes the big-endian binary legacy format instead (the
+ * reference writes ASCII only).  I/O failures return CFDX_ERR_IO. */
+CFDX_API int cfdx_write_vtk_3d(const char* path, size_t nx, size_t ny, size_t nz, const double* scalar,
+                               const double* velocity, const uint8_t* solid, const char* scalar_name, int binary);
+CFDX_API int cfdx_write_json_state_3d(const char* path, size_t nx, size_t ny, size_t nz, uint64_t step,
+                                      const double* scalar, const uint8_t* solid, const char* scalar_name);
+
+/* Q-criterion (|Omega|^2 - |S|^2)/2 of a velocity field (3 doubles per cell,
+ * x,y,z; host or device memory of `device`) with central differences over
+ * spacings dx, dy, dz, 0 on the outer layer of cells: reference q_criterion_3d
+ * (visualization.cpp:122-148) on the device, equal to it bit for bit.  Grids
+ * need nx, ny, nz >= 3. */
+CFDX_API int cfdx_q_criterion(const double* velocity, size_t nx, size_t ny, size_t nz, double dx, double dy,
+                              double dz, double* q, int where, int device);
+
+/* The Q-criterion of the handle's current velocity (u + a/2 as
+ * cfdx_lbm_macroscopic_f64 reports it; walls 0), without a host round trip.
+ * Whole lattices only (a slab's edge planes need the neighbours' velocities). */
+CFDX_API int cfdx_lbm_q_criterion(cfdx_lbm* lbm, double dx, double dy, double dz, double* q, int where);
+
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */

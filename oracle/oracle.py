@@ -271,6 +271,35 @@ def transform_surface(tris, translation, axis, angle: float) -> np.ndarray:
     return out
 
 
+def q_criterion(velocity, nx: int, ny: int, nz: int, dx: float = 1.0, dy: float = 1.0, dz: float = 1.0):
+    """Q-criterion restated in numpy, operand for operand as the reference's q_criterion_3d
+    (src/lbm/visualization.cpp:122-148): central differences (p - m) / (2 d), then
+    s2, o2 accumulated over (i, j) in row order; 0 on the outer layer."""
+    u = np.asarray(velocity, np.float64).reshape(nz, ny, nx, 3)
+    q = np.zeros((nz, ny, nx), np.float64)
+    c = (slice(1, -1),) * 3
+
+    def d(axis, comp, h):
+        sl_p = [slice(1, -1)] * 3
+        sl_m = [slice(1, -1)] * 3
+        sl_p[axis] = slice(2, None)
+        sl_m[axis] = slice(0, -2)
+        return (u[tuple(sl_p) + (comp,)] - u[tuple(sl_m) + (comp,)]) / (2 * h)
+
+    # axes of the array: 0 = z, 1 = y, 2 = x
+    g = [[d(2, i, dx), d(1, i, dy), d(0, i, dz)] for i in range(3)]
+    s2 = np.zeros(q[c].shape)
+    o2 = np.zeros(q[c].shape)
+    for i in range(3):
+        for j in range(3):
+            sij = 0.5 * (g[i][j] + g[j][i])
+            oij = 0.5 * (g[i][j] - g[j][i])
+            s2 = s2 + sij * sij
+            o2 = o2 + oij * oij
+    q[c] = 0.5 * (o2 - s2)
+    return q.reshape(-1)
+
+
 def f32_to_f16_bits(v: float) -> int:
     return int(oracle_lib().ora_f32_to_f16(v))
 

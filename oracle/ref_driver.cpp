@@ -18,6 +18,7 @@
 #include "cfd/solvers/lbm/esoteric_pull.hpp"
 #include "cfd/solvers/lbm/one_step_pull.hpp"
 #include "cfd/solvers/lbm/precision_pull.hpp"
+#include "cfd/solvers/lbm/visualization.hpp"
 #include "cfd/solvers/lbm/voxelize.hpp"
 
 #include <chrono>
@@ -250,6 +251,44 @@ int ref_transform_surface(const double* tris, std::size_t count, const double* t
             const double v[9] = {q.a.x, q.a.y, q.a.z, q.b.x, q.b.y, q.b.z, q.c.x, q.c.y, q.c.z};
             std::memcpy(out + 9 * t, v, sizeof v);
         }
+    });
+}
+
+// The reference's field writers and Q-criterion (src/lbm/visualization.cpp:39-148);
+// velocity is 3 doubles per cell (x, y, z), solid may be null.
+int ref_write_vtk_3d(const char* path, std::size_t nx, std::size_t ny, std::size_t nz, const double* scalar,
+                     const double* velocity, const std::uint8_t* solid, const char* name) {
+    return guarded([&] {
+        const std::size_t n = nx * ny * nz;
+        std::vector<cfd::lbm::Vector3> u;
+        if (velocity)
+            for (std::size_t i = 0; i < n; ++i) u.push_back({velocity[3 * i], velocity[3 * i + 1], velocity[3 * i + 2]});
+        cfd::lbm::write_vtk_structured_3d(path, nx, ny, nz, std::span<const double>(scalar, n), u,
+                                          solid ? std::span<const std::uint8_t>(solid, n)
+                                                : std::span<const std::uint8_t>(),
+                                          name);
+    });
+}
+
+int ref_write_json_3d(const char* path, std::size_t nx, std::size_t ny, std::size_t nz, std::uint64_t step,
+                      const double* scalar, const std::uint8_t* solid, const char* name) {
+    return guarded([&] {
+        const std::size_t n = nx * ny * nz;
+        cfd::lbm::write_json_state_3d(path, nx, ny, nz, step, std::span<const double>(scalar, n),
+                                      solid ? std::span<const std::uint8_t>(solid, n)
+                                            : std::span<const std::uint8_t>(),
+                                      name);
+    });
+}
+
+int ref_q_criterion(std::size_t nx, std::size_t ny, std::size_t nz, const double* velocity, double dx, double dy,
+                    double dz, double* q) {
+    return guarded([&] {
+        const std::size_t n = nx * ny * nz;
+        std::vector<cfd::lbm::Vector3> u;
+        for (std::size_t i = 0; i < n; ++i) u.push_back({velocity[3 * i], velocity[3 * i + 1], velocity[3 * i + 2]});
+        const auto r = cfd::lbm::q_criterion_3d(nx, ny, nz, u, dx, dy, dz);
+        std::memcpy(q, r.data(), n * sizeof(double));
     });
 }
 
