@@ -152,17 +152,15 @@ struct cfdx_lbm {
     LaunchShape shape{};
     int variant = 0; // step kernel: 0 auto, 1 one cell per thread, 2 paired cells
     // Automatic choice between the one-cell and the paired-cell kernel, from
-    // B200 measurements at 512^3: pairs win for D3Q19 FP16 storage (2-7%),
-    // lose for FP32 storage and for D3Q27 (the 26 neighbour words of a pair
-    // need more shuffles and registers than the kernel can hold).
-    static bool paired_default(int storage, int q) { return storage == kStoreF16S && q == 19; }
-    // ... and only while few fluid cells touch a wall: the two-cell kernel
-    // reloads wall links in a second pass, the one-cell kernel loads them
-    // directly.  Measured at 512^3 FP16 D3Q19: cavity (2.3 % near-wall)
-    // 46.2 vs 41.9 GLUPS two-cell vs one-cell; 512x256x256 sphere pack with
-    // 10 % solid 35.7 vs 39.2.
-    static constexpr double kPairedNearWallLimit = 0.04;
-    double near_wall_fraction = 0.0; // fluid cells with a wall neighbour / fluid cells
+    // B200 measurements (GLUPS, FP16 D3Q19, one-cell vs two-cell): pairs win
+    // only on lattices without flags (BGK periodic 512^3: 63.7 vs 55.1).  With
+    // flags the one-cell kernel, whose wall links cost no divergence, wins:
+    // LES cavity 48.5 vs 45.8, TRT cavity 51.6 vs 49.6, 512x256x256 sphere
+    // pack 45.4 vs 35.4.  Pairs lose for FP32 storage and for D3Q27 (the 26
+    // neighbour words of a pair need more registers than the kernel can hold).
+    static bool paired_default(int storage, int q, bool flags) {
+        return storage == kStoreF16S && q == 19 && !flags;
+    }
     double les_k = 0.0;
     std::uint64_t h2d = 0, d2h = 0, syncs = 0;
     bool moving_walls = false; // some flag is a moving-wall id (2..15)
@@ -298,8 +296,7 @@ struct cfdx_lbm {
     }
     void choose_variant() {
         key.narrow = static_cast<unsigned long long>(key.q) * N < (1ULL << 32);
-        key.paired = variant == 2 || (variant == 0 && paired_eligible() && paired_default(key.storage, key.q) &&
-                                      near_wall_fraction < kPairedNearWallLimit);
+        key.paired = variant == 2 || (variant == 0 && paired_eligible() && paired_default(key.storage, key.q, key.flags));
     }
     dim3 step_block() const {
         if (!key.paired) return block();
@@ -747,7 +744,6 @@ void apply_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
     if (!flags && !h->slab.on) {
         h->key.flags = false;
         h->moving_walls = false;
-        h->near_wall_fraction = 0.0;
         h->choose_variant();
         return;
     }
@@ -777,24 +773,6 @@ void apply_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
         check_cuda(launch_prepare_flags(h->key.q, h->args(), user, h->flags, h->wall_mask, h->slab.on, h->grid(),
                                         h->block(), h->stream),
                    "flag preparation kernel");
-        // count fluid cells and near-wall fluid cells (for the kernel choice)
-        unsigned long long* counts =
-            static_cast<unsigned long long*>(device_alloc(2 * sizeof(unsigned long long), "flag counters"));
-        unsigned long long host_counts[2] = {0, 0};
-        try {
-            check_cuda(cudaMemsetAsync(counts, 0, sizeof host_counts, h->stream), "cudaMemsetAsync");
-            check_cuda(launch_count_flags(h->flags, static_cast<std::uint32_t>(h->N), counts, h->stream),
-                       "flag count kernel");
-            check_cuda(cudaMemcpyAsync(host_counts, counts, sizeof host_counts, cudaMemcpyDeviceToHost, h->stream),
-                       "cudaMemcpyAsync (flag counts)");
-            h->sync();
-        } catch (...) {
-            device_free(counts);
-            throw;
-        }
-        device_free(counts);
-        h->near_wall_fraction =
-            host_counts[0] ? static_cast<double>(host_counts[1]) / static_cast<double>(host_counts[0]) : 0.0;
         h->sync();
     } catch (...) {
         device_free(user);

@@ -300,15 +300,18 @@ __device__ __forceinline__ void moving_wall_pairs(const LbmArgs& a, u32 n, const
     }
 }
 
+// With flags every fluid cell takes the wall-link path; cells without a wall
+// neighbour have an empty mask, so the links pick the plain slots.  A warp of
+// mixed near-wall and interior cells then runs one gather instead of both
+// (measured on B200, 512^3 LES cavity / 512x256x256 sphere pack: +14 % / +13 %
+// FP16, +2 % / +7 % FP32 over branching on the near-wall bit).
 template <class L, class S, bool FLAGS, bool NARROW = false, bool RAW = false>
 __device__ __forceinline__ void gather_loads(const LbmArgs& a, u32 n, const Nbr& o, std::uint8_t flag,
                                              typename S::R* fin) {
     fin[0] = ld<S, L, 0, RAW>(Slots<S, NARROW>::rest(a, n), a);
     if constexpr (FLAGS) {
-        if (flag & kFlagNearWall) {
-            gather_walls<L, S, NARROW, RAW>(a, n, o, a.wall_mask[n], fin);
-            return;
-        }
+        gather_walls<L, S, NARROW, RAW>(a, n, o, (flag & kFlagNearWall) ? a.wall_mask[n] : 0U, fin);
+        return;
     }
     gather_plain<L, S, NARROW, RAW>(a, n, o, fin);
 }
@@ -967,10 +970,12 @@ __device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, V* h) {
 // it caps registers at 65536 / (128 * blocks).  The step is latency bound at
 // the occupancy its natural register count allows: measured on B200 at 512^3,
 // 10 blocks (48 registers, a few spilled words that stay in L1) beat the
-// uncapped 64-96 registers by 10-55% for FP32 and FP16 storage; FP64 storage
-// keeps its full register set.  The macros exist for tuning builds.
+// uncapped 64-96 registers by 10-55% for FP32 and FP16 storage, and for D3Q19
+// 12 blocks (40 registers) beat 10 once the wall path stopped branching (LES
+// cavity FP16 48.4 vs 46.9, FP32 40.6 vs 40.0; sphere pack within 0.5 %);
+// FP64 storage keeps its full register set.  The macros exist for tuning builds.
 #ifndef CFDX_STEP_MIN_BLOCKS_Q19
-#define CFDX_STEP_MIN_BLOCKS_Q19 10
+#define CFDX_STEP_MIN_BLOCKS_Q19 12
 #endif
 #ifndef CFDX_STEP_MIN_BLOCKS_Q27_F16
 #define CFDX_STEP_MIN_BLOCKS_Q27_F16 10
@@ -1242,28 +1247,6 @@ __global__ void __launch_bounds__(128) k_slot_in(const __grid_constant__ LbmArgs
         *p = __float2half_rn((in[n] - w) * a.scale[d]);
     } else {
         *p = typename S::T(in[n]);
-    }
-}
-
-// Counts fluid cells (out[0]) and fluid cells with a wall neighbour (out[1])
-// of the internal flags; the host uses the ratio to pick the step kernel.
-static __global__ void __launch_bounds__(256) k_count_flags(const std::uint8_t* flags, u32 n, unsigned long long* out) {
-    unsigned long long fluid = 0, near = 0;
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const std::uint8_t f = flags[i];
-        if ((f & kFlagTypeMask) == 0) {
-            ++fluid;
-            if (f & kFlagNearWall) ++near;
-        }
-    }
-#pragma unroll
-    for (int s = 16; s > 0; s >>= 1) {
-        fluid += __shfl_down_sync(0xffffffffU, fluid, s);
-        near += __shfl_down_sync(0xffffffffU, near, s);
-    }
-    if ((threadIdx.x & 31U) == 0U) {
-        atomicAdd(out, fluid);
-        atomicAdd(out + 1, near);
     }
 }
 

@@ -14,11 +14,6 @@ cudaError_t launch_sum_partials(const double* partials, std::size_t count, doubl
     return cudaGetLastError();
 }
 
-cudaError_t launch_count_flags(const std::uint8_t* flags, std::uint32_t n, unsigned long long* out, cudaStream_t s) {
-    k_count_flags<<<592, 256, 0, s>>>(flags, n, out);
-    return cudaGetLastError();
-}
-
 // Flag preparation does not depend on the storage type; it lives here once.
 cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out,
                                  std::uint32_t* mask, bool ghost, dim3 g, dim3 b, cudaStream_t s) {

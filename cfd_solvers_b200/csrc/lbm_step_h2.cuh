@@ -183,11 +183,15 @@ __device__ __forceinline__ void h2_fixup(const LbmArgs& a, const __half* base, c
 #ifndef CFDX_H2_MIN_BLOCKS_LES
 #define CFDX_H2_MIN_BLOCKS_LES 6
 #endif
+#ifndef CFDX_H2_MIN_BLOCKS_WALLS
+#define CFDX_H2_MIN_BLOCKS_WALLS 6
+#endif
 #ifndef CFDX_H2_FAST_STORES
 #define CFDX_H2_FAST_STORES 1
 #endif
 template <class L, bool LES, bool FLAGS, bool GRAY>
-__global__ void __launch_bounds__(128, (LES || FLAGS) ? CFDX_H2_MIN_BLOCKS_LES : CFDX_H2_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, LES ? CFDX_H2_MIN_BLOCKS_LES
+                                          : (FLAGS ? CFDX_H2_MIN_BLOCKS_WALLS : CFDX_H2_MIN_BLOCKS))
     k_step_h2(const __grid_constant__ LbmArgs a) {
     H2Ctx c;
     c.x0 = 2U * (blockIdx.x * blockDim.x + threadIdx.x);

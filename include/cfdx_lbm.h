@@ -231,9 +231,9 @@ CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* lbm, void** device_ptr, size_t* 
 /* Launch shape of the cell kernels: threads per block (x, y) and the step
  * kernel variant: 0 automatic, 1 one cell per thread, 2 two adjacent x cells
  * per thread (FP32/FP16 storage, even nx).  Both variants give bitwise equal
- * results.  Automatic: two cells for D3Q19 FP16 unless more than 4 % of the
- * fluid cells touch a wall (measured: wall-dense lattices run faster one
- * cell per thread).  Zeros restore the defaults. */
+ * results.  Automatic: two cells for D3Q19 FP16 on lattices without flags,
+ * one cell otherwise (measured: with walls the one-cell kernel is faster).
+ * Zeros restore the defaults. */
 CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, int variant);
 
 /* The reduction of cfdx_lbm_reduce() without any allocation: no
