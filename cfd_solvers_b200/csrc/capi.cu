@@ -138,6 +138,9 @@ struct cfdx_lbm {
     std::size_t f_bytes = 0;
     std::uint8_t* flags = nullptr; // internal flag bytes
     std::uint32_t* wall_mask = nullptr; // wall-link bits of near-wall fluid cells
+    std::uint32_t* near_list = nullptr; // two-cell FP16 step with flags: cells of the pairs with walls (k_step_list)
+    std::uint32_t near_count = 0;
+    bool near_built = false;            // near_list matches the current flags
     float* local_a = nullptr;
     float* ns = nullptr;
     float* macro_scratch = nullptr; // 4*N floats, lazily allocated
@@ -153,11 +156,13 @@ struct cfdx_lbm {
     int variant = 0; // step kernel: 0 auto, 1 one cell per thread, 2 paired cells
     // Automatic choice between the one-cell and the paired-cell kernel, from
     // B200 measurements (GLUPS, FP16 D3Q19, one-cell vs two-cell): pairs win
-    // only on lattices without flags (BGK periodic 512^3: 63.7 vs 55.1).  With
+    // only on lattices without flags (BGK periodic 512^3: 64.3 vs 55.6).  With
     // flags the one-cell kernel, whose wall links cost no divergence, wins:
-    // LES cavity 48.5 vs 45.8, TRT cavity 51.6 vs 49.6, 512x256x256 sphere
-    // pack 45.4 vs 35.4.  Pairs lose for FP32 storage and for D3Q27 (the 26
-    // neighbour words of a pair need more registers than the kernel can hold).
+    // LES cavity 48.7 vs 44.6, TRT cavity 52.0 vs 43.8, 512x256x256 sphere
+    // pack 45.5 vs 34.4 (the two-cell kernel then leaves the pairs with walls
+    // to a list kernel whose scattered cells coalesce poorly).  Pairs lose for
+    // FP32 storage and for D3Q27 (the 26 neighbour words of a pair need more
+    // registers than the kernel can hold).
     static bool paired_default(int storage, int q, bool flags) {
         return storage == kStoreF16S && q == 19 && !flags;
     }
@@ -226,6 +231,8 @@ struct cfdx_lbm {
         set_parity(a, odd);
         a.flags = key.flags ? flags : nullptr;
         a.wall_mask = key.flags ? wall_mask : nullptr;
+        a.near_list = key.flags ? near_list : nullptr;
+        a.near_count = key.flags ? near_count : 0U;
         a.ax_field = local_a;
         a.ay_field = local_a ? local_a + N : nullptr;
         a.az_field = local_a ? local_a + 2 * N : nullptr;
@@ -416,6 +423,7 @@ void release(cfdx_lbm* h) {
     device_free(h->f);
     device_free(h->flags);
     device_free(h->wall_mask);
+    device_free(h->near_list);
     device_free(h->local_a);
     device_free(h->ns);
     device_free(h->macro_scratch);
@@ -737,6 +745,60 @@ CFDX_API int cfdx_lbm_init_fields(cfdx_lbm* h, const float* fields, int where) {
 
 namespace {
 
+// FP16 storage with even nx (the two-cell step): the list of fluid cells of
+// the x-pairs that are not interior, selected on the device from the
+// internal flags, kept at its exact size.
+void build_near_list(cfdx_lbm* h) {
+    device_free(h->near_list);
+    h->near_list = nullptr;
+    h->near_count = 0;
+    h->near_built = false;
+    if (h->key.storage != kStoreF16S || h->cfg.nx % 2U != 0U) return;
+    const auto cells = static_cast<std::uint32_t>(h->N);
+    std::size_t temp_bytes = 0;
+    check_cuda(select_near_cells(h->flags, cells, nullptr, nullptr, nullptr, &temp_bytes, h->stream),
+               "near-cell selection (size)");
+    const std::size_t list_bytes = ((h->N * sizeof(std::uint32_t)) + 255U) / 256U * 256U;
+    char* scratch = static_cast<char*>(device_alloc(list_bytes + 256U + temp_bytes, "near-cell selection scratch"));
+    try {
+        auto* all = reinterpret_cast<std::uint32_t*>(scratch);
+        auto* count = reinterpret_cast<std::uint32_t*>(scratch + list_bytes);
+        check_cuda(select_near_cells(h->flags, cells, all, count, scratch + list_bytes + 256U, &temp_bytes, h->stream),
+                   "near-cell selection");
+        std::uint32_t host_count = 0;
+        check_cuda(cudaMemcpyAsync(&host_count, count, sizeof host_count, cudaMemcpyDeviceToHost, h->stream),
+                   "cudaMemcpyAsync (near-cell count)");
+        h->sync();
+        if (host_count > 0U) {
+            h->near_list = static_cast<std::uint32_t*>(device_alloc(host_count * sizeof(std::uint32_t), "near-cell list"));
+            check_cuda(cudaMemcpyAsync(h->near_list, all, host_count * sizeof(std::uint32_t), cudaMemcpyDeviceToDevice,
+                                       h->stream),
+                       "cudaMemcpyAsync (near-cell list)");
+            h->sync();
+        }
+        h->near_count = host_count;
+        h->near_built = true;
+    } catch (...) {
+        device_free(scratch);
+        throw;
+    }
+    device_free(scratch);
+}
+
+// Keeps the near-cell list in step with the kernel choice: built when the
+// two-cell FP16 step runs with flags, dropped otherwise.  flags_changed: the
+// flag field was replaced, so a built list is stale.
+void refresh_near_list(cfdx_lbm* h, bool flags_changed) {
+    const bool need = h->key.paired && h->key.flags && h->key.storage == kStoreF16S;
+    if (flags_changed || !need) {
+        device_free(h->near_list);
+        h->near_list = nullptr;
+        h->near_count = 0;
+        h->near_built = false;
+    }
+    if (need && !h->near_built) build_near_list(h);
+}
+
 // Internal flags and wall-link masks from the caller's flags (nullptr: none;
 // on a slab, all own cells fluid -- its ghost planes stay marked).
 void apply_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
@@ -745,6 +807,7 @@ void apply_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
         h->key.flags = false;
         h->moving_walls = false;
         h->choose_variant();
+        refresh_near_list(h, true);
         return;
     }
     if (!h->flags) h->flags = static_cast<std::uint8_t*>(device_alloc(h->N, "flag field"));
@@ -781,6 +844,7 @@ void apply_flags(cfdx_lbm* h, const std::uint8_t* flags, int where) {
     device_free(user);
     h->key.flags = true;
     h->choose_variant();
+    refresh_near_list(h, true);
 }
 
 } // namespace
@@ -1260,6 +1324,7 @@ CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int variant)
                     "multiple of 32");
 
         h->choose_variant();
+        refresh_near_list(h, false);
     });
 }
 

@@ -79,6 +79,10 @@ struct LbmArgs {
     // Added to the local cell index before hashing: a z-slab hashes the
     // global index, so a decomposed lattice rounds like the whole one.
     std::uint32_t hash_base;
+    // Fluid cells of the x-pairs the two-cell FP16 step leaves out (pairs
+    // with a wall or a near-wall cell), in cell order; k_step_list steps them.
+    const std::uint32_t* near_list;
+    std::uint32_t near_count;
 };
 
 // Parameters of the adjoint kernels (lbm_adjoint.cuh).

@@ -66,6 +66,12 @@ cudaError_t launch_adjoint_step(const KernelKey& k, const AdjointArgs& a, dim3 g
 cudaError_t launch_slot_io(const KernelKey& k, const LbmArgs& a, int d, float* buffer, bool in, dim3 grid,
                            dim3 block, cudaStream_t s);
 cudaError_t launch_sum_partials(const double* partials, std::size_t count, double* out, cudaStream_t s);
+// Fluid cells of the pairs that are not interior (near_list.cu), in cell order:
+// the CUB select of `cells` indices into `out`, the count to *count (device).
+// With temp == nullptr it only sets *temp_bytes.
+cudaError_t select_near_cells(const std::uint8_t* flags, std::uint32_t cells, std::uint32_t* out,
+                              std::uint32_t* count, void* temp, std::size_t* temp_bytes, cudaStream_t s);
+
 // ghost: planes 0 and nz-1 are a z-slab's ghost planes (k_prepare_flags).
 cudaError_t launch_prepare_flags(int q, const LbmArgs& a, const std::uint8_t* user, std::uint8_t* out,
                                  std::uint32_t* mask, bool ghost, dim3 grid, dim3 block, cudaStream_t s);

@@ -46,10 +46,19 @@ cudaError_t step_paired(const LbmArgs& a, dim3 b, cudaStream_t s) {
     } else {
         const unsigned pairs = (a.nx + 1U) / 2U;
         dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, a.nz);
-        if constexpr (sizeof(typename S::T) == 2)
+        if constexpr (sizeof(typename S::T) == 2) {
+            // interior pairs two cells per thread, then the pairs with walls one cell per thread
             k_step_h2<L, LES, FL, GR><<<g, b, 0, s>>>(a);
-        else
+            if constexpr (FL) {
+                if (a.near_count > 0U) {
+                    const cudaError_t e = cudaGetLastError();
+                    if (e != cudaSuccess) return e;
+                    k_step_list<L, S, LES, GR><<<(a.near_count + 127U) / 128U, 128, 0, s>>>(a);
+                }
+            }
+        } else {
             k_step_x2<L, S, LES, FL, GR><<<g, b, 0, s>>>(a);
+        }
         return cudaGetLastError();
     }
 }
