@@ -17,6 +17,7 @@
 // cfd::lbm::cuda::InPlaceLbmConfig, which adds the engine's extensions.
 #pragma once
 
+#include <array>
 #include <cstddef>
 #include <cstdint>
 #include <new>
@@ -87,6 +88,19 @@ inline void check(int status, const char* what) {
     }
 }
 
+// 9 doubles (a, b, c) per triangle of any surface whose .triangles hold .a .b .c points.
+template <class Surface> std::vector<double> pack_triangles(const Surface& surface) {
+    std::vector<double> out;
+    out.reserve(9 * surface.triangles.size());
+    for (const auto& t : surface.triangles)
+        for (const auto* p : {&t.a, &t.b, &t.c}) {
+            out.push_back(p->x);
+            out.push_back(p->y);
+            out.push_back(p->z);
+        }
+    return out;
+}
+
 template <class C, class = void> struct has_extensions : std::false_type {};
 template <class C> struct has_extensions<C, std::void_t<decltype(std::declval<C>().storage)>> : std::true_type {};
 
@@ -100,6 +114,34 @@ public:
 
     template <class Config = cuda::InPlaceLbmConfig>
     explicit EsotericPullCudaSolver(const Config& config = Config{}) {
+        const cfdx_lbm_config c = native_config(config);
+        char error[1024] = {0};
+        const int status = cfdx_lbm_create(&c, &handle_, error, sizeof error);
+        if (status != CFDX_OK) {
+            handle_ = nullptr;
+            cuda::check(status, "cfdx_lbm_create");
+        }
+        config_ = c;
+        cells_ = c.nx * c.ny * c.nz;
+    }
+
+protected:
+    // A z-slab [z_begin, z_begin + z_extent) of the lattice `config` describes
+    // (EsotericPullCudaSlab): nx*ny*(z_extent + 2) local cells.
+    template <class Config>
+    EsotericPullCudaSolver(const Config& config, std::uint32_t z_begin, std::uint32_t z_extent) {
+        const cfdx_lbm_config c = native_config(config);
+        char error[1024] = {0};
+        const int status = cfdx_lbm_create_slab(&c, z_begin, z_extent, &handle_, error, sizeof error);
+        if (status != CFDX_OK) {
+            handle_ = nullptr;
+            cuda::check(status, "cfdx_lbm_create_slab");
+        }
+        config_ = c;
+        cells_ = c.nx * c.ny * (static_cast<std::size_t>(z_extent) + 2U);
+    }
+
+    template <class Config> static cfdx_lbm_config native_config(const Config& config) {
         cfdx_lbm_config c;
         cuda::check(cfdx_lbm_config_default(&c), "cfdx_lbm_config_default");
         c.nx = config.nx;
@@ -121,15 +163,10 @@ public:
             c.fp16_rounding = static_cast<int>(config.fp16_rounding);
             c.rounding_seed = config.rounding_seed;
         }
-        char error[1024] = {0};
-        const int status = cfdx_lbm_create(&c, &handle_, error, sizeof error);
-        if (status != CFDX_OK) {
-            handle_ = nullptr;
-            cuda::check(status, "cfdx_lbm_create");
-        }
-        config_ = c;
-        cells_ = c.nx * c.ny * c.nz;
+        return c;
     }
+
+public:
 
     ~EsotericPullCudaSolver() {
         if (handle_) cfdx_lbm_destroy(handle_);
@@ -242,6 +279,28 @@ public:
     void load_checkpoint(const std::string& path) {
         cuda::check(cfdx_lbm_checkpoint_load(handle_, path.c_str()), "load_checkpoint");
     }
+    // Flags from a closed triangle surface voxelized on the device over the box
+    // [minimum, maximum] (reference voxelize_surface + set_solid_mask,
+    // examples/real_lbm3d_model.cpp:146-150): `solid_id` inside, the base flags
+    // (or fluid) elsewhere.  Surface: any type whose .triangles hold .a .b .c
+    // points with .x .y .z (the reference's cfd::io::TriangleSurface).
+    template <class Surface, class Point>
+    void set_solid_surface(const Surface& surface, const Point& minimum, const Point& maximum,
+                           std::uint8_t solid_id = 1, std::span<const std::uint8_t> base_flags = {}) {
+        const std::vector<double> tris = cuda::pack_triangles(surface);
+        const double lo[3] = {minimum.x, minimum.y, minimum.z}, hi[3] = {maximum.x, maximum.y, maximum.z};
+        if (!base_flags.empty() && base_flags.size() != cells_)
+            throw std::invalid_argument("LBM flag field size mismatch");
+        cuda::check(cfdx_lbm_set_flags_surface(handle_, tris.data(), tris.size() / 9, lo, hi, solid_id,
+                                               base_flags.empty() ? nullptr : base_flags.data(), CFDX_HOST),
+                    "set_solid_surface");
+    }
+    // Q-criterion of the current velocity, computed on the device (reference q_criterion_3d).
+    [[nodiscard]] std::vector<double> q_criterion(double dx = 1.0, double dy = 1.0, double dz = 1.0) const {
+        std::vector<double> q(cells_);
+        cuda::check(cfdx_lbm_q_criterion(handle_, dx, dy, dz, q.data(), CFDX_HOST), "q_criterion");
+        return q;
+    }
     [[nodiscard]] cfdx_lbm* native_handle() const noexcept { return handle_; }
 
 private:
@@ -257,5 +316,117 @@ private:
     std::vector<std::uint8_t> mask_;
     bool local_{false};
 };
+
+// One z-slab of a lattice cut along z (the reference's DistributedPullBlock
+// brick, distributed_pull.hpp:35-60, cut along z only).  Per-cell arrays
+// cover the local planes, ghost planes first and last; after every step the
+// slab exchanges one message through each side (pack -> transport -> unpack,
+// or exchange_with for two slabs of one process).  See cfdx_lbm_create_slab.
+template <class Descriptor> class EsotericPullCudaSlab : public EsotericPullCudaSolver<Descriptor> {
+public:
+    template <class Config>
+    EsotericPullCudaSlab(const Config& config, std::uint32_t z_begin, std::uint32_t z_extent)
+        : EsotericPullCudaSolver<Descriptor>(config, z_begin, z_extent) {}
+
+    // (z_begin, z_extent, nz of the whole lattice)
+    [[nodiscard]] std::array<std::uint32_t, 3> slab_info() const {
+        std::array<std::uint32_t, 3> v{};
+        cuda::check(cfdx_lbm_slab_info(this->native_handle(), &v[0], &v[1], &v[2]), "slab_info");
+        return v;
+    }
+    [[nodiscard]] std::size_t halo_bytes() const {
+        std::size_t b = 0;
+        cuda::check(cfdx_lbm_halo_bytes(this->native_handle(), &b), "halo_bytes");
+        return b;
+    }
+    // side: CFDX_SIDE_LOWER / CFDX_SIDE_UPPER; buffers are device memory of halo_bytes()
+    void pack(int side, void* device_buffer) {
+        cuda::check(cfdx_lbm_halo_pack(this->native_handle(), side, device_buffer), "halo_pack");
+    }
+    void unpack(int side, const void* device_buffer) {
+        cuda::check(cfdx_lbm_halo_unpack(this->native_handle(), side, device_buffer), "halo_unpack");
+    }
+    // both messages of the cut between this slab's upper side and `upper`'s lower side
+    void exchange_with(EsotericPullCudaSlab& upper) {
+        cuda::check(cfdx_lbm_halo_exchange(this->native_handle(), upper.native_handle()), "halo_exchange");
+    }
+};
+
+namespace cuda {
+
+// Reference voxelize_surface (src/lbm/voxelize.cpp:5) on the device: the
+// same mask bit for bit.  Grid: any type with nx, ny, nz and .minimum /
+// .maximum points (the reference's VoxelGrid3D).
+template <class Surface, class Grid>
+[[nodiscard]] std::vector<unsigned char> voxelize_surface(const Surface& surface, const Grid& grid, int device = 0) {
+    const std::vector<double> tris = pack_triangles(surface);
+    cfdx_voxel_grid g{grid.nx, grid.ny, grid.nz, {grid.minimum.x, grid.minimum.y, grid.minimum.z},
+                      {grid.maximum.x, grid.maximum.y, grid.maximum.z}};
+    std::vector<unsigned char> mask(grid.nx * grid.ny * grid.nz);
+    check(cfdx_voxelize(tris.data(), tris.size() / 9, &g, 0U, static_cast<std::uint32_t>(grid.nz), 1U, mask.data(),
+                        CFDX_HOST, device),
+          "voxelize_surface");
+    return mask;
+}
+
+// The velocity type of a scalar-only VTK file.
+struct NoVector {
+    double x, y, z;
+};
+
+// 3 doubles per cell from any vector type with .x .y .z (the reference's Vector3).
+template <class V> std::vector<double> pack_vectors(std::span<const V> v) {
+    std::vector<double> out;
+    out.reserve(3 * v.size());
+    for (const auto& e : v) {
+        out.push_back(e.x);
+        out.push_back(e.y);
+        out.push_back(e.z);
+    }
+    return out;
+}
+
+// Reference write_vtk_structured_3d (visualization.cpp:39-67): the same ASCII
+// text; binary = true writes the big-endian binary legacy format.
+template <class V = NoVector>
+void write_vtk_structured_3d(const std::string& path, std::size_t nx, std::size_t ny, std::size_t nz,
+                             std::span<const double> scalar, std::span<const V> velocity = {},
+                             std::span<const std::uint8_t> solid = {}, const char* scalar_name = "field",
+                             bool binary = false) {
+    const std::size_t cells = nx * ny * nz;
+    if (scalar.size() != cells || (!velocity.empty() && velocity.size() != cells) ||
+        (!solid.empty() && solid.size() != cells))
+        throw std::invalid_argument("LBM 3-D VTK field size mismatch");
+    std::vector<double> u;
+    if constexpr (!std::is_same_v<V, NoVector>) u = pack_vectors(velocity);
+    check(cfdx_write_vtk_3d(path.c_str(), nx, ny, nz, scalar.data(), u.empty() ? nullptr : u.data(),
+                            solid.empty() ? nullptr : solid.data(), scalar_name, binary ? 1 : 0),
+          "write_vtk_structured_3d");
+}
+
+// Reference write_json_state_3d (visualization.cpp:68-109).
+inline void write_json_state_3d(const std::string& path, std::size_t nx, std::size_t ny, std::size_t nz,
+                                std::uint64_t step, std::span<const double> scalar,
+                                std::span<const std::uint8_t> solid = {}, const char* scalar_name = "field") {
+    if (scalar.size() != nx * ny * nz || (!solid.empty() && solid.size() != scalar.size()))
+        throw std::invalid_argument("LBM 3-D live state size mismatch");
+    check(cfdx_write_json_state_3d(path.c_str(), nx, ny, nz, step, scalar.data(), solid.empty() ? nullptr : solid.data(),
+                                   scalar_name),
+          "write_json_state_3d");
+}
+
+// Reference q_criterion_3d (visualization.cpp:122-148) on the device: the same values bit for bit.
+template <class V>
+[[nodiscard]] std::vector<double> q_criterion_3d(std::size_t nx, std::size_t ny, std::size_t nz,
+                                                 std::span<const V> velocity, double dx = 1.0, double dy = 1.0,
+                                                 double dz = 1.0, int device = 0) {
+    if (velocity.size() != nx * ny * nz) throw std::invalid_argument("invalid LBM Q-criterion grid");
+    const std::vector<double> u = pack_vectors(velocity);
+    std::vector<double> q(velocity.size());
+    check(cfdx_q_criterion(u.data(), nx, ny, nz, dx, dy, dz, q.data(), CFDX_HOST, device), "q_criterion_3d");
+    return q;
+}
+
+} // namespace cuda
 
 } // namespace cfd::lbm

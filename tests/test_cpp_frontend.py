@@ -72,6 +72,13 @@ def test_frontend_on_gpu_matches_python_api(frontend, tmp_path, engine):
         assert float(vals["checksum"]) == s.checksum()
         assert float(vals["mass"]) == s.mass()
     assert vals["restart_bitwise"] == "1"
+    # slab class, device voxelizer, Q-criterion and writers through the C++ front end
+    assert vals["slab_info"] == "0 16 16" and vals["slab_equals_whole"] == "1"
+    assert int(vals["halo_bytes"]) == 5 * 24 * 20 * 4
+    assert vals["voxel_cube"] == "1 0 64"  # the reference cube test's facts; 4^3 cells inside
+    assert vals["q_criterion_equal"] == "1" and vals["exported"] == "1"
+    assert (tmp_path / "frame.vtk").read_text().startswith("# vtk DataFile Version 3.0\ncfd_solvers LBM 3-D\nASCII")
+    assert '"dimensions": [24, 20, 16]' in (tmp_path / "state.json").read_text()
     assert vals["size_mismatch"] == "invalid_argument"
     assert vals["wall_id"] == "out_of_range"
 
