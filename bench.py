@@ -573,6 +573,48 @@ def voxelizer_measure(torch, device, n=512, subdivisions=7, cpu_sample=True):
     return res
 
 
+def q_criterion_measure(torch, cs, n, device, cpu_sample=True):
+    """The device Q-criterion of the cavity's velocity (macroscopic + Q kernels, output in
+    device memory), best of 3 after a warm-up; the reference's q_criterion_3d (one core)
+    timed on a 96^3 sample of the same field for comparison."""
+    s = make_cavity(cs, n, device=device)
+    try:
+        setup_cavity(s, cs, n)
+        s.step(20)
+        out = torch.empty(n ** 3, dtype=torch.float64, device=f"cuda:{device}")
+        s.q_criterion(out=out)
+        times = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.q_criterion(out=out)
+            times.append(time.perf_counter() - t0)
+        sec = min(times)
+        res = {"grid": f"{n}^3", "ms": sec * 1e3, "gcells_per_s": n ** 3 / sec / 1e9,
+               "note": "cfdx_lbm_q_criterion: FP64 macroscopic + Q kernels, device output, incl. scratch"}
+        if cpu_sample:
+            from oracle import oracle as O
+
+            if O.reference_available():
+                import ctypes
+
+                m = 96
+                rng = np.random.default_rng(1)
+                vel = np.ascontiguousarray(rng.normal(0, 0.05, (m ** 3, 3)))
+                q = np.zeros(m ** 3)
+                lib = O.ref_lib()
+                dp = ctypes.POINTER(ctypes.c_double)
+                lib.ref_q_criterion.argtypes = [ctypes.c_size_t] * 3 + [dp] + [ctypes.c_double] * 3 + [dp]
+                t0 = time.perf_counter()
+                lib.ref_q_criterion(m, m, m, vel.ctypes.data_as(dp), 1.0, 1.0, 1.0, q.ctypes.data_as(dp))
+                cpu = time.perf_counter() - t0
+                res["cpu_reference"] = {"sample": f"{m}^3 random field", "seconds": cpu, "cores": 1,
+                                        "gcells_per_s": m ** 3 / cpu / 1e9}
+    finally:
+        s.close()
+    return res
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -839,6 +881,8 @@ def main(argv=None):
             variants["d3q27_fp32"] = d27
             variants["z_slabs_one_gpu"] = slab_exchange_overhead(torch, cs, n, vs, local_rank, ms / args.steps)
             variants["voxelizer"] = voxelizer_measure(torch, local_rank, n, cpu_sample=not args.no_cpu_baseline)
+            variants["q_criterion"] = q_criterion_measure(torch, cs, n, local_rank,
+                                                          cpu_sample=not args.no_cpu_baseline)
         if not args.no_differentiation:
             variants["differentiation"] = differentiation_variants(torch, cs, local_rank)
         if not args.no_precision:
