@@ -169,6 +169,17 @@ SIGNATURES = {
     "cfdx_write_json_state_3d": (_i, [ctypes.c_char_p, _sz, _sz, _sz, ctypes.c_uint64, _vp, _vp, ctypes.c_char_p]),
     "cfdx_q_criterion": (_i, [_vp, _sz, _sz, _sz, ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp, _i, _i]),
     "cfdx_lbm_q_criterion": (_i, [_H, ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp, _i]),
+    "cfdx_thermal_create": (_i, [_H, ctypes.c_float, ctypes.POINTER(_vp), ctypes.c_char_p, _sz]),
+    "cfdx_thermal_destroy": (_i, [_vp]),
+    "cfdx_thermal_init_uniform": (_i, [_vp, ctypes.c_float]),
+    "cfdx_thermal_init_field": (_i, [_vp, _vp, _i]),
+    "cfdx_thermal_step": (_i, [_vp, _vp, _vp, _vp, ctypes.c_uint64]),
+    "cfdx_thermal_refresh_device_scalar": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "cfdx_thermal_temperature": (_i, [_vp, _vp, _i]),
+    "cfdx_thermal_add_boussinesq": (_i, [_vp, _vp, _vp, _vp] + [ctypes.c_float] * 5),
+    "cfdx_thermal_total": (_i, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "cfdx_thermal_info": (_i, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(ctypes.c_uint64),
+                               ctypes.POINTER(ctypes.c_uint64)]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

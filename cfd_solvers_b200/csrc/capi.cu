@@ -25,6 +25,7 @@
 #include "lbm_launch.h"
 #include "voxelize.h"
 #include "export.h"
+#include "thermal.h"
 
 namespace {
 
@@ -1912,6 +1913,192 @@ CFDX_API int cfdx_lbm_q_criterion(cfdx_lbm* h, double dx, double dy, double dz, 
             throw;
         }
         device_free(s);
+    });
+}
+
+// ------------------------------------------------- resident thermal lattice
+struct cfdx_thermal {
+    cfdx_lbm* flow = nullptr; // borrowed: its device and stream
+    ThermalGrid grid{};
+    float tau = 0.0F, omega = 0.0F;
+    float* g = nullptr;
+    float* next = nullptr;
+    float* scalar = nullptr;     // temperature scratch, lazily allocated
+    double* partials = nullptr;  // FP64 total: per-block sums, then the total
+    double* host_total = nullptr; // pinned
+    int blocks = 0;
+    std::uint64_t h2d = 0, d2h = 0;
+};
+
+namespace {
+
+cfdx_thermal* checked_thermal(cfdx_thermal* t) {
+    if (!t || !t->flow) throw std::invalid_argument("null cfdx_thermal handle");
+    t->flow->set_device();
+    return t;
+}
+
+void release_thermal(cfdx_thermal* t) {
+    if (!t) return;
+    if (t->flow) {
+        cudaSetDevice(t->flow->cfg.device);
+        cudaStreamSynchronize(t->flow->stream);
+    }
+    device_free(t->g);
+    device_free(t->next);
+    device_free(t->scalar);
+    device_free(t->partials);
+    if (t->host_total) cudaFreeHost(t->host_total);
+    delete t;
+}
+
+float* thermal_scalar(cfdx_thermal* t) {
+    if (!t->scalar) t->scalar = static_cast<float*>(device_alloc(t->grid.cells * sizeof(float), "temperature scratch"));
+    check_cuda(launch_thermal_scalar(t->g, t->grid, t->scalar, t->flow->stream), "temperature kernel");
+    return t->scalar;
+}
+
+} // namespace
+
+CFDX_API int cfdx_thermal_create(cfdx_lbm* flow, float diffusivity, cfdx_thermal** out, char* error,
+                                 std::size_t cap) {
+    cfdx_thermal* t = nullptr;
+    const int rc = guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = nullptr;
+        checked(flow);
+        require(!flow->slab.on, "the resident thermal lattice covers whole lattices, not slabs");
+        // reference resident_multiphysics_sycl.hpp:64-66
+        require(diffusivity > 0.0F && std::isfinite(diffusivity), "invalid resident thermal lattice");
+        t = new cfdx_thermal();
+        t->flow = flow;
+        t->grid = ThermalGrid{static_cast<std::uint32_t>(flow->cfg.nx), static_cast<std::uint32_t>(flow->cfg.ny),
+                              static_cast<std::uint32_t>(flow->cfg.nz), static_cast<std::uint32_t>(flow->N)};
+        t->tau = 0.5F + 4.0F * diffusivity;
+        t->omega = 1.0F / t->tau;
+        const std::size_t bytes = 7U * flow->N * sizeof(float);
+        t->g = static_cast<float*>(device_alloc(bytes, "thermal lattice"));
+        t->next = static_cast<float*>(device_alloc(bytes, "thermal lattice"));
+        t->blocks = static_cast<int>(std::min<std::size_t>(592U, (7U * flow->N + 255U) / 256U));
+        t->partials = static_cast<double*>(device_alloc((static_cast<std::size_t>(t->blocks) + 1U) * sizeof(double),
+                                                        "thermal reduction scratch"));
+        check_cuda(cudaMallocHost(&t->host_total, sizeof(double)), "cudaMallocHost");
+        check_cuda(launch_thermal_uniform(t->g, t->grid, 0.0F, flow->stream), "thermal init kernel");
+        flow->sync();
+        *out = t;
+    });
+    if (rc != CFDX_OK) {
+        release_thermal(t);
+        copy_error(error, cap, g_error);
+    }
+    return rc;
+}
+
+CFDX_API int cfdx_thermal_destroy(cfdx_thermal* t) {
+    return guarded([&] { release_thermal(t); });
+}
+
+CFDX_API int cfdx_thermal_init_uniform(cfdx_thermal* t, float temperature) {
+    return guarded([&] {
+        checked_thermal(t);
+        require(std::isfinite(temperature), "thermal state must be finite");
+        check_cuda(launch_thermal_uniform(t->g, t->grid, temperature, t->flow->stream), "thermal init kernel");
+    });
+}
+
+CFDX_API int cfdx_thermal_init_field(cfdx_thermal* t, const float* temperature, int where) {
+    return guarded([&] {
+        checked_thermal(t);
+        require(temperature != nullptr, "null temperature field");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        const std::size_t bytes = t->grid.cells * sizeof(float);
+        const float* src = temperature;
+        if (where == CFDX_HOST) {
+            float* s = thermal_scalar(t); // scratch, overwritten below
+            check_cuda(cudaMemcpyAsync(s, temperature, bytes, cudaMemcpyHostToDevice, t->flow->stream),
+                       "cudaMemcpyAsync (temperature)");
+            t->h2d += bytes;
+            src = s;
+        }
+        check_cuda(launch_thermal_field(t->g, t->grid, src, t->flow->stream), "thermal init kernel");
+        if (where == CFDX_HOST) t->flow->sync();
+    });
+}
+
+CFDX_API int cfdx_thermal_step(cfdx_thermal* t, const float* ux, const float* uy, const float* uz,
+                               std::uint64_t count) {
+    return guarded([&] {
+        checked_thermal(t);
+        require(ux != nullptr && uy != nullptr && uz != nullptr, "null velocity field");
+        for (std::uint64_t k = 0; k < count; ++k) {
+            check_cuda(launch_thermal_step(t->g, t->next, t->grid, ux, uy, uz, t->omega, t->flow->stream),
+                       "thermal step kernel");
+            std::swap(t->g, t->next);
+        }
+    });
+}
+
+CFDX_API int cfdx_thermal_refresh_device_scalar(cfdx_thermal* t, float** temperature) {
+    return guarded([&] {
+        checked_thermal(t);
+        require(temperature != nullptr, "null output pointer");
+        *temperature = thermal_scalar(t);
+    });
+}
+
+CFDX_API int cfdx_thermal_temperature(cfdx_thermal* t, float* out, int where) {
+    return guarded([&] {
+        checked_thermal(t);
+        require(out != nullptr, "null output buffer");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        const std::size_t bytes = t->grid.cells * sizeof(float);
+        float* s = thermal_scalar(t);
+        check_cuda(cudaMemcpyAsync(out, s, bytes, where == CFDX_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                   t->flow->stream),
+                   "cudaMemcpyAsync (temperature)");
+        if (where == CFDX_HOST) t->d2h += bytes;
+        t->flow->sync();
+    });
+}
+
+CFDX_API int cfdx_thermal_add_boussinesq(cfdx_thermal* t, float* ax, float* ay, float* az, float t_ref, float beta,
+                                         float gx, float gy, float gz) {
+    return guarded([&] {
+        checked_thermal(t);
+        require(ax != nullptr && ay != nullptr && az != nullptr, "null acceleration field");
+        // reference resident_multiphysics_sycl.hpp:141-145
+        require(std::isfinite(t_ref) && std::isfinite(beta) && std::isfinite(gx) && std::isfinite(gy) &&
+                    std::isfinite(gz),
+                "invalid resident Boussinesq coupling");
+        const float* temperature = thermal_scalar(t);
+        check_cuda(launch_boussinesq(temperature, t->grid, ax, ay, az, t_ref, beta, gx, gy, gz, t->flow->stream),
+                   "Boussinesq kernel");
+    });
+}
+
+CFDX_API int cfdx_thermal_total(cfdx_thermal* t, double* total) {
+    return guarded([&] {
+        checked_thermal(t);
+        require(total != nullptr, "null output");
+        double* out = t->partials + t->blocks;
+        check_cuda(launch_thermal_total(t->g, t->grid, t->partials, t->blocks, out, t->flow->stream),
+                   "thermal total kernel");
+        check_cuda(cudaMemcpyAsync(t->host_total, out, sizeof(double), cudaMemcpyDeviceToHost, t->flow->stream),
+                   "cudaMemcpyAsync (thermal total)");
+        t->flow->sync();
+        *total = *t->host_total;
+    });
+}
+
+CFDX_API int cfdx_thermal_info(cfdx_thermal* t, std::size_t* resident_bytes, std::uint64_t* host_to_device,
+                               std::uint64_t* device_to_host) {
+    return guarded([&] {
+        require(t != nullptr && resident_bytes && host_to_device && device_to_host, "null handle or output");
+        *resident_bytes = 14U * static_cast<std::size_t>(t->grid.cells) * sizeof(float) +
+                          (t->scalar ? t->grid.cells * sizeof(float) : 0U) +
+                          (static_cast<std::size_t>(t->blocks) + 1U) * sizeof(double);
+        *host_to_device = t->h2d;
+        *device_to_host = t->d2h;
     });
 }
 

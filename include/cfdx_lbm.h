@@ -432,6 +432,39 @@ CFDX_API int cfdx_q_criterion(const double* velocity, size_t nx, size_t ny, size
  * Whole lattices only (a slab's edge planes need the neighbours' velocities). */
 CFDX_API int cfdx_lbm_q_criterion(cfdx_lbm* lbm, double dx, double dy, double dz, double* q, int where);
 
+/* ---- Resident D3Q7 temperature lattice coupled to a flow handle (reference
+ * ResidentThermalD3Q7Sycl, resident_multiphysics_sycl.hpp:51-200): a two-grid
+ * BGK advection-diffusion lattice (c_s^2 = 1/4, tau = 1/2 + 4 D) on the flow's
+ * grid, device and stream, driven by the flow's device velocity
+ * (cfdx_lbm_refresh_device_macroscopic) and adding Boussinesq buoyancy into
+ * the flow's device acceleration field (cfdx_lbm_device_local_acceleration):
+ * no field passes through the host while coupled.  Whole lattices only;
+ * destroy it before its flow handle.  Every call is ordered on the flow's
+ * stream. */
+typedef struct cfdx_thermal cfdx_thermal;
+
+/* Reference constructor (resident_multiphysics_sycl.hpp:62-71); starts at T = 0. */
+CFDX_API int cfdx_thermal_create(cfdx_lbm* flow, float diffusivity, cfdx_thermal** out, char* error,
+                                 size_t error_capacity);
+CFDX_API int cfdx_thermal_destroy(cfdx_thermal* thermal);
+/* Reference initialize_uniform (:84-92); init_field sets a per-cell temperature (N floats). */
+CFDX_API int cfdx_thermal_init_uniform(cfdx_thermal* thermal, float temperature);
+CFDX_API int cfdx_thermal_init_field(cfdx_thermal* thermal, const float* temperature, int where);
+/* Reference step(flow view, count) (:94-130): `count` steps with the device velocity ux/uy/uz. */
+CFDX_API int cfdx_thermal_step(cfdx_thermal* thermal, const float* ux, const float* uy, const float* uz,
+                               uint64_t count);
+/* Reference refresh_device_scalar (:132-139): device pointer to the temperature (owned by the lattice). */
+CFDX_API int cfdx_thermal_refresh_device_scalar(cfdx_thermal* thermal, float** temperature);
+CFDX_API int cfdx_thermal_temperature(cfdx_thermal* thermal, float* out, int where);
+/* Reference add_boussinesq_acceleration (:141-159): a += -beta (T - t_ref) g per cell (device arrays). */
+CFDX_API int cfdx_thermal_add_boussinesq(cfdx_thermal* thermal, float* ax, float* ay, float* az, float t_ref,
+                                         float beta, float gx, float gy, float gz);
+/* Reference total_scalar (:161-171), summed in FP64. */
+CFDX_API int cfdx_thermal_total(cfdx_thermal* thermal, double* total);
+/* Reference resident_bytes / transfer_stats (:173-176). */
+CFDX_API int cfdx_thermal_info(cfdx_thermal* thermal, size_t* resident_bytes, uint64_t* host_to_device,
+                               uint64_t* device_to_host);
+
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */

@@ -300,6 +300,32 @@ def q_criterion(velocity, nx: int, ny: int, nz: int, dx: float = 1.0, dy: float 
     return q.reshape(-1)
 
 
+def thermal_d3q7_step(g, u, nx: int, ny: int, nz: int, diffusivity: float, steps: int = 1):
+    """The reference's resident D3Q7 thermal step (resident_multiphysics_sycl.hpp:94-130) restated in
+    float32 numpy, operand for operand: pull from the periodic neighbours, T = sum in direction order,
+    geq = (w T)(1 + 4 c.u) with c.u = (cx ux + cy uy) + cz uz, out = g - omega (g - geq),
+    tau = 0.5 + 4 D, omega = 1 / tau.  g is [7][nz][ny][nx], u = (ux, uy, uz) per cell."""
+    f32 = np.float32
+    cx, cy, cz = [0, 1, -1, 0, 0, 0, 0], [0, 0, 0, 1, -1, 0, 0], [0, 0, 0, 0, 0, 1, -1]
+    w = [f32(0.25)] + [f32(0.125)] * 6
+    tau = f32(f32(0.5) + f32(f32(4.0) * f32(diffusivity)))
+    omega = f32(f32(1.0) / tau)
+    g = np.asarray(g, f32).reshape(7, nz, ny, nx).copy()
+    ux, uy, uz = (np.asarray(c, f32).reshape(nz, ny, nx) for c in u)
+    for _ in range(steps):
+        local = [np.roll(g[d], shift=(cz[d], cy[d], cx[d]), axis=(0, 1, 2)) for d in range(7)]
+        t = np.zeros((nz, ny, nx), f32)
+        for d in range(7):
+            t = t + local[d]
+        out = np.empty_like(g)
+        for d in range(7):
+            cu = (f32(cx[d]) * ux + f32(cy[d]) * uy) + f32(cz[d]) * uz
+            geq = (w[d] * t) * (f32(1.0) + f32(4.0) * cu)
+            out[d] = local[d] - omega * (local[d] - geq)
+        g = out
+    return g.reshape(-1)
+
+
 def f32_to_f16_bits(v: float) -> int:
     return int(oracle_lib().ora_f32_to_f16(v))
 
