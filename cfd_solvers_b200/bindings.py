@@ -131,6 +131,7 @@ SIGNATURES = {
     "cfdx_lbm_set_wall_velocity": (_i, [_H, _i, _f, _f, _f]),
     "cfdx_lbm_set_local_acceleration": (_i, [_H, _vp, _i]),
     "cfdx_lbm_device_local_acceleration": (_i, [_H, ctypes.POINTER(_vp)]),
+    "cfdx_lbm_clear_device_acceleration": (_i, [_H]),
     "cfdx_lbm_set_solid_fraction": (_i, [_H, _vp, _i]),
     "cfdx_lbm_set_storage_scale": (_i, [_H, _vp]),
     "cfdx_lbm_step": (_i, [_H, ctypes.c_uint64]),

@@ -898,6 +898,15 @@ CFDX_API int cfdx_lbm_device_local_acceleration(cfdx_lbm* h, float** accel) {
     });
 }
 
+CFDX_API int cfdx_lbm_clear_device_acceleration(cfdx_lbm* h) {
+    return guarded([&] {
+        checked(h);
+        if (!h->local_a) return;
+        h->adj.ready = false;
+        check_cuda(cudaMemsetAsync(h->local_a, 0, 3U * h->N * sizeof(float), h->stream), "cudaMemsetAsync");
+    });
+}
+
 CFDX_API int cfdx_lbm_set_solid_fraction(cfdx_lbm* h, const float* ns, int where) {
     return guarded([&] {
         checked(h);

@@ -327,7 +327,7 @@ class EsotericPullCudaSolver:
         p = ctypes.c_void_p()
         self._call("cfdx_lbm_device_local_acceleration", ctypes.byref(p))
         if clear:
-            self.set_local_body_acceleration(*(np.zeros(self._cells, np.float32) for _ in range(3)))
+            self._call("cfdx_lbm_clear_device_acceleration")  # a device memset, no host transfer
         self._has_local = True
         base = p.value
         step = 4 * self._cells

@@ -173,6 +173,11 @@ CFDX_API int cfdx_lbm_set_local_acceleration(cfdx_lbm* lbm, const float* accel, 
  * and zeroed on first use.  Reference: device_local_acceleration, esoteric_pull_sycl.hpp:349-353. */
 CFDX_API int cfdx_lbm_device_local_acceleration(cfdx_lbm* lbm, float** accel);
 
+/* Zeroes the per-cell acceleration buffer on the device, ordered on the
+ * handle's stream (no host transfer; nothing when there is no buffer).
+ * Reference: clear_local_body_acceleration, esoteric_pull_sycl.hpp:355-358 (a queue memset). */
+CFDX_API int cfdx_lbm_clear_device_acceleration(cfdx_lbm* lbm);
+
 /* Gray-LBM solid fraction n_s per cell (N floats in [0,1), host or device);
  * NULL clears.  Partial bounce-back f_i <- (1-n_s) f_i* + n_s f_opp(i).
  * No reference counterpart (Walsh, Burwinkle & Saar 2009). */

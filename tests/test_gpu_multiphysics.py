@@ -71,6 +71,11 @@ def test_reference_resident_chain(engine):
             assert th.resident_bytes() >= 14 * nx * ny * nz * 4
             f0 = flow.transfer_stats()
             flow.step(2)
+            for _ in range(3):  # the coupled loop: velocity view, thermal step, cleared force, buoyancy, flow step
+                th.step(flow.refresh_device_macroscopic(), 1)
+                force = flow.device_local_acceleration(clear=True)
+                th.add_boussinesq_acceleration(force, 300.0, 3.0e-3, (0.0, -1.0, 0.0))
+                flow.step(1)
             flow.wait()
             f1 = flow.transfer_stats()
             assert (f1.host_to_device_bytes, f1.device_to_host_bytes) == (f0.host_to_device_bytes,
