@@ -615,6 +615,83 @@ def q_criterion_measure(torch, cs, n, device, cpu_sample=True):
     return res
 
 
+def resident_coupling_measure(torch, cs, n, device, particles=1 << 20, reps=5):
+    """One resident coupling cycle on the n^3 cavity, every kernel on the flow's stream and timed
+    there with CUDA events (best of `reps`): the device macroscopic view, a D3Q7 thermal step,
+    the cleared acceleration and Boussinesq term, a free-surface advection, its geometry and
+    surface tension, a two-way particle push and the FP32 Q-criterion; then one flow step that
+    consumes the acceleration.  Achieved GB/s use the algorithmic bytes per cell of each kernel
+    (thermal 68, advection 20, geometry + tension 64, Q 16)."""
+    from cfd_solvers_b200.multiphysics import (ImmersedBoundaryParticle, ParticleVector3, ResidentFlowDiagnostics3D,
+                                               ResidentFreeSurface3D, ResidentParticles3D, ResidentThermalD3Q7)
+
+    s = make_cavity(cs, n, device=device)
+    cells = n ** 3
+    res = {"grid": f"{n}^3", "particles": particles}
+    try:
+        setup_cavity(s, cs, n)
+        s.step(10)
+        stream = torch.cuda.ExternalStream(s.stream())
+        th = ResidentThermalD3Q7(s, 0.02)
+        fs = ResidentFreeSurface3D(s)
+        diag = ResidentFlowDiagnostics3D(s)
+        parts = ResidentParticles3D(s, particles)
+        try:
+            th.initialize_uniform(300.0)
+            fs.initialize_half_space_x(n / 2 + 0.25)
+            rng = np.random.default_rng(3)
+            rec = np.zeros((particles, 8))
+            rec[:, :3] = rng.uniform(0, n, (particles, 3))
+            rec[:, 6], rec[:, 7] = 1.0, 0.5
+            parts.upload(rec)
+            macro = s.refresh_device_macroscopic()
+            force = s.device_local_acceleration(clear=True)
+            stages = {
+                "macroscopic_view": lambda: s.refresh_device_macroscopic(),
+                "thermal_step": lambda: th.step(macro, 1),
+                "clear_acceleration": lambda: s.device_local_acceleration(clear=True),
+                "boussinesq": lambda: th.add_boussinesq_acceleration(force, 300.0, 3e-3, ParticleVector3(0, -1, 0)),
+                "free_surface_advect": lambda: fs.advect(macro, 0.5),
+                "surface_tension": lambda: fs.add_surface_tension_acceleration(force, 0.072),
+                "particles_two_way": lambda: parts.advance(macro, force, 0.5, True),
+                "q_criterion_fp32": lambda: diag.q_criterion(macro),
+                "flow_step": lambda: s.step(1),
+            }
+            def moved():
+                return sum(o.transfer_stats().host_to_device_bytes + o.transfer_stats().device_to_host_bytes
+                           for o in (s, th, fs, parts))
+
+            moved0 = moved()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(stages) + 1)]
+            best = {k: float("inf") for k in stages}
+            for _ in range(reps + 1):
+                s.wait()
+                ev[0].record(stream)
+                for i, fn in enumerate(stages.values()):
+                    fn()
+                    ev[i + 1].record(stream)
+                ev[-1].synchronize()
+                for i, k in enumerate(stages):
+                    best[k] = min(best[k], ev[i].elapsed_time(ev[i + 1]))
+            bytes_per_cell = {"thermal_step": 68, "free_surface_advect": 20, "surface_tension": 64,
+                              "q_criterion_fp32": 16}
+            peak = hbm_peak()[0]
+            res["ms"] = best
+            res["cycle_ms"] = sum(best.values())
+            res["achieved_gbs"] = {k: bytes_per_cell[k] * cells / (best[k] / 1e3) / 1e9 for k in bytes_per_cell}
+            res["roofline_frac"] = {k: v / peak for k, v in res["achieved_gbs"].items()}
+            res["mparticles_per_s"] = particles / (best["particles_two_way"] / 1e3) / 1e6
+            res["host_transfer_bytes_in_cycles"] = moved() - moved0
+            res["note"] = ("all kernels on the flow's stream through its device views; host bytes counted by the "
+                           "C ABI over all timed cycles")
+        finally:
+            for o in (parts, diag, fs, th):
+                o.close()
+    finally:
+        s.close()
+    return res
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -883,6 +960,7 @@ def main(argv=None):
             variants["voxelizer"] = voxelizer_measure(torch, local_rank, n, cpu_sample=not args.no_cpu_baseline)
             variants["q_criterion"] = q_criterion_measure(torch, cs, n, local_rank,
                                                           cpu_sample=not args.no_cpu_baseline)
+            variants["resident_coupling"] = resident_coupling_measure(torch, cs, n, local_rank)
         if not args.no_differentiation:
             variants["differentiation"] = differentiation_variants(torch, cs, local_rank)
         if not args.no_precision:

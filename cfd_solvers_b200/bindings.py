@@ -181,6 +181,31 @@ SIGNATURES = {
     "cfdx_thermal_total": (_i, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "cfdx_thermal_info": (_i, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(ctypes.c_uint64),
                                ctypes.POINTER(ctypes.c_uint64)]),
+    "cfdx_surface_create": (_i, [_H, ctypes.POINTER(_vp), ctypes.c_char_p, _sz]),
+    "cfdx_surface_destroy": (_i, [_vp]),
+    "cfdx_surface_init_uniform": (_i, [_vp, ctypes.c_float]),
+    "cfdx_surface_init_half_space_x": (_i, [_vp, ctypes.c_float]),
+    "cfdx_surface_init_field": (_i, [_vp, _vp, _i]),
+    "cfdx_surface_advect": (_i, [_vp, _vp, _vp, _vp, ctypes.c_float]),
+    "cfdx_surface_device_fill": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "cfdx_surface_refresh_geometry": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "cfdx_surface_add_tension": (_i, [_vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float]),
+    "cfdx_surface_volume": (_i, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "cfdx_surface_fill": (_i, [_vp, _vp, _i, _i]),
+    "cfdx_surface_info": (_i, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(ctypes.c_uint64),
+                               ctypes.POINTER(ctypes.c_uint64)]),
+    "cfdx_particles_create": (_i, [_H, _sz, ctypes.POINTER(_vp), ctypes.c_char_p, _sz]),
+    "cfdx_particles_destroy": (_i, [_vp]),
+    "cfdx_particles_upload": (_i, [_vp, _vp, _sz]),
+    "cfdx_particles_download": (_i, [_vp, _vp, _sz]),
+    "cfdx_particles_device_state": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "cfdx_particles_advance": (_i, [_vp] + [_vp] * 6 + [ctypes.c_float, _i] + [ctypes.c_float] * 3),
+    "cfdx_particles_info": (_i, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(ctypes.c_uint64),
+                                 ctypes.POINTER(ctypes.c_uint64)]),
+    "cfdx_diagnostics_create": (_i, [_H, ctypes.POINTER(_vp), ctypes.c_char_p, _sz]),
+    "cfdx_diagnostics_destroy": (_i, [_vp]),
+    "cfdx_diagnostics_q_criterion": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
+    "cfdx_diagnostics_info": (_i, [_vp, ctypes.POINTER(_sz)]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

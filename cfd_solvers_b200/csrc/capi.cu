@@ -25,6 +25,7 @@
 #include "lbm_launch.h"
 #include "voxelize.h"
 #include "export.h"
+#include "resident.h"
 #include "thermal.h"
 
 namespace {
@@ -1926,6 +1927,9 @@ CFDX_API int cfdx_lbm_q_criterion(cfdx_lbm* h, double dx, double dy, double dz, 
 }
 
 // ------------------------------------------------- resident thermal lattice
+// The resident solvers index cells with 32-bit integers.
+constexpr std::size_t kResidentMaxCells = 0xFFFF0000ULL;
+
 struct cfdx_thermal {
     cfdx_lbm* flow = nullptr; // borrowed: its device and stream
     ThermalGrid grid{};
@@ -1979,6 +1983,7 @@ CFDX_API int cfdx_thermal_create(cfdx_lbm* flow, float diffusivity, cfdx_thermal
         require(!flow->slab.on, "the resident thermal lattice covers whole lattices, not slabs");
         // reference resident_multiphysics_sycl.hpp:64-66
         require(diffusivity > 0.0F && std::isfinite(diffusivity), "invalid resident thermal lattice");
+        require(flow->N <= kResidentMaxCells, "resident thermal lattices hold at most 2^32 - 2^16 cells");
         t = new cfdx_thermal();
         t->flow = flow;
         t->grid = ThermalGrid{static_cast<std::uint32_t>(flow->cfg.nx), static_cast<std::uint32_t>(flow->cfg.ny),
@@ -2108,6 +2113,400 @@ CFDX_API int cfdx_thermal_info(cfdx_thermal* t, std::size_t* resident_bytes, std
                           (static_cast<std::size_t>(t->blocks) + 1U) * sizeof(double);
         *host_to_device = t->h2d;
         *device_to_host = t->d2h;
+    });
+}
+
+// ------------------------------------------------- resident free surface
+struct cfdx_surface {
+    cfdx_lbm* flow = nullptr; // borrowed: its device and stream
+    ThermalGrid grid{};
+    float* fill = nullptr;
+    float* next = nullptr;
+    float* geometry = nullptr;   // normals x | y | z | curvature
+    double* partials = nullptr;  // FP64 volume: per-block sums, then the total
+    double* host_total = nullptr; // pinned
+    int blocks = 0;
+    std::uint64_t h2d = 0, d2h = 0;
+};
+
+// ------------------------------------------------- resident particles
+struct cfdx_particles {
+    cfdx_lbm* flow = nullptr;
+    ThermalGrid grid{};
+    std::uint32_t count = 0;
+    float* state = nullptr; // x | y | z | vx | vy | vz | mass | response, count floats each
+    std::uint64_t h2d = 0, d2h = 0;
+};
+
+// ------------------------------------------------- resident diagnostics
+struct cfdx_diagnostics {
+    cfdx_lbm* flow = nullptr;
+    ThermalGrid grid{};
+    float* q = nullptr;
+};
+
+extern "C++" {
+namespace {
+
+// the resident solvers cover whole lattices of at least `minimum` cells per axis
+ThermalGrid resident_grid(cfdx_lbm* flow, std::size_t minimum, const char* what) {
+    checked(flow);
+    require(!flow->slab.on, (std::string(what) + " covers whole lattices, not slabs").c_str());
+    require(flow->cfg.nx >= minimum && flow->cfg.ny >= minimum && flow->cfg.nz >= minimum,
+            (std::string("invalid ") + what + " lattice").c_str());
+    require(flow->N <= kResidentMaxCells, (std::string(what) + " lattices hold at most 2^32 - 2^16 cells").c_str());
+    return ThermalGrid{static_cast<std::uint32_t>(flow->cfg.nx), static_cast<std::uint32_t>(flow->cfg.ny),
+                       static_cast<std::uint32_t>(flow->cfg.nz), static_cast<std::uint32_t>(flow->N)};
+}
+
+template <class H> H* checked_resident(H* h, const char* what) {
+    if (!h || !h->flow) throw std::invalid_argument(std::string("null ") + what + " handle");
+    h->flow->set_device();
+    return h;
+}
+
+template <class H> void sync_flow(H* h) {
+    if (h && h->flow) {
+        cudaSetDevice(h->flow->cfg.device);
+        cudaStreamSynchronize(h->flow->stream);
+    }
+}
+
+void release_surface(cfdx_surface* s) {
+    if (!s) return;
+    sync_flow(s);
+    device_free(s->fill);
+    device_free(s->next);
+    device_free(s->geometry);
+    device_free(s->partials);
+    if (s->host_total) cudaFreeHost(s->host_total);
+    delete s;
+}
+
+void release_particles(cfdx_particles* p) {
+    if (!p) return;
+    sync_flow(p);
+    device_free(p->state);
+    delete p;
+}
+
+void release_diagnostics(cfdx_diagnostics* d) {
+    if (!d) return;
+    sync_flow(d);
+    device_free(d->q);
+    delete d;
+}
+
+void require_velocity(const float* ux, const float* uy, const float* uz) {
+    require(ux != nullptr && uy != nullptr && uz != nullptr, "null velocity field");
+}
+
+void require_acceleration(const float* ax, const float* ay, const float* az) {
+    require(ax != nullptr && ay != nullptr && az != nullptr, "null acceleration field");
+}
+
+// normals and curvature of the current fill (reference resident_multiphysics_sycl.hpp:269-298)
+void surface_geometry(cfdx_surface* s) {
+    check_cuda(launch_fill_geometry(s->fill, s->geometry, s->grid, s->flow->stream), "free-surface geometry kernel");
+}
+
+} // namespace
+} // extern "C++"
+
+CFDX_API int cfdx_surface_create(cfdx_lbm* flow, cfdx_surface** out, char* error, std::size_t cap) {
+    cfdx_surface* s = nullptr;
+    const int rc = guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = nullptr;
+        // reference resident_multiphysics_sycl.hpp:204-206
+        const ThermalGrid grid = resident_grid(flow, 2U, "resident free-surface");
+        s = new cfdx_surface();
+        s->flow = flow;
+        s->grid = grid;
+        const std::size_t bytes = flow->N * sizeof(float);
+        s->fill = static_cast<float*>(device_alloc(bytes, "free-surface fill"));
+        s->next = static_cast<float*>(device_alloc(bytes, "free-surface fill"));
+        s->geometry = static_cast<float*>(device_alloc(4U * bytes, "free-surface geometry"));
+        s->blocks = static_cast<int>(std::min<std::size_t>(592U, (flow->N + 255U) / 256U));
+        s->partials = static_cast<double*>(device_alloc((static_cast<std::size_t>(s->blocks) + 1U) * sizeof(double),
+                                                        "free-surface reduction scratch"));
+        check_cuda(cudaMallocHost(&s->host_total, sizeof(double)), "cudaMallocHost");
+        check_cuda(launch_fill_uniform(s->fill, s->grid, 0.0F, flow->stream), "free-surface init kernel");
+        flow->sync();
+        *out = s;
+    });
+    if (rc != CFDX_OK) {
+        release_surface(s);
+        copy_error(error, cap, g_error);
+    }
+    return rc;
+}
+
+CFDX_API int cfdx_surface_destroy(cfdx_surface* s) {
+    return guarded([&] { release_surface(s); });
+}
+
+CFDX_API int cfdx_surface_init_uniform(cfdx_surface* s, float fill) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        // reference resident_multiphysics_sycl.hpp:223-224
+        require(fill >= 0.0F && fill <= 1.0F, "free-surface fill must be in [0,1]");
+        check_cuda(launch_fill_uniform(s->fill, s->grid, fill, s->flow->stream), "free-surface init kernel");
+    });
+}
+
+CFDX_API int cfdx_surface_init_half_space_x(cfdx_surface* s, float interface_x) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        require(std::isfinite(interface_x), "invalid free-surface interface position");
+        check_cuda(launch_fill_half_space_x(s->fill, s->grid, interface_x, s->flow->stream),
+                   "free-surface init kernel");
+    });
+}
+
+CFDX_API int cfdx_surface_init_field(cfdx_surface* s, const float* fill, int where) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        require(fill != nullptr, "null fill field");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        const std::size_t bytes = s->grid.cells * sizeof(float);
+        if (where == CFDX_HOST) {
+            for (std::size_t n = 0; n < s->grid.cells; ++n)
+                require(fill[n] >= 0.0F && fill[n] <= 1.0F, "free-surface fill must be in [0,1]");
+            s->h2d += bytes;
+        }
+        check_cuda(cudaMemcpyAsync(s->fill, fill, bytes,
+                                   where == CFDX_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                   s->flow->stream),
+                   "cudaMemcpyAsync (fill)");
+        if (where == CFDX_HOST) s->flow->sync();
+    });
+}
+
+CFDX_API int cfdx_surface_advect(cfdx_surface* s, const float* ux, const float* uy, const float* uz, float dt) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        require_velocity(ux, uy, uz);
+        // reference resident_multiphysics_sycl.hpp:238-239
+        require(dt > 0.0F, "invalid resident free-surface advection");
+        check_cuda(launch_fill_advect(s->fill, s->next, s->grid, ux, uy, uz, dt, s->flow->stream),
+                   "free-surface advection kernel");
+        std::swap(s->fill, s->next);
+    });
+}
+
+CFDX_API int cfdx_surface_device_fill(cfdx_surface* s, float** fill) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        require(fill != nullptr, "null output pointer");
+        *fill = s->fill;
+    });
+}
+
+CFDX_API int cfdx_surface_refresh_geometry(cfdx_surface* s, float** geometry) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        surface_geometry(s);
+        if (geometry) *geometry = s->geometry;
+    });
+}
+
+CFDX_API int cfdx_surface_add_tension(cfdx_surface* s, float* ax, float* ay, float* az, float surface_tension,
+                                      float density) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        require_acceleration(ax, ay, az);
+        // reference resident_multiphysics_sycl.hpp:302-304
+        require(surface_tension >= 0.0F && density > 0.0F && std::isfinite(surface_tension) &&
+                    std::isfinite(density),
+                "invalid resident surface-tension coupling");
+        surface_geometry(s);
+        check_cuda(launch_surface_tension(s->fill, s->geometry + 3U * static_cast<std::size_t>(s->grid.cells),
+                                          s->grid, ax, ay, az, surface_tension, density, s->flow->stream),
+                   "surface-tension kernel");
+    });
+}
+
+CFDX_API int cfdx_surface_volume(cfdx_surface* s, double* volume) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        require(volume != nullptr, "null output");
+        double* out = s->partials + s->blocks;
+        check_cuda(launch_sum_floats(s->fill, s->grid.cells, s->partials, s->blocks, out, s->flow->stream),
+                   "free-surface volume kernel");
+        check_cuda(cudaMemcpyAsync(s->host_total, out, sizeof(double), cudaMemcpyDeviceToHost, s->flow->stream),
+                   "cudaMemcpyAsync (volume)");
+        s->flow->sync();
+        *volume = *s->host_total;
+    });
+}
+
+CFDX_API int cfdx_surface_fill(cfdx_surface* s, float* out, int which, int where) {
+    return guarded([&] {
+        checked_resident(s, "cfdx_surface");
+        require(out != nullptr, "null output buffer");
+        require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
+        require(which >= 0 && which <= 4, "which must be 0 (fill) or 1-4 (normal x, y, z, curvature)");
+        const std::size_t bytes = s->grid.cells * sizeof(float);
+        const float* src = which == 0 ? s->fill : s->geometry + (static_cast<std::size_t>(which) - 1U) * s->grid.cells;
+        check_cuda(cudaMemcpyAsync(out, src, bytes, where == CFDX_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                   s->flow->stream),
+                   "cudaMemcpyAsync (fill)");
+        if (where == CFDX_HOST) s->d2h += bytes;
+        s->flow->sync();
+    });
+}
+
+CFDX_API int cfdx_surface_info(cfdx_surface* s, std::size_t* resident_bytes, std::uint64_t* host_to_device,
+                               std::uint64_t* device_to_host) {
+    return guarded([&] {
+        require(s != nullptr && resident_bytes && host_to_device && device_to_host, "null handle or output");
+        *resident_bytes = 6U * static_cast<std::size_t>(s->grid.cells) * sizeof(float) +
+                          (static_cast<std::size_t>(s->blocks) + 1U) * sizeof(double);
+        *host_to_device = s->h2d;
+        *device_to_host = s->d2h;
+    });
+}
+
+CFDX_API int cfdx_particles_create(cfdx_lbm* flow, std::size_t count, cfdx_particles** out, char* error,
+                                   std::size_t cap) {
+    cfdx_particles* p = nullptr;
+    const int rc = guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = nullptr;
+        // reference resident_multiphysics_sycl.hpp:326-329
+        const ThermalGrid grid = resident_grid(flow, 2U, "resident particle");
+        require(count <= (std::size_t{1} << 28), "too many resident particles");
+        p = new cfdx_particles();
+        p->flow = flow;
+        p->grid = grid;
+        p->count = static_cast<std::uint32_t>(count);
+        if (count) p->state = static_cast<float*>(device_alloc(8U * count * sizeof(float), "particle state"));
+        *out = p;
+    });
+    if (rc != CFDX_OK) {
+        release_particles(p);
+        copy_error(error, cap, g_error);
+    }
+    return rc;
+}
+
+CFDX_API int cfdx_particles_destroy(cfdx_particles* p) {
+    return guarded([&] { release_particles(p); });
+}
+
+CFDX_API int cfdx_particles_upload(cfdx_particles* p, const double* particles, std::size_t count) {
+    return guarded([&] {
+        checked_resident(p, "cfdx_particles");
+        // reference resident_multiphysics_sycl.hpp:337-344
+        require(count == p->count, "resident particle count mismatch");
+        require(particles != nullptr || count == 0U, "null particle array");
+        std::vector<float> host(8U * count);
+        for (std::size_t i = 0; i < count; ++i) {
+            const double* q = particles + 8U * i;
+            require(q[6] > 0.0 && q[7] > 0.0, "particle mass and response time must be positive");
+            for (std::size_t k = 0; k < 8U; ++k) host[k * count + i] = static_cast<float>(q[k]);
+        }
+        if (count) {
+            check_cuda(cudaMemcpyAsync(p->state, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                       p->flow->stream),
+                       "cudaMemcpyAsync (particles)");
+            p->flow->sync();
+            p->h2d += host.size() * sizeof(float);
+        }
+    });
+}
+
+CFDX_API int cfdx_particles_download(cfdx_particles* p, double* particles, std::size_t count) {
+    return guarded([&] {
+        checked_resident(p, "cfdx_particles");
+        require(count == p->count, "resident particle count mismatch");
+        require(particles != nullptr || count == 0U, "null particle array");
+        std::vector<float> host(8U * count);
+        if (count) {
+            check_cuda(cudaMemcpyAsync(host.data(), p->state, host.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                       p->flow->stream),
+                       "cudaMemcpyAsync (particles)");
+            p->flow->sync();
+            p->d2h += host.size() * sizeof(float);
+        }
+        for (std::size_t i = 0; i < count; ++i)
+            for (std::size_t k = 0; k < 8U; ++k) particles[8U * i + k] = static_cast<double>(host[k * count + i]);
+    });
+}
+
+CFDX_API int cfdx_particles_device_state(cfdx_particles* p, float** state) {
+    return guarded([&] {
+        checked_resident(p, "cfdx_particles");
+        require(state != nullptr, "null output pointer");
+        *state = p->state;
+    });
+}
+
+CFDX_API int cfdx_particles_advance(cfdx_particles* p, const float* ux, const float* uy, const float* uz, float* ax,
+                                    float* ay, float* az, float dt, int two_way, float gx, float gy, float gz) {
+    return guarded([&] {
+        checked_resident(p, "cfdx_particles");
+        require_velocity(ux, uy, uz);
+        if (two_way) require_acceleration(ax, ay, az);
+        // reference resident_multiphysics_sycl.hpp:351-352
+        require(dt > 0.0F && std::isfinite(dt), "invalid resident particle coupling");
+        require(std::isfinite(gx) && std::isfinite(gy) && std::isfinite(gz), "invalid resident particle gravity");
+        check_cuda(launch_particles_advance(p->state, p->count, p->grid, ux, uy, uz, ax, ay, az, dt, two_way != 0, gx,
+                                            gy, gz, p->flow->stream),
+                   "particle kernel");
+    });
+}
+
+CFDX_API int cfdx_particles_info(cfdx_particles* p, std::size_t* resident_bytes, std::uint64_t* host_to_device,
+                                 std::uint64_t* device_to_host) {
+    return guarded([&] {
+        require(p != nullptr && resident_bytes && host_to_device && device_to_host, "null handle or output");
+        *resident_bytes = 8U * static_cast<std::size_t>(p->count) * sizeof(float);
+        *host_to_device = p->h2d;
+        *device_to_host = p->d2h;
+    });
+}
+
+CFDX_API int cfdx_diagnostics_create(cfdx_lbm* flow, cfdx_diagnostics** out, char* error, std::size_t cap) {
+    cfdx_diagnostics* d = nullptr;
+    const int rc = guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = nullptr;
+        // reference resident_multiphysics_sycl.hpp:389-392
+        const ThermalGrid grid = resident_grid(flow, 3U, "Q-criterion (at least 3x3x3)");
+        d = new cfdx_diagnostics();
+        d->flow = flow;
+        d->grid = grid;
+        d->q = static_cast<float*>(device_alloc(flow->N * sizeof(float), "Q-criterion field"));
+        *out = d;
+    });
+    if (rc != CFDX_OK) {
+        release_diagnostics(d);
+        copy_error(error, cap, g_error);
+    }
+    return rc;
+}
+
+CFDX_API int cfdx_diagnostics_destroy(cfdx_diagnostics* d) {
+    return guarded([&] { release_diagnostics(d); });
+}
+
+CFDX_API int cfdx_diagnostics_q_criterion(cfdx_diagnostics* d, const float* ux, const float* uy, const float* uz,
+                                          float** q) {
+    return guarded([&] {
+        checked_resident(d, "cfdx_diagnostics");
+        require_velocity(ux, uy, uz);
+        require(q != nullptr, "null output pointer");
+        check_cuda(launch_resident_q(ux, uy, uz, d->grid, d->q, d->flow->stream), "Q-criterion kernel");
+        *q = d->q;
+    });
+}
+
+CFDX_API int cfdx_diagnostics_info(cfdx_diagnostics* d, std::size_t* resident_bytes) {
+    return guarded([&] {
+        require(d != nullptr && resident_bytes != nullptr, "null handle or output");
+        *resident_bytes = static_cast<std::size_t>(d->grid.cells) * sizeof(float);
     });
 }
 

@@ -74,6 +74,15 @@ struct MacroscopicFields {
     std::vector<float> uz;
 };
 
+// Host-transfer counters (reference cfd::core::DeviceTransferStats, core/device_residency.hpp:11-42).
+struct TransferStats {
+    std::uint64_t host_to_device_bytes{0};
+    std::uint64_t device_to_host_bytes{0};
+    [[nodiscard]] std::uint64_t host_transfer_bytes() const noexcept {
+        return host_to_device_bytes + device_to_host_bytes;
+    }
+};
+
 // Converts a C ABI status into the reference's exception types.
 inline void check(int status, const char* what) {
     if (status == CFDX_OK) return;
@@ -175,7 +184,7 @@ public:
     EsotericPullCudaSolver& operator=(const EsotericPullCudaSolver&) = delete;
     EsotericPullCudaSolver(EsotericPullCudaSolver&& other) noexcept
         : handle_(std::exchange(other.handle_, nullptr)), config_(other.config_), cells_(other.cells_),
-          mask_(std::move(other.mask_)), local_(other.local_) {}
+          mask_(std::move(other.mask_)), local_(other.local_), transfer_base_(other.transfer_base_) {}
 
     // ------------------------------------------------ reference API (CPU class)
     void initialize_uniform(float rho = 1.0F, float ux = 0.0F, float uy = 0.0F, float uz = 0.0F) {
@@ -248,6 +257,48 @@ public:
     [[nodiscard]] std::size_t resident_bytes() const { return info().resident_bytes; }
     [[nodiscard]] std::string device_name() const { return "CUDA device " + std::to_string(config_.device); }
 
+    // Bytes moved through the host since construction or reset_transfer_stats().
+    [[nodiscard]] cuda::TransferStats transfer_stats() const {
+        const cfdx_lbm_info i = info();
+        return {i.host_to_device_bytes - transfer_base_.host_to_device_bytes,
+                i.device_to_host_bytes - transfer_base_.device_to_host_bytes};
+    }
+    void reset_transfer_stats() {
+        const cfdx_lbm_info i = info();
+        transfer_base_ = {i.host_to_device_bytes, i.device_to_host_bytes};
+    }
+
+    // Device views for resident coupling (reference esoteric_pull_sycl.hpp:218-372):
+    // the step's macroscopic fields and the per-cell acceleration it consumes.
+    struct DeviceMacroscopicView {
+        float* rho;
+        float* ux;
+        float* uy;
+        float* uz;
+        std::size_t cells;
+    };
+    struct DeviceAccelerationView {
+        float* ax;
+        float* ay;
+        float* az;
+        std::size_t cells;
+    };
+    // rho and u + a/2 of the current state in device memory owned by the solver.
+    [[nodiscard]] DeviceMacroscopicView refresh_device_macroscopic() {
+        DeviceMacroscopicView v{nullptr, nullptr, nullptr, nullptr, cells_};
+        cuda::check(cfdx_lbm_refresh_device_macroscopic(handle_, &v.rho, &v.ux, &v.uy, &v.uz),
+                    "refresh_device_macroscopic");
+        return v;
+    }
+    // The per-cell acceleration the step reads (zeroed on the device with clear).
+    [[nodiscard]] DeviceAccelerationView device_local_acceleration(bool clear = false) {
+        float* a = nullptr;
+        cuda::check(cfdx_lbm_device_local_acceleration(handle_, &a), "device_local_acceleration");
+        if (clear) cuda::check(cfdx_lbm_clear_device_acceleration(handle_), "device_local_acceleration");
+        local_ = true;
+        return {a, a + cells_, a + 2U * cells_, cells_};
+    }
+
     // ------------------------------------------------------------ extensions
     // Cell flags: 0 fluid, 1 wall, 2..15 moving wall (velocity from set_wall_velocity).
     void set_flags(std::span<const std::uint8_t> flags) {
@@ -315,6 +366,7 @@ private:
     std::size_t cells_{0};
     std::vector<std::uint8_t> mask_;
     bool local_{false};
+    cuda::TransferStats transfer_base_{};
 };
 
 // One z-slab of a lattice cut along z (the reference's DistributedPullBlock

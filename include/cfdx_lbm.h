@@ -470,6 +470,86 @@ CFDX_API int cfdx_thermal_total(cfdx_thermal* thermal, double* total);
 CFDX_API int cfdx_thermal_info(cfdx_thermal* thermal, size_t* resident_bytes, uint64_t* host_to_device,
                                uint64_t* device_to_host);
 
+/* ---- Resident free surface (reference ResidentFreeSurfaceSycl3D,
+ * resident_multiphysics_sycl.hpp:202-318): a fill fraction in [0, 1] per
+ * cell, advected by the flow's device velocity with first-order upwind face
+ * fluxes (face velocity = mean of the two cells) and clamped, its normals and
+ * curvature from central differences, and the surface-tension acceleration
+ * sigma * kappa * grad(fill) / rho added into the flow's device acceleration.
+ * Periodic in every axis; whole lattices with nx, ny, nz >= 2; ordered on the
+ * flow's stream; destroy it before its flow handle. */
+typedef struct cfdx_surface cfdx_surface;
+
+/* Reference constructor (:204-212); starts empty (fill 0). */
+CFDX_API int cfdx_surface_create(cfdx_lbm* flow, cfdx_surface** out, char* error, size_t error_capacity);
+CFDX_API int cfdx_surface_destroy(cfdx_surface* surface);
+/* Reference initialize_uniform (:222-226): fill in [0, 1] else CFDX_ERR_INVALID. */
+CFDX_API int cfdx_surface_init_uniform(cfdx_surface* surface, float fill);
+/* Reference initialize_half_space_x (:227-236): the fraction of each cell left of x = interface_x. */
+CFDX_API int cfdx_surface_init_half_space_x(cfdx_surface* surface, float interface_x);
+/* A per-cell fill (N floats, host values checked to lie in [0, 1]). */
+CFDX_API int cfdx_surface_init_field(cfdx_surface* surface, const float* fill, int where);
+/* Reference advect(flow view, dt) (:238-264): one upwind step with the device velocity; dt > 0. */
+CFDX_API int cfdx_surface_advect(cfdx_surface* surface, const float* ux, const float* uy, const float* uz,
+                                 float dt);
+/* Reference fill_device (:266-267): device pointer to the current fill (valid until the next advect). */
+CFDX_API int cfdx_surface_device_fill(cfdx_surface* surface, float** fill);
+/* Reference refresh_geometry (:269-298): normals (0 where |grad| <= 1e-12) and
+ * curvature -div(n)/2; *geometry (may be NULL) = device [normal x | y | z | curvature], 4 N floats. */
+CFDX_API int cfdx_surface_refresh_geometry(cfdx_surface* surface, float** geometry);
+/* Reference add_surface_tension_acceleration (:300-318): refreshes the geometry,
+ * then a += sigma * kappa / rho * grad(fill); sigma >= 0, rho > 0. */
+CFDX_API int cfdx_surface_add_tension(cfdx_surface* surface, float* ax, float* ay, float* az, float surface_tension,
+                                      float density);
+/* Reference volume (:322-327): the sum of the fill (in FP64 here; the reference sums in FP32). */
+CFDX_API int cfdx_surface_volume(cfdx_surface* surface, double* volume);
+/* Copy out the fill (which 0) or a geometry component (1-3 normal x/y/z, 4 curvature). */
+CFDX_API int cfdx_surface_fill(cfdx_surface* surface, float* out, int which, int where);
+CFDX_API int cfdx_surface_info(cfdx_surface* surface, size_t* resident_bytes, uint64_t* host_to_device,
+                               uint64_t* device_to_host);
+
+/* ---- Resident point particles (reference ResidentParticlesSycl3D,
+ * resident_multiphysics_sycl.hpp:333-382): per particle x, y, z, vx, vy, vz,
+ * mass, response time on the device.  advance() interpolates the flow's
+ * device velocity trilinearly (periodic), applies the drag m (u - v) / tau_p
+ * and gravity with an explicit Euler step, wraps the position, and with
+ * two_way != 0 spreads -drag onto the eight surrounding cells of the flow's
+ * device acceleration with atomic adds (whose order, and so the last bits of
+ * the sum where particles share a cell, is not fixed). */
+typedef struct cfdx_particles cfdx_particles;
+
+/* Reference constructor (:326-330); count may be 0. */
+CFDX_API int cfdx_particles_create(cfdx_lbm* flow, size_t count, cfdx_particles** out, char* error,
+                                   size_t error_capacity);
+CFDX_API int cfdx_particles_destroy(cfdx_particles* particles);
+/* Reference upload (:337-346): `count` records of 8 doubles laid out as the
+ * reference's ImmersedBoundaryParticle (position x y z, velocity x y z, mass,
+ * response_time; particles.hpp:13-18); mass and response time > 0. */
+CFDX_API int cfdx_particles_upload(cfdx_particles* particles, const double* records, size_t count);
+/* Reference download (:371-380): the same 8-double records. */
+CFDX_API int cfdx_particles_download(cfdx_particles* particles, double* records, size_t count);
+/* Device state, 8 planes of `count` floats (x | y | z | vx | vy | vz | mass | response). */
+CFDX_API int cfdx_particles_device_state(cfdx_particles* particles, float** state);
+/* Reference advance(flow view, force view, dt, two_way, gravity) (:348-369). */
+CFDX_API int cfdx_particles_advance(cfdx_particles* particles, const float* ux, const float* uy, const float* uz,
+                                    float* ax, float* ay, float* az, float dt, int two_way, float gx, float gy,
+                                    float gz);
+CFDX_API int cfdx_particles_info(cfdx_particles* particles, size_t* resident_bytes, uint64_t* host_to_device,
+                                 uint64_t* device_to_host);
+
+/* ---- Resident FP32 Q-criterion of a device velocity (reference
+ * ResidentFlowDiagnosticsSycl3D, resident_multiphysics_sycl.hpp:384-405):
+ * periodic central differences, Q = (|Omega|^2 - |S|^2) / 2 in FP32, into a
+ * device field owned by the handle.  Whole lattices with nx, ny, nz >= 3. */
+typedef struct cfdx_diagnostics cfdx_diagnostics;
+
+CFDX_API int cfdx_diagnostics_create(cfdx_lbm* flow, cfdx_diagnostics** out, char* error, size_t error_capacity);
+CFDX_API int cfdx_diagnostics_destroy(cfdx_diagnostics* diagnostics);
+/* *q = the device Q field (N floats, owned by the handle; overwritten by the next call). */
+CFDX_API int cfdx_diagnostics_q_criterion(cfdx_diagnostics* diagnostics, const float* ux, const float* uy,
+                                          const float* uz, float** q);
+CFDX_API int cfdx_diagnostics_info(cfdx_diagnostics* diagnostics, size_t* resident_bytes);
+
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */

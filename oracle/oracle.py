@@ -363,6 +363,10 @@ def ref_lib(fast: bool = False):
         lib.ref_bench.restype = ctypes.c_double
         lib.ref_voxelize.argtypes = [_d, sz, sz, sz, sz, _d, _d, _u8]
         lib.ref_transform_surface.argtypes = [_d, sz, _d, _d, ctypes.c_double, _d]
+        lib.ref_free_surface.argtypes = [sz, sz, sz, _d, _f, _f, _f, ctypes.c_double, sz, ctypes.c_double,
+                                         ctypes.c_double, _d, _d, _d, _d]
+        lib.ref_particles.argtypes = [sz, sz, sz, _f, _f, _f, _d, sz, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, _f]
         _ref[key] = lib
     return _ref[key]
 
@@ -385,6 +389,182 @@ def ref_transform_surface(tris, translation, axis, angle: float) -> np.ndarray:
     _check(lib, lib.ref_transform_surface(_ptr(t, _d), len(t), _ptr(tr, _d), _ptr(ax, _d), float(angle),
                                           _ptr(out, _d)))
     return out
+
+
+def ref_free_surface(fill, u, nx: int, ny: int, nz: int, dt: float, steps: int, sigma: float = 0.0,
+                     density: float = 1.0) -> dict:
+    """The reference's CPU free surface (src/lbm/free_surface.cpp): `steps` advect_free_surface_vof
+    calls (interface epsilon 0), then normals, curvature, surface-tension acceleration and volume."""
+    lib = ref_lib()
+    n = nx * ny * nz
+    f = np.ascontiguousarray(fill, np.float64).reshape(-1).copy()
+    ux, uy, uz = (np.ascontiguousarray(c, np.float32).reshape(-1) for c in u)
+    normals, tension = np.zeros(3 * n), np.zeros(3 * n)
+    curvature, volume = np.zeros(n), np.zeros(1)
+    _check(lib, lib.ref_free_surface(nx, ny, nz, _ptr(f, _d), _ptr(ux, _f), _ptr(uy, _f), _ptr(uz, _f), float(dt),
+                                     int(steps), float(sigma), float(density), _ptr(normals, _d),
+                                     _ptr(curvature, _d), _ptr(tension, _d), _ptr(volume, _d)))
+    return {"fill": f, "normals": normals.reshape(n, 3).T.copy(), "curvature": curvature,
+            "tension": tension.reshape(n, 3).T.copy(), "volume": float(volume[0])}
+
+
+def ref_particles(records, u, nx: int, ny: int, nz: int, dt: float, two_way: bool, gravity=(0.0, 0.0, 0.0)):
+    """The reference's CPU advance_immersed_boundary_particles (src/lbm/particles.cpp:86-140), once:
+    (records after the step, count x 8 doubles; acceleration 3 x N floats or None)."""
+    lib = ref_lib()
+    n = nx * ny * nz
+    r = np.ascontiguousarray(records, np.float64).reshape(-1, 8).copy()
+    ux, uy, uz = (np.ascontiguousarray(c, np.float32).reshape(-1) for c in u)
+    acc = np.zeros(3 * n, np.float32)
+    _check(lib, lib.ref_particles(nx, ny, nz, _ptr(ux, _f), _ptr(uy, _f), _ptr(uz, _f), _ptr(r, _d), len(r), float(dt),
+                                  int(bool(two_way)), *(float(g) for g in gravity), _ptr(acc, _f)))
+    return r, (acc.reshape(3, n) if two_way else None)
+
+
+# ------------------------------------------------ resident free surface, particles, Q
+# Restatements of the reference's resident SYCL solvers (resident_multiphysics_sycl.hpp:202-405)
+# in float32 numpy, one rounding per operation in the reference's operand order.  Fields are
+# flat arrays of nx*ny*nz cells, x fastest; every axis is periodic.
+
+def _shifts(v, nx: int, ny: int, nz: int):
+    """(xp, xm, yp, ym, zp, zm): the periodic neighbour values of every cell."""
+    a = np.asarray(v).reshape(nz, ny, nx)
+    return tuple(np.roll(a, s, axis=ax).reshape(-1) for ax in (2, 1, 0) for s in (-1, 1))
+
+
+def fill_half_space_x(nx: int, ny: int, nz: int, interface_x: float) -> np.ndarray:
+    """initialize_half_space_x (resident_multiphysics_sycl.hpp:227-236)."""
+    f32 = np.float32
+    left = (np.arange(nx * ny * nz) % nx).astype(f32)
+    right = left + f32(1.0)
+    i = f32(interface_x)
+    return np.where(i <= left, f32(0.0), np.where(i >= right, f32(1.0), i - left)).astype(f32)
+
+
+def fill_advect(phi, u, nx: int, ny: int, nz: int, dt: float) -> np.ndarray:
+    """advect (resident_multiphysics_sycl.hpp:238-264): face velocity 0.5 (u_n + u_nb), upwind
+    flux u_face * phi_upwind, phi - dt ((fxp - fxm) + (fyp - fym) + (fzp - fzm)), clamped to [0, 1]."""
+    f32 = np.float32
+    half, dt = f32(0.5), f32(dt)
+    p = np.asarray(phi, f32).reshape(-1)
+    ux, uy, uz = (np.asarray(c, f32).reshape(-1) for c in u)
+    pxp, pxm, pyp, pym, pzp, pzm = _shifts(p, nx, ny, nz)
+    uxp_, uxm_, _, _, _, _ = _shifts(ux, nx, ny, nz)
+    _, _, uyp_, uym_, _, _ = _shifts(uy, nx, ny, nz)
+    _, _, _, _, uzp_, uzm_ = _shifts(uz, nx, ny, nz)
+
+    def up(v, here, there):
+        return np.where(v >= 0, v * here, v * there)
+
+    uxp, uxm = half * (ux + uxp_), half * (uxm_ + ux)
+    uyp, uym = half * (uy + uyp_), half * (uym_ + uy)
+    uzp, uzm = half * (uz + uzp_), half * (uzm_ + uz)
+    div = ((up(uxp, p, pxp) - up(uxm, pxm, p)) + (up(uyp, p, pyp) - up(uym, pym, p))) + (up(uzp, p, pzp) -
+                                                                                       up(uzm, pzm, p))
+    v = p - dt * div
+    return np.where(v < 0, f32(0.0), np.where(v > 1, f32(1.0), v)).astype(f32)
+
+
+def _half_gradient(p, nx, ny, nz):
+    f32 = np.float32
+    pxp, pxm, pyp, pym, pzp, pzm = _shifts(p, nx, ny, nz)
+    return f32(0.5) * (pxp - pxm), f32(0.5) * (pyp - pym), f32(0.5) * (pzp - pzm)
+
+
+def fill_geometry(phi, nx: int, ny: int, nz: int):
+    """refresh_geometry (resident_multiphysics_sycl.hpp:269-298): normals grad/|grad| (0 where
+    |grad| <= 1e-12) and curvature -0.5 ((nx_xp - nx_xm) + (ny_yp - ny_ym) + (nz_zp - nz_zm))."""
+    f32 = np.float32
+    p = np.asarray(phi, f32).reshape(-1)
+    gx, gy, gz = _half_gradient(p, nx, ny, nz)
+    mag = np.sqrt((gx * gx + gy * gy) + gz * gz)
+    ok = mag > f32(1.0e-12)
+    safe = np.where(ok, mag, f32(1.0))
+    nrm = [np.where(ok, g / safe, f32(0.0)).astype(f32) for g in (gx, gy, gz)]
+    sx = _shifts(nrm[0], nx, ny, nz)
+    sy = _shifts(nrm[1], nx, ny, nz)
+    sz = _shifts(nrm[2], nx, ny, nz)
+    curvature = f32(-0.5) * (((sx[0] - sx[1]) + (sy[2] - sy[3])) + (sz[4] - sz[5]))
+    return nrm[0], nrm[1], nrm[2], curvature.astype(f32)
+
+
+def surface_tension(phi, curvature, acceleration, nx: int, ny: int, nz: int, sigma: float, density: float = 1.0):
+    """add_surface_tension_acceleration (resident_multiphysics_sycl.hpp:300-318) on (ax, ay, az):
+    c = sigma * kappa / rho; a += c * 0.5 (phi_p - phi_m) per axis."""
+    f32 = np.float32
+    p = np.asarray(phi, f32).reshape(-1)
+    c = (f32(sigma) * np.asarray(curvature, f32)) / f32(density)
+    return tuple((np.asarray(a, f32) + c * g).astype(f32) for a, g in zip(acceleration, _half_gradient(p, nx, ny, nz)))
+
+
+def _periodic32(v, extent: int):
+    f32 = np.float32
+    e = f32(extent)
+    turns = np.floor(v / e).astype(f32)
+    v = v - turns * e
+    v = np.where(v >= e, v - e, v)
+    return np.where(v < 0, v + e, v).astype(f32)
+
+
+def particles_advance(state, u, acceleration, nx: int, ny: int, nz: int, dt: float, two_way: bool,
+                      gravity=(0.0, 0.0, 0.0)):
+    """ResidentParticlesSycl3D::advance (resident_multiphysics_sycl.hpp:348-369) on the float32
+    state [8][count] (x, y, z, vx, vy, vz, mass, response): trilinear velocity in (dz, dy, dx)
+    order, drag = mass (u - v) / response, two-way spreading of -drag * w (added here in particle
+    order; the device adds atomically), v += dt (drag / mass + g), x = periodic(x + dt v)."""
+    f32 = np.float32
+    st = np.asarray(state, f32).reshape(8, -1).copy()
+    dt = f32(dt)
+    g = [f32(v) for v in gravity]
+    ux, uy, uz = (np.asarray(c, f32).reshape(-1) for c in u)
+    acc = None if acceleration is None else [np.asarray(a, f32).reshape(-1).copy() for a in acceleration]
+    pos = [_periodic32(st[k], e) for k, e in enumerate((nx, ny, nz))]
+    vel = [st[3], st[4], st[5]]
+    mass, response = st[6], st[7]
+    base = [np.floor(p).astype(np.int64) for p in pos]
+    t = [p - b.astype(f32) for p, b in zip(pos, base)]
+    fu = [np.zeros_like(mass) for _ in range(3)]
+    corners = []
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                w = [t[k] if d else f32(1.0) - t[k] for k, d in enumerate((dx, dy, dz))]
+                ix = (base[0] + dx) % nx
+                iy = (base[1] + dy) % ny
+                iz = (base[2] + dz) % nz
+                n = (iz * ny + iy) * nx + ix
+                wt = (w[0] * w[1]) * w[2]
+                corners.append((n, wt))
+                fu = [f + wt * c[n] for f, c in zip(fu, (ux, uy, uz))]
+    drag = [(mass * (f - v)) / response for f, v in zip(fu, vel)]
+    if two_way:
+        for p_ in range(mass.size):
+            for n, wt in corners:
+                for k in range(3):
+                    acc[k][n[p_]] = f32(acc[k][n[p_]] + f32(-drag[k][p_]) * wt[p_])
+    vel = [v + dt * (d / mass + gk) for v, d, gk in zip(vel, drag, g)]
+    pos = [_periodic32(p + dt * v, e) for p, v, e in zip(pos, vel, (nx, ny, nz))]
+    for k in range(3):
+        st[k] = pos[k]
+        st[3 + k] = vel[k]
+    return st, (None if acc is None else tuple(acc))
+
+
+def resident_q(u, nx: int, ny: int, nz: int) -> np.ndarray:
+    """ResidentFlowDiagnosticsSycl3D::q_criterion (resident_multiphysics_sycl.hpp:394-402): periodic
+    g[i][axis] = 0.5 (u_i(+) - u_i(-)), s2 and o2 over (i, j) in row order, Q = 0.5 (o2 - s2)."""
+    f32 = np.float32
+    half = f32(0.5)
+    comps = [_shifts(np.asarray(c, f32).reshape(-1), nx, ny, nz) for c in u]
+    g = [[half * (comps[i][2 * a] - comps[i][2 * a + 1]) for a in range(3)] for i in range(3)]
+    s2 = np.zeros_like(g[0][0])
+    o2 = np.zeros_like(g[0][0])
+    for i in range(3):
+        for j in range(3):
+            sij, oij = half * (g[i][j] + g[j][i]), half * (g[i][j] - g[j][i])
+            s2 = s2 + sij * sij
+            o2 = o2 + oij * oij
+    return (half * (o2 - s2)).astype(f32)
 
 
 def _init_args(init):

@@ -13,10 +13,13 @@
 //   cfd::lbm::PrecisionPullSolver<D,double>    include/cfd/solvers/lbm/precision_pull.hpp:49-213
 //   cfd::lbm::CompressedPopulationPullSolver<D, ShiftedHalfCodec<D>>
 //                                              include/cfd/solvers/lbm/compressed_pull.hpp:95-147
+//   the CPU free surface and point particles   src/lbm/free_surface.cpp, src/lbm/particles.cpp
 #include "cfd/core/parallel.hpp"
 #include "cfd/solvers/lbm/compressed_pull.hpp"
 #include "cfd/solvers/lbm/esoteric_pull.hpp"
+#include "cfd/solvers/lbm/free_surface.hpp"
 #include "cfd/solvers/lbm/one_step_pull.hpp"
+#include "cfd/solvers/lbm/particles.hpp"
 #include "cfd/solvers/lbm/precision_pull.hpp"
 #include "cfd/solvers/lbm/visualization.hpp"
 #include "cfd/solvers/lbm/voxelize.hpp"
@@ -289,6 +292,64 @@ int ref_q_criterion(std::size_t nx, std::size_t ny, std::size_t nz, const double
         for (std::size_t i = 0; i < n; ++i) u.push_back({velocity[3 * i], velocity[3 * i + 1], velocity[3 * i + 2]});
         const auto r = cfd::lbm::q_criterion_3d(nx, ny, nz, u, dx, dy, dz);
         std::memcpy(q, r.data(), n * sizeof(double));
+    });
+}
+
+// advect_free_surface_vof `steps` times (eps 0) on fill (N doubles, in place), then the
+// normals (3N, xyz interleaved), curvature (N) and surface-tension acceleration (3N) of the result.
+int ref_free_surface(std::size_t nx, std::size_t ny, std::size_t nz, double* fill, const float* ux, const float* uy,
+                     const float* uz, double dt, std::size_t steps, double sigma, double density, double* normals,
+                     double* curvature, double* tension, double* volume) {
+    return guarded([&] {
+        const std::size_t n = nx * ny * nz;
+        auto s = cfd::lbm::make_free_surface_field(nx, ny, nz, std::span<const double>(fill, n), 0.0);
+        for (std::size_t k = 0; k < steps; ++k)
+            cfd::lbm::advect_free_surface_vof(s, std::span<const float>(ux, n), std::span<const float>(uy, n),
+                                              std::span<const float>(uz, n), dt, 0.0);
+        std::memcpy(fill, s.fill.data(), n * sizeof(double));
+        const auto nrm = cfd::lbm::free_surface_normals(s);
+        const auto k = cfd::lbm::free_surface_curvature(s);
+        const auto a = cfd::lbm::free_surface_surface_tension_acceleration(s, sigma, density);
+        for (std::size_t i = 0; i < n; ++i) {
+            normals[3 * i] = nrm[i].x;
+            normals[3 * i + 1] = nrm[i].y;
+            normals[3 * i + 2] = nrm[i].z;
+            tension[3 * i] = a[i].x;
+            tension[3 * i + 1] = a[i].y;
+            tension[3 * i + 2] = a[i].z;
+        }
+        std::memcpy(curvature, k.data(), n * sizeof(double));
+        *volume = cfd::lbm::free_surface_volume(s);
+    });
+}
+
+// advance_immersed_boundary_particles once: records = count x 8 doubles (position, velocity, mass,
+// response time; updated in place); with two_way, acceleration = 3N floats (x | y | z planes).
+int ref_particles(std::size_t nx, std::size_t ny, std::size_t nz, const float* ux, const float* uy, const float* uz,
+                  double* records, std::size_t count, double dt, int two_way, double gx, double gy, double gz,
+                  float* acceleration) {
+    return guarded([&] {
+        const std::size_t n = nx * ny * nz;
+        std::vector<cfd::lbm::ImmersedBoundaryParticle> ps(count);
+        for (std::size_t i = 0; i < count; ++i) {
+            const double* r = records + 8 * i;
+            ps[i] = {{r[0], r[1], r[2]}, {r[3], r[4], r[5]}, r[6], r[7]};
+        }
+        const auto out = cfd::lbm::advance_immersed_boundary_particles(
+            nx, ny, nz, std::span<const float>(ux, n), std::span<const float>(uy, n), std::span<const float>(uz, n),
+            ps, dt, two_way != 0, {gx, gy, gz});
+        for (std::size_t i = 0; i < count; ++i) {
+            double* r = records + 8 * i;
+            const auto& p = ps[i];
+            const double v[8] = {p.position.x, p.position.y, p.position.z, p.velocity.x,
+                                 p.velocity.y, p.velocity.z, p.mass,       p.response_time};
+            std::memcpy(r, v, sizeof(v));
+        }
+        if (two_way) {
+            std::memcpy(acceleration, out.acceleration_x.data(), n * sizeof(float));
+            std::memcpy(acceleration + n, out.acceleration_y.data(), n * sizeof(float));
+            std::memcpy(acceleration + 2 * n, out.acceleration_z.data(), n * sizeof(float));
+        }
     });
 }
 

@@ -3,6 +3,7 @@
 //   frontend_check nodevice        -> expects std::runtime_error from the constructor (no CUDA device)
 //   frontend_check gpu <dir>       -> runs a small case, prints "key value" lines for the test to check
 #include "cfd/solvers/lbm/esoteric_pull_cuda.hpp"
+#include "cfd/solvers/lbm/resident_multiphysics_cuda.hpp"
 
 #include <cmath>
 #include <cstdio>
@@ -117,6 +118,53 @@ int main(int argc, char** argv) {
         cfd::lbm::cuda::write_json_state_3d(dir + "/state.json", config.nx, config.ny, config.nz, body.time_step(),
                                             std::span<const double>(speed));
         std::printf("exported 1\n");
+    }
+    // the reference's resident chain (tests/test_v0156_gpu_lbm_multiphysics.cpp:26-67) through the C++ classes
+    {
+        namespace lc = cfd::lbm::cuda;
+        lc::InPlaceLbmConfig c;
+        c.nx = 10;
+        c.ny = 8;
+        c.nz = 6;
+        c.tau = 0.72F;
+        const std::size_t cells = 480;
+        cfd::lbm::EsotericPullCudaSolver<lc::D3Q19> flow(c);
+        flow.initialize_uniform(1.0F, 0.0F, 0.0F, 0.0F);
+        auto force = flow.device_local_acceleration(true);
+        auto macro = flow.refresh_device_macroscopic();
+        cfd::lbm::ResidentThermalD3Q7Cuda thermal(flow, lc::ResidentThermalConfig{10, 8, 6, 0.02F});
+        thermal.initialize_uniform(300.0F);
+        const double heat0 = thermal.total_scalar();
+        thermal.reset_transfer_stats();
+        thermal.step(macro, 3U);
+        thermal.add_boussinesq_acceleration(force, 300.0F, 3.0e-3F, lc::ParticleVector3{0.0, -1.0, 0.0});
+        const double heat1 = thermal.total_scalar();
+        std::printf("chain_thermal %d\n",
+                    std::abs(heat1 - heat0) / heat0 < 2.0e-5 && thermal.transfer_stats().host_transfer_bytes() == 0U);
+        cfd::lbm::ResidentFreeSurfaceCuda3D surface(flow, 10, 8, 6);
+        surface.initialize_half_space_x(3.5F);
+        const double volume0 = surface.volume();
+        surface.advect(macro, 0.2F);
+        const double volume1 = surface.volume();
+        std::printf("chain_volume %d\n", std::abs(volume1 - volume0) < 2.0e-4 * static_cast<double>(cells));
+        surface.add_surface_tension_acceleration(force, 0.072F, 1.0F);
+        lc::ImmersedBoundaryParticle seed{{2.25, 3.5, 2.75}, {}, 1.0, 0.5};
+        cfd::lbm::ResidentParticlesCuda3D particles(flow, 10, 8, 6, 1U);
+        particles.upload(std::span<const lc::ImmersedBoundaryParticle>(&seed, 1U));
+        particles.reset_transfer_stats();
+        particles.advance(macro, force, 0.05F, true);
+        std::printf("chain_particles %d\n", particles.transfer_stats().host_transfer_bytes() == 0U);
+        cfd::lbm::ResidentFlowDiagnosticsCuda3D diagnostics(flow, 10, 8, 6);
+        std::printf("chain_q %d\n", diagnostics.q_criterion(macro) != nullptr);
+        flow.reset_transfer_stats();
+        flow.step(2U);
+        flow.wait();
+        std::printf("chain_flow %d\n", flow.transfer_stats().host_transfer_bytes() == 0U);
+        try {
+            cfd::lbm::ResidentFreeSurfaceCuda3D wrong(flow, 10, 8, 7);
+        } catch (const std::invalid_argument&) {
+            std::printf("chain_grid invalid_argument\n");
+        }
     }
     try {
         solver.set_solid_mask(std::vector<std::uint8_t>(3));

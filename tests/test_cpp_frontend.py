@@ -79,6 +79,11 @@ def test_frontend_on_gpu_matches_python_api(frontend, tmp_path, engine):
     assert vals["q_criterion_equal"] == "1" and vals["exported"] == "1"
     assert (tmp_path / "frame.vtk").read_text().startswith("# vtk DataFile Version 3.0\ncfd_solvers LBM 3-D\nASCII")
     assert '"dimensions": [24, 20, 16]' in (tmp_path / "state.json").read_text()
+    # the reference's resident chain through ResidentThermalD3Q7Cuda, ResidentFreeSurfaceCuda3D,
+    # ResidentParticlesCuda3D and ResidentFlowDiagnosticsCuda3D
+    for key in ("chain_thermal", "chain_volume", "chain_particles", "chain_q", "chain_flow"):
+        assert vals[key] == "1", key
+    assert vals["chain_grid"] == "invalid_argument"
     assert vals["size_mismatch"] == "invalid_argument"
     assert vals["wall_id"] == "out_of_range"
 
