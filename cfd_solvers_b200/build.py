@@ -3,8 +3,9 @@
 Compiles every ``csrc/*.cu`` with nvcc (``-gencode arch=compute_100a,code=sm_100a``)
 in parallel into ``_build/`` at the repository root and links the shared
 library next to this file, where ``cfd_solvers_b200.bindings`` loads it.  The
-C++ front end (``cfd_solvers_b200/apps/cfd_bench.cpp``, ``include/cfd/solvers/lbm/esoteric_pull_cuda.hpp``)
-links against the same library.
+C++ front end (``include/cfd/solvers/lbm/esoteric_pull_cuda.hpp``) and its two CLIs
+(``cfd_solvers_b200/apps/cfd_bench.cpp``, ``cfd_solvers_b200/apps/cfd_solve.cpp``) link against the
+same library.
 
 Usage: ``python -m cfd_solvers_b200.build [--force] [--jobs N]``.
 """
@@ -26,6 +27,7 @@ BUILD = ROOT / "_build"
 LIB = PKG / "libcfdx_lbm.so"
 APPS = PKG / "apps"
 BENCH_BIN = PKG / "cfd-bench-cuda"
+SOLVE_BIN = PKG / "cfd-solve-cuda"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr",
@@ -72,7 +74,7 @@ def _compile(src: Path, verbose: bool) -> Path:
 
 
 def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
-    """Builds libcfdx_lbm.so (and the cfd-bench-cuda CLI); returns the library path."""
+    """Builds libcfdx_lbm.so (and the cfd-bench-cuda and cfd-solve-cuda CLIs); returns the library path."""
     BUILD.mkdir(exist_ok=True)
     if force:
         for o in BUILD.glob("*.o"):
@@ -86,14 +88,14 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    bench_src = APPS / "cfd_bench.cpp"
-    if bench_src.exists() and (force or _stale(BENCH_BIN, [bench_src, LIB] + _headers() +
-                                               list((INCLUDE / "cfd" / "solvers" / "lbm").glob("*.hpp")))):
-        cmd = [host_cxx(), "-std=c++20", "-O2", f"-I{INCLUDE}", str(bench_src), "-o", str(BENCH_BIN),
-               f"-L{PKG}", "-lcfdx_lbm", "-Wl,-rpath,$ORIGIN"]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+    headers = _headers() + list((INCLUDE / "cfd" / "solvers" / "lbm").glob("*.hpp"))
+    for src, exe in ((APPS / "cfd_bench.cpp", BENCH_BIN), (APPS / "cfd_solve.cpp", SOLVE_BIN)):
+        if src.exists() and (force or _stale(exe, [src, LIB] + headers)):
+            cmd = [host_cxx(), "-std=c++20", "-O2", f"-I{INCLUDE}", str(src), "-o", str(exe),
+                   f"-L{PKG}", "-lcfdx_lbm", "-Wl,-rpath,$ORIGIN"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
     return LIB
 
 

@@ -352,6 +352,43 @@ public:
         cuda::check(cfdx_lbm_q_criterion(handle_, dx, dy, dz, q.data(), CFDX_HOST), "q_criterion");
         return q;
     }
+    // Symmetric relaxation time for the following steps (the adjoint's dJ/dtau is taken with respect to it).
+    void set_tau(float tau) {
+        cuda::check(cfdx_lbm_set_tau(handle_, tau), "set_tau");
+        config_.tau = tau;
+    }
+
+    // ------------------------------------------------ discrete adjoint (gray LBM)
+    // `steps` steps from the current state keeping a checkpoint every `interval` steps.
+    void adjoint_forward(std::uint64_t steps, std::uint32_t interval) {
+        cuda::check(cfdx_lbm_adjoint_forward(handle_, steps, interval), "adjoint_forward");
+    }
+    struct AdjointGradient {
+        std::vector<double> solid_fraction; // dJ/dn_s per cell (0 on walls)
+        double tau{0.0};                    // dJ/dtau
+    };
+    // Reverse sweep for J(final state) given dJ/du (and optionally dJ/drho) of the
+    // fields compute_macroscopic reports (u includes +a/2).
+    [[nodiscard]] AdjointGradient adjoint_backward(std::span<const float> g_ux, std::span<const float> g_uy,
+                                                   std::span<const float> g_uz, std::span<const float> g_rho = {}) {
+        if (g_ux.size() != cells_ || g_uy.size() != cells_ || g_uz.size() != cells_ ||
+            (!g_rho.empty() && g_rho.size() != cells_))
+            throw std::invalid_argument("adjoint seed size mismatch");
+        AdjointGradient g;
+        g.solid_fraction.resize(cells_);
+        cuda::check(cfdx_lbm_adjoint_backward(handle_, g_rho.empty() ? nullptr : g_rho.data(), g_ux.data(),
+                                              g_uy.data(), g_uz.data(), CFDX_HOST, g.solid_fraction.data(), CFDX_HOST,
+                                              &g.tau),
+                    "adjoint_backward");
+        return g;
+    }
+    [[nodiscard]] std::size_t adjoint_memory() const {
+        std::size_t b = 0;
+        cuda::check(cfdx_lbm_adjoint_memory(handle_, &b), "adjoint_memory");
+        return b;
+    }
+    void adjoint_release() { cuda::check(cfdx_lbm_adjoint_release(handle_), "adjoint_release"); }
+
     [[nodiscard]] cfdx_lbm* native_handle() const noexcept { return handle_; }
 
 private:
