@@ -326,6 +326,20 @@ def thermal_d3q7_step(g, u, nx: int, ny: int, nz: int, diffusivity: float, steps
     return g.reshape(-1)
 
 
+# The velocity sets in the reference's direction order (descriptors.hpp:59-146): D3Q19 is the first
+# 19 directions of D3Q27; pairs (i, i+1) for odd i are opposites.
+_CX = (0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1)
+_CY = (0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1)
+_CZ = (0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1)
+
+
+def velocity_set(q: int) -> np.ndarray:
+    """(q, 3) integer lattice velocities of D3Q19 or D3Q27."""
+    if q not in (19, 27):
+        raise ValueError("q must be 19 or 27")
+    return np.stack([_CX[:q], _CY[:q], _CZ[:q]], 1).astype(np.int64)
+
+
 def f32_to_f16_bits(v: float) -> int:
     return int(oracle_lib().ora_f32_to_f16(v))
 

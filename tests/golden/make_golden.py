@@ -21,6 +21,10 @@ Cases (reference files and tests they restate):
                      A = 0.02, one step: logical populations (esoteric_pull.hpp:434-492)
   trt_q19/q27_s7/s8  two-grid TRT 18x14x10, tau 0.73, tau- 1.1, a = (2e-6,-1e-6,5e-7), A = 0.017
                      (one_step_pull.hpp:187-204; tests/test_main.cpp:340-434)
+  bgk_q19/q27_s7/s8  two-grid BGK OneStepPullSolver(config) 18x14x10, tau 0.73, A = 0.017
+                     (tests/test_main.cpp:340-372, odd and even step counts)
+  bgk_forced_q19/q27 the same from rest with a = (2e-6, -1e-6, 5e-7), 60 steps
+                     (tests/test_main.cpp:403-434)
   f64_q19            two-grid FP64 18x14x10, tau 0.73, A = 0.017, 8 steps (precision_pull.hpp)
   f16_q19            two-grid shifted-FP16 16x14x12, tau 0.72, A = 0.025, 16 steps
                      (compressed_pull.hpp; tests/test_v0141_lbm_les_qcriterion.cpp:143-180)
@@ -91,6 +95,16 @@ def main():
             r = O.ref_twogrid(q, 18, 14, 10, 0.73, 1.1, s, init=("tg", 0.017), accel=(2e-6, -1e-6, 0.5e-6))
             for k, v in fields(r).items():
                 out[f"trt_q{q}_s{s}_{k}"] = v
+
+    # BGK two-grid: the in-place/two-grid gates of tests/test_main.cpp:340-434
+    for q in (19, 27):
+        for s in (7, 8):
+            r = O.ref_twogrid(q, 18, 14, 10, 0.73, 0.0, s, init=("tg", 0.017))
+            for k, v in fields(r).items():
+                out[f"bgk_q{q}_s{s}_{k}"] = v
+        r = O.ref_twogrid(q, 18, 14, 10, 0.73, 0.0, 60, init=("uniform",), accel=(2e-6, -1e-6, 0.5e-6))
+        for k, v in fields(r).items():
+            out[f"bgk_forced_q{q}_{k}"] = v
 
     # FP64 two-grid
     r = O.ref_precision(19, 18, 14, 10, 0.73, 8, init=("tg", 0.017))

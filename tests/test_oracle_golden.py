@@ -112,6 +112,32 @@ def test_trt_against_reference_two_grid(oracle_mod, golden, q, steps):
         assert maxabs(arr, data[f"trt_q{q}_s{steps}_{name}"]) < 7e-6, name
 
 
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("steps", [7, 8])
+def test_bgk_inplace_against_reference_two_grid(oracle_mod, golden, q, steps):
+    """tests/test_main.cpp:340-372: in-place vs the reference's two-grid pull, Taylor-Green
+    A = 0.017 on 18x14x10, tau 0.73, odd and even step counts; gate 5e-6."""
+    data, _ = golden
+    L = oracle_mod.OracleLattice(q, 18, 14, 10, tau=0.73)
+    L.init_taylor_green(0.017)
+    L.step(steps)
+    for name, arr in zip(("rho", "ux", "uy", "uz"), L.macroscopic()):
+        assert maxabs(arr, data[f"bgk_q{q}_s{steps}_{name}"]) < 5e-6, name
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_forced_inplace_against_reference_two_grid(oracle_mod, golden, q):
+    """tests/test_main.cpp:403-434: from rest with a = (2e-6, -1e-6, 5e-7), 60 steps; gate 7e-6."""
+    data, _ = golden
+    L = oracle_mod.OracleLattice(q, 18, 14, 10, tau=0.73, accel=(2e-6, -1e-6, 0.5e-6))
+    L.init_uniform()
+    L.step(60)
+    got = L.macroscopic()
+    for name, arr in zip(("rho", "ux", "uy", "uz"), got):
+        assert maxabs(arr, data[f"bgk_forced_q{q}_{name}"]) < 7e-6, name
+    assert got[1][got[1].size // 2] > 0
+
+
 def test_fp64_against_reference_precision_solver(oracle_mod, golden):
     """FP64 oracle vs PrecisionPullSolver<D3Q19,double> (precision_pull.hpp:49-213).
 
@@ -217,3 +243,19 @@ def test_live_reference_forced_parity(oracle_mod, q):
     L.step(9)
     r = oracle_mod.ref_esoteric(q, 17, 15, 13, 0.66, 9, init=("tg", 0.03), accel=acc, les=True, logical=True)
     assert np.array_equal(bits(L.logical()), bits(r["logical"]))
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_velocity_set_moments(oracle_mod, q):
+    """tests/test_main.cpp:278-310 on the oracle's velocity set with the reference's weights
+    (descriptors.hpp:59-146): sum w = 1, isotropic second moments, opposite pairs (i, i+1)."""
+    c = oracle_mod.velocity_set(q).astype(np.float64)
+    speed2 = (c * c).sum(1)
+    table = {19: {0: 1 / 3, 1: 1 / 18, 2: 1 / 36}, 27: {0: 8 / 27, 1: 2 / 27, 2: 1 / 54, 3: 1 / 216}}[q]
+    w = np.array([table[int(s)] for s in speed2])
+    assert abs(w.sum() - 1) < 2e-7
+    for a in range(3):
+        assert abs((w * c[:, a] ** 2).sum() - 1 / 3) < 2e-7
+    assert abs((w * c[:, 0] * c[:, 1]).sum()) < 2e-7
+    for i in range(1, q, 2):
+        assert np.array_equal(c[i], -c[i + 1])
