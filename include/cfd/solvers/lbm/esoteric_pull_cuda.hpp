@@ -253,6 +253,8 @@ public:
 
     // ------------------------------------------------ reference API (SYCL class)
     void wait() { cuda::check(cfdx_lbm_synchronize(handle_), "wait"); }
+    // Reference download_macroscopic (esoteric_pull_sycl.hpp:309-325): the device fields copied to the host.
+    [[nodiscard]] cuda::MacroscopicFields download_macroscopic() const { return compute_macroscopic(); }
     [[nodiscard]] double total_mass() const { return mass(); }
     [[nodiscard]] std::size_t resident_bytes() const { return info().resident_bytes; }
     [[nodiscard]] std::string device_name() const { return "CUDA device " + std::to_string(config_.device); }

@@ -48,6 +48,7 @@ int main(int argc, char** argv) {
     std::printf("mass %.17g\n", solver.mass());
     std::printf("kinetic_energy %.17g\n", solver.kinetic_energy());
     const auto fields = solver.compute_macroscopic();
+    std::printf("download_equal %d\n", solver.download_macroscopic().ux == fields.ux ? 1 : 0);
     double sum_ux = 0.0;
     for (const float v : fields.ux) sum_ux += v;
     std::printf("sum_ux %.17g\n", sum_ux);

@@ -72,6 +72,7 @@ def test_frontend_on_gpu_matches_python_api(frontend, tmp_path, engine):
         assert float(vals["checksum"]) == s.checksum()
         assert float(vals["mass"]) == s.mass()
     assert vals["restart_bitwise"] == "1"
+    assert vals["download_equal"] == "1"
     # slab class, device voxelizer, Q-criterion and writers through the C++ front end
     assert vals["slab_info"] == "0 16 16" and vals["slab_equals_whole"] == "1"
     assert int(vals["halo_bytes"]) == 5 * 24 * 20 * 4
