@@ -106,6 +106,11 @@ class cfdx_halo_entry(ctypes.Structure):
     _fields_ = [("plane", ctypes.c_uint32), ("direction", ctypes.c_uint32)]
 
 
+class cfdx_slot_audit(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in ("slots", "touched", "read_twice", "written_twice", "read_only",
+                                               "write_only", "foreign")]
+
+
 class cfdx_voxel_grid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_size_t), ("ny", ctypes.c_size_t), ("nz", ctypes.c_size_t),
                 ("minimum", ctypes.c_double * 3), ("maximum", ctypes.c_double * 3)]
@@ -206,6 +211,8 @@ SIGNATURES = {
     "cfdx_diagnostics_destroy": (_i, [_vp]),
     "cfdx_diagnostics_q_criterion": (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
     "cfdx_diagnostics_info": (_i, [_vp, ctypes.POINTER(_sz)]),
+    "cfdx_lbm_debug_slot_audit": (_i, [_H, _i, ctypes.POINTER(cfdx_slot_audit)]),
+    "cfdx_debug_audit_classify": (_i, [ctypes.c_uint32] * 5 + [ctypes.POINTER(ctypes.c_uint)]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

@@ -26,6 +26,7 @@
 #include "voxelize.h"
 #include "export.h"
 #include "resident.h"
+#include "slot_audit.h"
 #include "thermal.h"
 
 namespace {
@@ -2507,6 +2508,39 @@ CFDX_API int cfdx_diagnostics_info(cfdx_diagnostics* d, std::size_t* resident_by
     return guarded([&] {
         require(d != nullptr && resident_bytes != nullptr, "null handle or output");
         *resident_bytes = static_cast<std::size_t>(d->grid.cells) * sizeof(float);
+    });
+}
+
+CFDX_API int cfdx_lbm_debug_slot_audit(cfdx_lbm* h, int parity, cfdx_slot_audit* out) {
+    std::uint32_t* counters = nullptr;
+    AuditCounts* counts = nullptr;
+    const int rc = guarded([&] {
+        checked(h);
+        require(out != nullptr, "null output");
+        require(parity == 0 || parity == 1, "parity must be 0 or 1");
+        const std::size_t slots = static_cast<std::size_t>(h->key.q) * h->N;
+        require(slots <= (std::size_t{1} << 28), "the slot audit takes lattices of at most 2^28 slots");
+        counters = static_cast<std::uint32_t*>(device_alloc(5U * slots * sizeof(std::uint32_t), "slot audit counters"));
+        counts = static_cast<AuditCounts*>(device_alloc(sizeof(AuditCounts), "slot audit counts"));
+        const LbmArgs a = h->args_at(counters, static_cast<int>(sizeof(std::uint32_t)), parity);
+        check_cuda(launch_slot_audit(h->key, a, counters, h->grid(), h->block(), counts, h->stream), "slot audit");
+        AuditCounts host{};
+        check_cuda(cudaMemcpyAsync(&host, counts, sizeof host, cudaMemcpyDeviceToHost, h->stream),
+                   "cudaMemcpyAsync (slot audit)");
+        h->sync();
+        *out = cfdx_slot_audit{slots, host.touched, host.read_twice, host.written_twice, host.read_only,
+                               host.write_only, host.foreign};
+    });
+    device_free(counters);
+    device_free(counts);
+    return rc;
+}
+
+CFDX_API int cfdx_debug_audit_classify(uint32_t reads, uint32_t writes, uint32_t lowest_reader,
+                                       uint32_t highest_reader, uint32_t writer, unsigned* classes) {
+    return guarded([&] {
+        require(classes != nullptr, "null output");
+        *classes = audit_classify(reads, writes, lowest_reader, highest_reader, writer);
     });
 }
 

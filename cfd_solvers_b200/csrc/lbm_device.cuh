@@ -60,10 +60,45 @@ struct StF16 {
     static constexpr bool scaled = true;
 };
 
+// Slot-ownership audit (a test hook; see slot_audit.cu): a storage type whose
+// loads and stores record who touched each slot instead of moving data.  The
+// step kernels instantiated with it run their real addressing code.  Per slot
+// there are five 32-bit counters, `stride` = q * cells apart: reads, writes,
+// lowest and highest reading thread, writing thread (threads numbered from 1).
+template <bool SCALED> struct StAudit {
+    using T = std::uint32_t;
+    using R = float;
+    static constexpr bool delta = SCALED;
+    static constexpr bool scaled = SCALED;
+};
+template <class S> struct IsAudit {
+    static constexpr bool value = false;
+};
+template <bool SCALED> struct IsAudit<StAudit<SCALED>> {
+    static constexpr bool value = true;
+};
+__device__ __forceinline__ std::uint32_t audit_thread() {
+    const std::uint32_t block = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    return block * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x + 1U;
+}
+__device__ __forceinline__ void audit_read(std::uint32_t* p, std::uint32_t stride) {
+    const std::uint32_t id = audit_thread();
+    atomicAdd(p, 1U);
+    atomicMin(p + 2U * stride, id);
+    atomicMax(p + 3U * stride, id);
+}
+__device__ __forceinline__ void audit_write(std::uint32_t* p, std::uint32_t stride) {
+    atomicAdd(p + stride, 1U);
+    atomicExch(p + 4U * stride, audit_thread());
+}
+
 // RAW: FP16 values stay in storage units h (no scale applied).
 template <class S, class L, int D, bool RAW = false>
 __device__ __forceinline__ typename S::R ld(const typename S::T* p, const LbmArgs& a) {
-    if constexpr (sizeof(typename S::T) == 2) {
+    if constexpr (IsAudit<S>::value) {
+        audit_read(const_cast<std::uint32_t*>(p), static_cast<std::uint32_t>(L::Q) * a.N);
+        return 0.0F;
+    } else if constexpr (sizeof(typename S::T) == 2) {
         if constexpr (RAW)
             return __half2float(*p);
         else
@@ -75,7 +110,10 @@ __device__ __forceinline__ typename S::R ld(const typename S::T* p, const LbmArg
 
 template <class S, class L, int D, bool RAW = false>
 __device__ __forceinline__ void st(typename S::T* p, typename S::R v, const LbmArgs& a) {
-    if constexpr (sizeof(typename S::T) == 2) {
+    if constexpr (IsAudit<S>::value) {
+        (void)v;
+        audit_write(p, static_cast<std::uint32_t>(L::Q) * a.N);
+    } else if constexpr (sizeof(typename S::T) == 2) {
         if constexpr (RAW)
             *p = __float2half_rn(v);
         else

@@ -333,6 +333,14 @@ class EsotericPullCudaSolver:
         step = 4 * self._cells
         return DeviceAccelerationView(base, base + step, base + 2 * step, self._cells)
 
+    def debug_slot_audit(self, parity: int) -> dict:
+        """Slot-ownership audit of the step of `parity` (cfdx_lbm_debug_slot_audit): per-class slot
+        counts.  A race-free step has written_twice == foreign == 0; read_only and write_only
+        count the links into wall cells (one of each per link)."""
+        out = B.cfdx_slot_audit()
+        self._call("cfdx_lbm_debug_slot_audit", int(parity), ctypes.byref(out))
+        return {k: int(getattr(out, k)) for k, _ in B.cfdx_slot_audit._fields_}
+
     def resident_bytes(self) -> int:
         return int(self._info().resident_bytes)
 

@@ -550,6 +550,39 @@ CFDX_API int cfdx_diagnostics_q_criterion(cfdx_diagnostics* diagnostics, const f
                                           const float* uz, float** q);
 CFDX_API int cfdx_diagnostics_info(cfdx_diagnostics* diagnostics, size_t* resident_bytes);
 
+/* ---- Slot-ownership audit (a test hook standing in for a race detector).
+ * In-place streaming is race-free because, within a step, every population
+ * slot is loaded and then stored by exactly one cell.  The audit runs the
+ * one-cell step kernel's own addressing (gather, wall links, moving walls,
+ * slab ghost planes) for the step of the given parity with a storage type that
+ * records, per slot, its loads, its stores and the threads that made them,
+ * and counts the slots in each class below.  The lattice is not modified; the
+ * audit uses 20 bytes per slot of scratch (at most 2^28 slots).  A race-free
+ * step has written_twice = foreign = 0 (and read_twice = 0).  A fluid cell
+ * touches q slots plus one per link into a wall cell: such a link loads one of
+ * the wall cell's two slots of the pair and stores the other (half-way
+ * bounce-back in place), so read_only = write_only = the number of wall links,
+ * and touched = q * fluid cells + wall links. */
+typedef struct cfdx_slot_audit {
+    uint64_t slots;         /* q * cells */
+    uint64_t touched;       /* read or written */
+    uint64_t read_twice;    /* loaded more than once */
+    uint64_t written_twice; /* stored more than once: a write-write race */
+    uint64_t read_only;     /* loaded, never stored */
+    uint64_t write_only;    /* stored, never loaded */
+    uint64_t foreign;       /* stored by a thread other than the one that loaded it */
+} cfdx_slot_audit;
+
+CFDX_API int cfdx_lbm_debug_slot_audit(cfdx_lbm* lbm, int parity, cfdx_slot_audit* out);
+
+/* The audit's classification of one slot from its counters (loads, stores,
+ * lowest and highest loading thread, storing thread; threads numbered from
+ * 1): a bit set of 1 touched, 2 read twice, 4 written twice, 8 read only,
+ * 16 write only, 32 foreign.  Host-only; lets the classification be tested
+ * without a GPU. */
+CFDX_API int cfdx_debug_audit_classify(uint32_t reads, uint32_t writes, uint32_t lowest_reader,
+                                       uint32_t highest_reader, uint32_t writer, unsigned* classes);
+
 /* Test hook: the next `count` device allocations of this process fail with
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */
