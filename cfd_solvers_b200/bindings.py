@@ -108,7 +108,7 @@ class cfdx_halo_entry(ctypes.Structure):
 
 class cfdx_slot_audit(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("slots", "touched", "read_twice", "written_twice", "read_only",
-                                               "write_only", "foreign")]
+                                               "write_only", "foreign", "out_of_range")]
 
 
 class cfdx_voxel_grid(ctypes.Structure):

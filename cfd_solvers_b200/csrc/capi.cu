@@ -2520,7 +2520,8 @@ CFDX_API int cfdx_lbm_debug_slot_audit(cfdx_lbm* h, int parity, cfdx_slot_audit*
         require(parity == 0 || parity == 1, "parity must be 0 or 1");
         const std::size_t slots = static_cast<std::size_t>(h->key.q) * h->N;
         require(slots <= (std::size_t{1} << 28), "the slot audit takes lattices of at most 2^28 slots");
-        counters = static_cast<std::uint32_t*>(device_alloc(5U * slots * sizeof(std::uint32_t), "slot audit counters"));
+        counters =
+            static_cast<std::uint32_t*>(device_alloc((5U * slots + 1U) * sizeof(std::uint32_t), "slot audit counters"));
         counts = static_cast<AuditCounts*>(device_alloc(sizeof(AuditCounts), "slot audit counts"));
         const LbmArgs a = h->args_at(counters, static_cast<int>(sizeof(std::uint32_t)), parity);
         check_cuda(launch_slot_audit(h->key, a, counters, h->grid(), h->block(), counts, h->stream), "slot audit");
@@ -2528,8 +2529,8 @@ CFDX_API int cfdx_lbm_debug_slot_audit(cfdx_lbm* h, int parity, cfdx_slot_audit*
         check_cuda(cudaMemcpyAsync(&host, counts, sizeof host, cudaMemcpyDeviceToHost, h->stream),
                    "cudaMemcpyAsync (slot audit)");
         h->sync();
-        *out = cfdx_slot_audit{slots, host.touched, host.read_twice, host.written_twice, host.read_only,
-                               host.write_only, host.foreign};
+        *out = cfdx_slot_audit{slots,          host.touched,    host.read_twice, host.written_twice,
+                               host.read_only, host.write_only, host.foreign,    host.out_of_range};
     });
     device_free(counters);
     device_free(counts);

@@ -64,7 +64,8 @@ struct StF16 {
 // loads and stores record who touched each slot instead of moving data.  The
 // step kernels instantiated with it run their real addressing code.  Per slot
 // there are five 32-bit counters, `stride` = q * cells apart: reads, writes,
-// lowest and highest reading thread, writing thread (threads numbered from 1).
+// lowest and highest reading thread, writing thread (threads numbered from 1);
+// one more word counts accesses outside the slots.
 template <bool SCALED> struct StAudit {
     using T = std::uint32_t;
     using R = float;
@@ -81,13 +82,23 @@ __device__ __forceinline__ std::uint32_t audit_thread() {
     const std::uint32_t block = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
     return block * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x + 1U;
 }
-__device__ __forceinline__ void audit_read(std::uint32_t* p, std::uint32_t stride) {
+// An address outside the lattice's q * cells slots is not accessed: it is
+// counted in the word after the five arrays.
+__device__ __forceinline__ bool audit_in_range(const std::uint32_t* p, const void* base, std::uint32_t stride) {
+    const auto* b = static_cast<const std::uint32_t*>(base);
+    if (p >= b && p < b + stride) return true;
+    atomicAdd(const_cast<std::uint32_t*>(b) + 5U * stride, 1U);
+    return false;
+}
+__device__ __forceinline__ void audit_read(std::uint32_t* p, const void* base, std::uint32_t stride) {
+    if (!audit_in_range(p, base, stride)) return;
     const std::uint32_t id = audit_thread();
     atomicAdd(p, 1U);
     atomicMin(p + 2U * stride, id);
     atomicMax(p + 3U * stride, id);
 }
-__device__ __forceinline__ void audit_write(std::uint32_t* p, std::uint32_t stride) {
+__device__ __forceinline__ void audit_write(std::uint32_t* p, const void* base, std::uint32_t stride) {
+    if (!audit_in_range(p, base, stride)) return;
     atomicAdd(p + stride, 1U);
     atomicExch(p + 4U * stride, audit_thread());
 }
@@ -96,7 +107,7 @@ __device__ __forceinline__ void audit_write(std::uint32_t* p, std::uint32_t stri
 template <class S, class L, int D, bool RAW = false>
 __device__ __forceinline__ typename S::R ld(const typename S::T* p, const LbmArgs& a) {
     if constexpr (IsAudit<S>::value) {
-        audit_read(const_cast<std::uint32_t*>(p), static_cast<std::uint32_t>(L::Q) * a.N);
+        audit_read(const_cast<std::uint32_t*>(p), a.base, static_cast<std::uint32_t>(L::Q) * a.N);
         return 0.0F;
     } else if constexpr (sizeof(typename S::T) == 2) {
         if constexpr (RAW)
@@ -112,7 +123,7 @@ template <class S, class L, int D, bool RAW = false>
 __device__ __forceinline__ void st(typename S::T* p, typename S::R v, const LbmArgs& a) {
     if constexpr (IsAudit<S>::value) {
         (void)v;
-        audit_write(p, static_cast<std::uint32_t>(L::Q) * a.N);
+        audit_write(p, a.base, static_cast<std::uint32_t>(L::Q) * a.N);
     } else if constexpr (sizeof(typename S::T) == 2) {
         if constexpr (RAW)
             *p = __float2half_rn(v);

@@ -16,6 +16,7 @@ namespace cfdx {
 namespace {
 
 __global__ void k_audit_reset(std::uint32_t* c, std::uint32_t slots) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) c[5U * slots] = 0U;
     for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < slots; i += gridDim.x * blockDim.x) {
         c[i] = 0U;
         c[slots + i] = 0U;
@@ -34,6 +35,7 @@ __global__ void k_audit_classify(const std::uint32_t* c, std::uint32_t slots, Au
     unsigned long long* o = &out->touched;
     for (int b = 0; b < 6; ++b)
         if (n[b]) atomicAdd(o + b, n[b]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) out->out_of_range = c[5U * slots];
 }
 
 template <class L, bool SCALED>

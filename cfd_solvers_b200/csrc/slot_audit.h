@@ -21,6 +21,7 @@ struct AuditCounts {
     unsigned long long read_only;     // read, never written
     unsigned long long write_only;    // written, never read
     unsigned long long foreign;       // written by a thread that did not read it
+    unsigned long long out_of_range;  // accesses outside the q * cells slots (not performed)
 };
 
 // The class bits of one slot from its five counters (host and device).
@@ -45,8 +46,8 @@ __host__ __device__ inline unsigned audit_classify(std::uint32_t reads, std::uin
     return c;
 }
 
-// counters: 5 * q * cells words (reads | writes | lowest reader | highest
-// reader | writer), initialised here; `a` is the step's argument block with
+// counters: 5 * q * cells + 1 words (reads | writes | lowest reader | highest
+// reader | writer | out-of-range count), initialised here; `a` is the step's argument block with
 // base / rest_off / pa_off / pb_off addressing the reads array (NARROW form).
 cudaError_t launch_slot_audit(const KernelKey& k, const LbmArgs& a, std::uint32_t* counters, dim3 grid, dim3 block,
                               AuditCounts* device_counts, cudaStream_t s);

@@ -558,7 +558,7 @@ CFDX_API int cfdx_diagnostics_info(cfdx_diagnostics* diagnostics, size_t* reside
  * records, per slot, its loads, its stores and the threads that made them,
  * and counts the slots in each class below.  The lattice is not modified; the
  * audit uses 20 bytes per slot of scratch (at most 2^28 slots).  A race-free
- * step has written_twice = foreign = 0 (and read_twice = 0).  A fluid cell
+ * step has written_twice = foreign = 0 (and read_twice = out_of_range = 0).  A fluid cell
  * touches q slots plus one per link into a wall cell: such a link loads one of
  * the wall cell's two slots of the pair and stores the other (half-way
  * bounce-back in place), so read_only = write_only = the number of wall links,
@@ -571,6 +571,7 @@ typedef struct cfdx_slot_audit {
     uint64_t read_only;     /* loaded, never stored */
     uint64_t write_only;    /* stored, never loaded */
     uint64_t foreign;       /* stored by a thread other than the one that loaded it */
+    uint64_t out_of_range;  /* loads and stores outside the lattice's slots (counted, not performed) */
 } cfdx_slot_audit;
 
 CFDX_API int cfdx_lbm_debug_slot_audit(cfdx_lbm* lbm, int parity, cfdx_slot_audit* out);

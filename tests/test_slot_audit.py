@@ -91,6 +91,7 @@ def test_every_slot_has_one_owner(engine, lattice, q, storage, walls):
             r = s.debug_slot_audit(parity)
             assert r["slots"] == q * nx * ny * nz
             assert r["written_twice"] == 0 and r["foreign"] == 0 and r["read_twice"] == 0, (parity, r)
+            assert r["out_of_range"] == 0, (parity, r)
             assert r["touched"] == q * fluid + links, (parity, r)
             assert r["read_only"] == links and r["write_only"] == links, (parity, r)
         assert np.array_equal(s.logical_populations(), before)  # the audit leaves the lattice alone
@@ -105,6 +106,7 @@ def test_paired_and_gray_handles_audit_the_one_cell_addressing(engine):
         for parity in (0, 1):
             r = s.debug_slot_audit(parity)
             assert r["touched"] == 19 * n ** 3 and r["foreign"] == r["written_twice"] == r["read_twice"] == 0
+            assert r["out_of_range"] == 0
 
 
 @pytest.mark.gpu
@@ -124,6 +126,7 @@ def test_slab_ghost_planes(engine, lattice, q):
             assert r["slots"] == q * nx * ny * (6 + 2)
             assert r["touched"] == q * nx * ny * 6, r
             assert r["read_twice"] == r["written_twice"] == r["read_only"] == r["write_only"] == r["foreign"] == 0
+            assert r["out_of_range"] == 0
 
 
 @pytest.mark.gpu
