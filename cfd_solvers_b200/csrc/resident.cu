@@ -12,6 +12,8 @@
 // atomically summed particle force, whose order of additions is not fixed.
 #include "resident.h"
 
+#include <cstdint>
+
 namespace cfdx {
 namespace {
 
@@ -42,6 +44,70 @@ __device__ __forceinline__ float half_sum(float a, float b) { return __fmul_rn(0
 __device__ __forceinline__ float half_diff(float a, float b) { return __fmul_rn(0.5F, __fsub_rn(a, b)); }
 __device__ __forceinline__ float upwind(float u, float here, float there) { return __fmul_rn(u, u >= 0.0F ? here : there); }
 
+// A field at a cell and its six periodic neighbours.
+struct Nb {
+    float c, xp, xm, yp, ym, zp, zm;
+};
+
+__device__ __forceinline__ Nb nb_of(const float* f, const Stencil& s) {
+    return Nb{f[s.n], f[s.xp], f[s.xm], f[s.yp], f[s.ym], f[s.zp], f[s.zm]};
+}
+
+// ---- the per-cell arithmetic, shared by the one-cell and four-cell kernels
+__device__ __forceinline__ float advect_cell(const Nb& p, const Nb& ux, const Nb& uy, const Nb& uz, float dt) {
+    const float uxp = half_sum(ux.c, ux.xp), uxm = half_sum(ux.xm, ux.c);
+    const float uyp = half_sum(uy.c, uy.yp), uym = half_sum(uy.ym, uy.c);
+    const float uzp = half_sum(uz.c, uz.zp), uzm = half_sum(uz.zm, uz.c);
+    const float fxp = upwind(uxp, p.c, p.xp), fxm = upwind(uxm, p.xm, p.c);
+    const float fyp = upwind(uyp, p.c, p.yp), fym = upwind(uym, p.ym, p.c);
+    const float fzp = upwind(uzp, p.c, p.zp), fzm = upwind(uzm, p.zm, p.c);
+    const float div = __fadd_rn(__fadd_rn(__fsub_rn(fxp, fxm), __fsub_rn(fyp, fym)), __fsub_rn(fzp, fzm));
+    const float value = __fsub_rn(p.c, __fmul_rn(dt, div));
+    return value < 0.0F ? 0.0F : (value > 1.0F ? 1.0F : value);
+}
+
+__device__ __forceinline__ float3 normal_cell(const Nb& p) {
+    const float gx = half_diff(p.xp, p.xm), gy = half_diff(p.yp, p.ym), gz = half_diff(p.zp, p.zm);
+    const float mag = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)), __fmul_rn(gz, gz)));
+    if (!(mag > 1.0e-12F)) return make_float3(0.0F, 0.0F, 0.0F);
+    return make_float3(__fdiv_rn(gx, mag), __fdiv_rn(gy, mag), __fdiv_rn(gz, mag));
+}
+
+__device__ __forceinline__ float curvature_cell(const Nb& nx, const Nb& ny, const Nb& nz) {
+    const float d =
+        __fadd_rn(__fadd_rn(__fsub_rn(nx.xp, nx.xm), __fsub_rn(ny.yp, ny.ym)), __fsub_rn(nz.zp, nz.zm));
+    return __fmul_rn(-0.5F, d);
+}
+
+// sigma * kappa / rho * grad(phi), to be added to the acceleration
+__device__ __forceinline__ float3 tension_cell(const Nb& p, float kappa, float sigma, float density) {
+    const float gx = half_diff(p.xp, p.xm), gy = half_diff(p.yp, p.ym), gz = half_diff(p.zp, p.zm);
+    const float c = __fdiv_rn(__fmul_rn(sigma, kappa), density);
+    return make_float3(__fmul_rn(c, gx), __fmul_rn(c, gy), __fmul_rn(c, gz));
+}
+
+__device__ __forceinline__ float q_cell(const Nb& ux, const Nb& uy, const Nb& uz) {
+    const Nb* u[3] = {&ux, &uy, &uz};
+    float g[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        g[i][0] = half_diff(u[i]->xp, u[i]->xm);
+        g[i][1] = half_diff(u[i]->yp, u[i]->ym);
+        g[i][2] = half_diff(u[i]->zp, u[i]->zm);
+    }
+    float s2 = 0.0F, o2 = 0.0F;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float sij = half_sum(g[i][j], g[j][i]), oij = half_diff(g[i][j], g[j][i]);
+            s2 = __fadd_rn(s2, __fmul_rn(sij, sij));
+            o2 = __fadd_rn(o2, __fmul_rn(oij, oij));
+        }
+    return __fmul_rn(0.5F, __fsub_rn(o2, s2));
+}
+
+// ---- one cell per thread (any nx)
 __global__ void __launch_bounds__(256) k_fill_uniform(float* fill, u32 cells, float value) {
     const u32 n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n < cells) fill[n] = value;
@@ -58,42 +124,24 @@ __global__ void __launch_bounds__(128) k_fill_advect(const float* phi, float* ou
                                                      const float* uy, const float* uz, float dt) {
     Stencil s;
     if (!stencil(t, s)) return;
-    const u32 n = s.n;
-    const float uxp = half_sum(ux[n], ux[s.xp]), uxm = half_sum(ux[s.xm], ux[n]);
-    const float uyp = half_sum(uy[n], uy[s.yp]), uym = half_sum(uy[s.ym], uy[n]);
-    const float uzp = half_sum(uz[n], uz[s.zp]), uzm = half_sum(uz[s.zm], uz[n]);
-    const float fxp = upwind(uxp, phi[n], phi[s.xp]), fxm = upwind(uxm, phi[s.xm], phi[n]);
-    const float fyp = upwind(uyp, phi[n], phi[s.yp]), fym = upwind(uym, phi[s.ym], phi[n]);
-    const float fzp = upwind(uzp, phi[n], phi[s.zp]), fzm = upwind(uzm, phi[s.zm], phi[n]);
-    const float div = __fadd_rn(__fadd_rn(__fsub_rn(fxp, fxm), __fsub_rn(fyp, fym)), __fsub_rn(fzp, fzm));
-    float value = __fsub_rn(phi[n], __fmul_rn(dt, div));
-    value = value < 0.0F ? 0.0F : (value > 1.0F ? 1.0F : value);
-    out[n] = value;
+    out[s.n] = advect_cell(nb_of(phi, s), nb_of(ux, s), nb_of(uy, s), nb_of(uz, s), dt);
 }
 
 __global__ void __launch_bounds__(128) k_fill_normals(const float* phi, float* g, ThermalGrid t) {
     Stencil s;
     if (!stencil(t, s)) return;
-    const float gx = half_diff(phi[s.xp], phi[s.xm]), gy = half_diff(phi[s.yp], phi[s.ym]),
-                gz = half_diff(phi[s.zp], phi[s.zm]);
-    const float mag = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)), __fmul_rn(gz, gz)));
-    const bool ok = mag > 1.0e-12F;
+    const float3 v = normal_cell(nb_of(phi, s));
     const std::size_t cells = t.cells;
-    g[s.n] = ok ? __fdiv_rn(gx, mag) : 0.0F;
-    g[cells + s.n] = ok ? __fdiv_rn(gy, mag) : 0.0F;
-    g[2U * cells + s.n] = ok ? __fdiv_rn(gz, mag) : 0.0F;
+    g[s.n] = v.x;
+    g[cells + s.n] = v.y;
+    g[2U * cells + s.n] = v.z;
 }
 
 __global__ void __launch_bounds__(128) k_fill_curvature(float* g, ThermalGrid t) {
     Stencil s;
     if (!stencil(t, s)) return;
     const std::size_t cells = t.cells;
-    const float* nx = g;
-    const float* ny = g + cells;
-    const float* nz = g + 2U * cells;
-    const float d = __fadd_rn(__fadd_rn(__fsub_rn(nx[s.xp], nx[s.xm]), __fsub_rn(ny[s.yp], ny[s.ym])),
-                              __fsub_rn(nz[s.zp], nz[s.zm]));
-    g[3U * cells + s.n] = __fmul_rn(-0.5F, d);
+    g[3U * cells + s.n] = curvature_cell(nb_of(g, s), nb_of(g + cells, s), nb_of(g + 2U * cells, s));
 }
 
 __global__ void __launch_bounds__(128) k_surface_tension(const float* phi, const float* curvature, ThermalGrid t,
@@ -101,12 +149,164 @@ __global__ void __launch_bounds__(128) k_surface_tension(const float* phi, const
                                                          float density) {
     Stencil s;
     if (!stencil(t, s)) return;
-    const float gx = half_diff(phi[s.xp], phi[s.xm]), gy = half_diff(phi[s.yp], phi[s.ym]),
-                gz = half_diff(phi[s.zp], phi[s.zm]);
-    const float c = __fdiv_rn(__fmul_rn(sigma, curvature[s.n]), density);
-    ax[s.n] = __fadd_rn(ax[s.n], __fmul_rn(c, gx));
-    ay[s.n] = __fadd_rn(ay[s.n], __fmul_rn(c, gy));
-    az[s.n] = __fadd_rn(az[s.n], __fmul_rn(c, gz));
+    const float3 d = tension_cell(nb_of(phi, s), curvature[s.n], sigma, density);
+    ax[s.n] = __fadd_rn(ax[s.n], d.x);
+    ay[s.n] = __fadd_rn(ay[s.n], d.y);
+    az[s.n] = __fadd_rn(az[s.n], d.z);
+}
+
+__global__ void __launch_bounds__(128) k_resident_q(const float* ux, const float* uy, const float* uz, ThermalGrid t,
+                                                    float* q) {
+    Stencil s;
+    if (!stencil(t, s)) return;
+    q[s.n] = q_cell(nb_of(ux, s), nb_of(uy, s), nb_of(uz, s));
+}
+
+// ---- four x-adjacent cells per thread (nx % 4 == 0, 16-byte aligned fields):
+// each row segment is one float4 load; the x neighbours of the segment's ends
+// are two scalar loads.  Same arithmetic as the one-cell kernels.
+struct Rows {
+    u32 c, yp, ym, zp, zm; // element offsets of the x0 of the five rows
+    u32 x0, xl, xr;        // x0, x0 - 1 and x0 + 4 (periodic)
+};
+
+__device__ __forceinline__ bool rows_of(const ThermalGrid& t, Rows& r) {
+    r.x0 = 4U * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (r.x0 >= t.nx) return false;
+    const u32 y = blockIdx.y, z = blockIdx.z;
+    r.c = at(r.x0, y, z, t);
+    r.yp = at(r.x0, shp(y, t.ny), z, t);
+    r.ym = at(r.x0, shm(y, t.ny), z, t);
+    r.zp = at(r.x0, y, shp(z, t.nz), t);
+    r.zm = at(r.x0, y, shm(z, t.nz), t);
+    r.xl = r.x0 == 0U ? t.nx - 1U : r.x0 - 1U;
+    r.xr = r.x0 + 4U == t.nx ? 0U : r.x0 + 4U;
+    return true;
+}
+
+__device__ __forceinline__ float4 ld4(const float* f, u32 off) { return *reinterpret_cast<const float4*>(f + off); }
+__device__ __forceinline__ void st4(float* f, u32 off, float4 v) { *reinterpret_cast<float4*>(f + off) = v; }
+__device__ __forceinline__ float lane(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+
+// The four cells' neighbourhoods of one field; X / YZ select which neighbours are loaded.
+template <bool X, bool YZ> struct Quad {
+    float4 c, yp, ym, zp, zm;
+    float xl, xr;
+    __device__ __forceinline__ Quad(const float* f, const Rows& r) {
+        c = ld4(f, r.c);
+        if constexpr (X) {
+            xl = f[r.c - r.x0 + r.xl];
+            xr = f[r.c - r.x0 + r.xr];
+        }
+        if constexpr (YZ) {
+            yp = ld4(f, r.yp);
+            ym = ld4(f, r.ym);
+            zp = ld4(f, r.zp);
+            zm = ld4(f, r.zm);
+        }
+    }
+    __device__ __forceinline__ Nb at(int k) const {
+        Nb n{};
+        n.c = lane(c, k);
+        if constexpr (X) {
+            n.xm = k == 0 ? xl : lane(c, k - 1);
+            n.xp = k == 3 ? xr : lane(c, k + 1);
+        }
+        if constexpr (YZ) {
+            n.yp = lane(yp, k);
+            n.ym = lane(ym, k);
+            n.zp = lane(zp, k);
+            n.zm = lane(zm, k);
+        }
+        return n;
+    }
+};
+
+__global__ void __launch_bounds__(128) k_fill_advect4(const float* phi, float* out, ThermalGrid t, const float* ux,
+                                                      const float* uy, const float* uz, float dt) {
+    Rows r;
+    if (!rows_of(t, r)) return;
+    const Quad<true, true> p(phi, r);
+    const Quad<true, false> u(ux, r);
+    const Nb v0{}; // uy / uz: only their y / z neighbours enter
+    const float4 vc = ld4(uy, r.c), vp = ld4(uy, r.yp), vm = ld4(uy, r.ym);
+    const float4 wc = ld4(uz, r.c), wp = ld4(uz, r.zp), wm = ld4(uz, r.zm);
+    float o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        Nb v = v0, w = v0;
+        v.c = lane(vc, k);
+        v.yp = lane(vp, k);
+        v.ym = lane(vm, k);
+        w.c = lane(wc, k);
+        w.zp = lane(wp, k);
+        w.zm = lane(wm, k);
+        o[k] = advect_cell(p.at(k), u.at(k), v, w, dt);
+    }
+    st4(out, r.c, make_float4(o[0], o[1], o[2], o[3]));
+}
+
+__global__ void __launch_bounds__(128) k_fill_normals4(const float* phi, float* g, ThermalGrid t) {
+    Rows r;
+    if (!rows_of(t, r)) return;
+    const Quad<true, true> p(phi, r);
+    float3 v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = normal_cell(p.at(k));
+    const std::size_t cells = t.cells;
+    st4(g, r.c, make_float4(v[0].x, v[1].x, v[2].x, v[3].x));
+    st4(g + cells, r.c, make_float4(v[0].y, v[1].y, v[2].y, v[3].y));
+    st4(g + 2U * cells, r.c, make_float4(v[0].z, v[1].z, v[2].z, v[3].z));
+}
+
+__global__ void __launch_bounds__(128) k_fill_curvature4(float* g, ThermalGrid t) {
+    Rows r;
+    if (!rows_of(t, r)) return;
+    const std::size_t cells = t.cells;
+    const Quad<true, false> nx(g, r);
+    const float4 yp = ld4(g + cells, r.yp), ym = ld4(g + cells, r.ym);
+    const float4 zp = ld4(g + 2U * cells, r.zp), zm = ld4(g + 2U * cells, r.zm);
+    float o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        Nb ny{}, nz{};
+        ny.yp = lane(yp, k);
+        ny.ym = lane(ym, k);
+        nz.zp = lane(zp, k);
+        nz.zm = lane(zm, k);
+        o[k] = curvature_cell(nx.at(k), ny, nz);
+    }
+    st4(g + 3U * cells, r.c, make_float4(o[0], o[1], o[2], o[3]));
+}
+
+__global__ void __launch_bounds__(128) k_surface_tension4(const float* phi, const float* curvature, ThermalGrid t,
+                                                          float* ax, float* ay, float* az, float sigma,
+                                                          float density) {
+    Rows r;
+    if (!rows_of(t, r)) return;
+    const Quad<true, true> p(phi, r);
+    const float4 kappa = ld4(curvature, r.c);
+    float4 a = ld4(ax, r.c), b = ld4(ay, r.c), c = ld4(az, r.c);
+    float3 d[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) d[k] = tension_cell(p.at(k), lane(kappa, k), sigma, density);
+    a = make_float4(__fadd_rn(a.x, d[0].x), __fadd_rn(a.y, d[1].x), __fadd_rn(a.z, d[2].x), __fadd_rn(a.w, d[3].x));
+    b = make_float4(__fadd_rn(b.x, d[0].y), __fadd_rn(b.y, d[1].y), __fadd_rn(b.z, d[2].y), __fadd_rn(b.w, d[3].y));
+    c = make_float4(__fadd_rn(c.x, d[0].z), __fadd_rn(c.y, d[1].z), __fadd_rn(c.z, d[2].z), __fadd_rn(c.w, d[3].z));
+    st4(ax, r.c, a);
+    st4(ay, r.c, b);
+    st4(az, r.c, c);
+}
+
+__global__ void __launch_bounds__(128) k_resident_q4(const float* ux, const float* uy, const float* uz, ThermalGrid t,
+                                                     float* q) {
+    Rows r;
+    if (!rows_of(t, r)) return;
+    const Quad<true, true> u(ux, r), v(uy, r), w(uz, r);
+    float o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = q_cell(u.at(k), v.at(k), w.at(k));
+    st4(q, r.c, make_float4(o[0], o[1], o[2], o[3]));
 }
 
 __global__ void __launch_bounds__(256) k_sum_floats(const float* v, std::size_t count, double* partials) {
@@ -217,31 +417,14 @@ __global__ void __launch_bounds__(128) k_particles(float* st, u32 count, Thermal
     st[5U * count + p] = vz;
 }
 
-__global__ void __launch_bounds__(128) k_resident_q(const float* ux, const float* uy, const float* uz, ThermalGrid t,
-                                                    float* q) {
-    Stencil s;
-    if (!stencil(t, s)) return;
-    const u32 P[3] = {s.xp, s.yp, s.zp}, M[3] = {s.xm, s.ym, s.zm};
-    float g[3][3];
-#pragma unroll
-    for (int axis = 0; axis < 3; ++axis) {
-        g[0][axis] = half_diff(ux[P[axis]], ux[M[axis]]);
-        g[1][axis] = half_diff(uy[P[axis]], uy[M[axis]]);
-        g[2][axis] = half_diff(uz[P[axis]], uz[M[axis]]);
-    }
-    float s2 = 0.0F, o2 = 0.0F;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const float sij = half_sum(g[i][j], g[j][i]), oij = half_diff(g[i][j], g[j][i]);
-            s2 = __fadd_rn(s2, __fmul_rn(sij, sij));
-            o2 = __fadd_rn(o2, __fmul_rn(oij, oij));
-        }
-    q[s.n] = __fmul_rn(0.5F, __fsub_rn(o2, s2));
-}
-
 dim3 cell_grid3(const ThermalGrid& t) { return dim3((t.nx + 127U) / 128U, t.ny, t.nz); }
+dim3 quad_grid(const ThermalGrid& t) { return dim3((t.nx / 4U + 127U) / 128U, t.ny, t.nz); }
+
+bool aligned16(const void* p) { return (reinterpret_cast<std::uintptr_t>(p) & 15U) == 0U; }
+// The four-cell kernels need whole float4 rows: nx % 4 == 0 and 16-byte aligned fields.
+template <class... P> bool quads(const ThermalGrid& t, P... fields) {
+    return t.nx % 4U == 0U && (aligned16(fields) && ...);
+}
 
 } // namespace
 
@@ -257,21 +440,34 @@ cudaError_t launch_fill_half_space_x(float* fill, ThermalGrid t, float interface
 
 cudaError_t launch_fill_advect(const float* fill, float* out, ThermalGrid t, const float* ux, const float* uy,
                                const float* uz, float dt, cudaStream_t s) {
-    k_fill_advect<<<cell_grid3(t), 128, 0, s>>>(fill, out, t, ux, uy, uz, dt);
+    if (quads(t, fill, out, ux, uy, uz))
+        k_fill_advect4<<<quad_grid(t), 128, 0, s>>>(fill, out, t, ux, uy, uz, dt);
+    else
+        k_fill_advect<<<cell_grid3(t), 128, 0, s>>>(fill, out, t, ux, uy, uz, dt);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fill_geometry(const float* fill, float* geometry, ThermalGrid t, cudaStream_t s) {
-    k_fill_normals<<<cell_grid3(t), 128, 0, s>>>(fill, geometry, t);
+    const bool q4 = quads(t, fill, geometry);
+    if (q4)
+        k_fill_normals4<<<quad_grid(t), 128, 0, s>>>(fill, geometry, t);
+    else
+        k_fill_normals<<<cell_grid3(t), 128, 0, s>>>(fill, geometry, t);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_fill_curvature<<<cell_grid3(t), 128, 0, s>>>(geometry, t);
+    if (q4)
+        k_fill_curvature4<<<quad_grid(t), 128, 0, s>>>(geometry, t);
+    else
+        k_fill_curvature<<<cell_grid3(t), 128, 0, s>>>(geometry, t);
     return cudaGetLastError();
 }
 
 cudaError_t launch_surface_tension(const float* fill, const float* curvature, ThermalGrid t, float* ax, float* ay,
                                    float* az, float sigma, float density, cudaStream_t s) {
-    k_surface_tension<<<cell_grid3(t), 128, 0, s>>>(fill, curvature, t, ax, ay, az, sigma, density);
+    if (quads(t, fill, curvature, ax, ay, az))
+        k_surface_tension4<<<quad_grid(t), 128, 0, s>>>(fill, curvature, t, ax, ay, az, sigma, density);
+    else
+        k_surface_tension<<<cell_grid3(t), 128, 0, s>>>(fill, curvature, t, ax, ay, az, sigma, density);
     return cudaGetLastError();
 }
 
@@ -295,7 +491,10 @@ cudaError_t launch_particles_advance(float* state, std::uint32_t count, ThermalG
 
 cudaError_t launch_resident_q(const float* ux, const float* uy, const float* uz, ThermalGrid t, float* q,
                               cudaStream_t s) {
-    k_resident_q<<<cell_grid3(t), 128, 0, s>>>(ux, uy, uz, t, q);
+    if (quads(t, ux, uy, uz, q))
+        k_resident_q4<<<quad_grid(t), 128, 0, s>>>(ux, uy, uz, t, q);
+    else
+        k_resident_q<<<cell_grid3(t), 128, 0, s>>>(ux, uy, uz, t, q);
     return cudaGetLastError();
 }
 

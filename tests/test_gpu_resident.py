@@ -44,11 +44,12 @@ def device_write(ptr, values):
     assert rt.cudaMemcpy(ptr, v.ctypes.data, v.nbytes, 1) == 0  # host to device
 
 
-def test_free_surface_matches_oracle_bitwise(engine, oracle_mod):
+@pytest.mark.parametrize("nx", [12, 14])  # four-cell kernels (nx % 4 == 0) and the one-cell fallback
+def test_free_surface_matches_oracle_bitwise(engine, oracle_mod, nx):
     from cfd_solvers_b200.multiphysics import ResidentFreeSurface3D
 
     cs = engine
-    nx, ny, nz = 12, 10, 8
+    ny, nz = 10, 8
     n = nx * ny * nz
     with cavity(cs, nx, ny, nz) as flow:
         with ResidentFreeSurface3D(flow) as fs:
@@ -140,11 +141,12 @@ def test_single_particle_spread_bitwise(engine, oracle_mod):
         assert np.array_equal(parts.download_records()[0, :6].astype(np.float32), st[:6, 0])
 
 
-def test_resident_q_matches_oracle(engine, oracle_mod):
+@pytest.mark.parametrize("nx", [12, 14])
+def test_resident_q_matches_oracle(engine, oracle_mod, nx):
     from cfd_solvers_b200.multiphysics import ResidentFlowDiagnostics3D
 
     cs = engine
-    nx, ny, nz = 12, 10, 8
+    ny, nz = 10, 8
     with cavity(cs, nx, ny, nz) as flow, ResidentFlowDiagnostics3D(flow) as diag:
         macro = flow.refresh_device_macroscopic()
         f = flow.compute_macroscopic()
