@@ -1169,7 +1169,7 @@ __global__ void __launch_bounds__(128) k_init(const __grid_constant__ LbmArgs a,
 
 // Macroscopic fields rho and u + a/2 (reference esoteric_pull.hpp:180-209 and
 // esoteric_pull_sycl.hpp:229-307); wall cells report rho = 0, u = 0.
-template <class L, class S, bool FLAGS, class OutT>
+template <class L, class S, bool FLAGS, class OutT, bool NARROW = false>
 __global__ void __launch_bounds__(128) k_macro(const __grid_constant__ LbmArgs a, OutT* rho_out, OutT* ux_out,
                                                OutT* uy_out, OutT* uz_out) {
     using R = typename S::R;
@@ -1190,7 +1190,9 @@ __global__ void __launch_bounds__(128) k_macro(const __grid_constant__ LbmArgs a
         }
     }
     R fin[L::Q];
-    gather<L, S, FLAGS>(a, n, make_nbr(a, x, y, z), flag, fin);
+    const Nbr o = make_nbr(a, x, y, z);
+    gather_loads<L, S, FLAGS, NARROW>(a, n, o, flag, fin);
+    gather_fixup<L, S, FLAGS>(a, n, o, flag, fin);
     R rho, ux, uy, uz, ax, ay, az;
     moments<L, R, S::delta>(fin, rho, ux, uy, uz);
     cell_acceleration<R>(a, n, ax, ay, az);

@@ -2,6 +2,8 @@
 // one storage type.  Included by lbm_kernels_{f32,f16s,f64}.cu only.
 #pragma once
 
+#include <type_traits>
+
 #include "lbm_adjoint.cuh"
 #include "lbm_device.cuh"
 #include "lbm_launch.h"
@@ -108,21 +110,26 @@ cudaError_t Launcher<STORAGE>::macro(const KernelKey& k, const LbmArgs& a, void*
     using S = typename StorageOf<STORAGE>::type;
     return with_lattice(k.q, [&](auto lat) {
         using L = decltype(lat);
-        if (out_f64) {
-            auto r = static_cast<double*>(rho), x = static_cast<double*>(ux), y = static_cast<double*>(uy),
-                 z = static_cast<double*>(uz);
-            if (k.flags)
-                k_macro<L, S, true, double><<<g, b, 0, s>>>(a, r, x, y, z);
-            else
-                k_macro<L, S, false, double><<<g, b, 0, s>>>(a, r, x, y, z);
-        } else {
-            auto r = static_cast<float*>(rho), x = static_cast<float*>(ux), y = static_cast<float*>(uy),
-                 z = static_cast<float*>(uz);
-            if (k.flags)
-                k_macro<L, S, true, float><<<g, b, 0, s>>>(a, r, x, y, z);
-            else
-                k_macro<L, S, false, float><<<g, b, 0, s>>>(a, r, x, y, z);
-        }
+        // 32-bit slot offsets (as the step) whenever q * cells < 2^32
+        const auto run = [&](auto* r, auto* x, auto* y, auto* z) {
+            using O = std::remove_pointer_t<decltype(r)>;
+            if (k.narrow) {
+                if (k.flags)
+                    k_macro<L, S, true, O, true><<<g, b, 0, s>>>(a, r, x, y, z);
+                else
+                    k_macro<L, S, false, O, true><<<g, b, 0, s>>>(a, r, x, y, z);
+            } else {
+                if (k.flags)
+                    k_macro<L, S, true, O, false><<<g, b, 0, s>>>(a, r, x, y, z);
+                else
+                    k_macro<L, S, false, O, false><<<g, b, 0, s>>>(a, r, x, y, z);
+            }
+        };
+        if (out_f64)
+            run(static_cast<double*>(rho), static_cast<double*>(ux), static_cast<double*>(uy),
+                static_cast<double*>(uz));
+        else
+            run(static_cast<float*>(rho), static_cast<float*>(ux), static_cast<float*>(uy), static_cast<float*>(uz));
         return cudaGetLastError();
     });
 }
