@@ -2085,8 +2085,10 @@ CFDX_API int cfdx_thermal_add_boussinesq(cfdx_thermal* t, float* ax, float* ay, 
         require(std::isfinite(t_ref) && std::isfinite(beta) && std::isfinite(gx) && std::isfinite(gy) &&
                     std::isfinite(gz),
                 "invalid resident Boussinesq coupling");
-        const float* temperature = thermal_scalar(t);
-        check_cuda(launch_boussinesq(temperature, t->grid, ax, ay, az, t_ref, beta, gx, gy, gz, t->flow->stream),
+        if (!t->scalar)
+            t->scalar = static_cast<float*>(device_alloc(t->grid.cells * sizeof(float), "temperature scratch"));
+        check_cuda(launch_thermal_boussinesq(t->g, t->grid, t->scalar, ax, ay, az, t_ref, beta, gx, gy, gz,
+                                             t->flow->stream),
                    "Boussinesq kernel");
     });
 }

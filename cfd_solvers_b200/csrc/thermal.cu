@@ -70,12 +70,19 @@ __global__ void __launch_bounds__(256) k_thermal_scalar(const float* g, ThermalG
     temperature[n] = v;
 }
 
-__global__ void __launch_bounds__(256) k_boussinesq(const float* temperature, ThermalGrid t, float* ax, float* ay,
-                                                    float* az, float t_ref, float beta, float gx, float gy,
-                                                    float gz) {
+// The temperature (as k_thermal_scalar) and the Boussinesq term in one pass:
+// the temperature is written (the device scalar field) and used without
+// being read back.
+__global__ void __launch_bounds__(256) k_thermal_boussinesq(const float* g, ThermalGrid t, float* temperature,
+                                                            float* ax, float* ay, float* az, float t_ref, float beta,
+                                                            float gx, float gy, float gz) {
     const std::uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= t.cells) return;
-    const float scale = __fmul_rn(-beta, __fsub_rn(temperature[n], t_ref));
+    float v = 0.0F;
+#pragma unroll
+    for (int d = 0; d < 7; ++d) v = __fadd_rn(v, g[std::size_t(d) * t.cells + n]);
+    temperature[n] = v;
+    const float scale = __fmul_rn(-beta, __fsub_rn(v, t_ref));
     ax[n] = __fadd_rn(ax[n], __fmul_rn(scale, gx));
     ay[n] = __fadd_rn(ay[n], __fmul_rn(scale, gy));
     az[n] = __fadd_rn(az[n], __fmul_rn(scale, gz));
@@ -135,9 +142,10 @@ cudaError_t launch_thermal_scalar(const float* g, ThermalGrid t, float* temperat
     return cudaGetLastError();
 }
 
-cudaError_t launch_boussinesq(const float* temperature, ThermalGrid t, float* ax, float* ay, float* az, float t_ref,
-                              float beta, float gx, float gy, float gz, cudaStream_t s) {
-    k_boussinesq<<<blocks_for(t.cells), 256, 0, s>>>(temperature, t, ax, ay, az, t_ref, beta, gx, gy, gz);
+cudaError_t launch_thermal_boussinesq(const float* g, ThermalGrid t, float* temperature, float* ax, float* ay,
+                                     float* az, float t_ref, float beta, float gx, float gy, float gz,
+                                     cudaStream_t s) {
+    k_thermal_boussinesq<<<blocks_for(t.cells), 256, 0, s>>>(g, t, temperature, ax, ay, az, t_ref, beta, gx, gy, gz);
     return cudaGetLastError();
 }
 

@@ -23,9 +23,10 @@ cudaError_t launch_thermal_step(const float* in, float* out, ThermalGrid t, cons
                                 const float* uz, float omega, cudaStream_t s);
 // temperature[n] = sum_d g[d][n].
 cudaError_t launch_thermal_scalar(const float* g, ThermalGrid t, float* temperature, cudaStream_t s);
-// a += -beta (T - t_ref) * gravity per cell.
-cudaError_t launch_boussinesq(const float* temperature, ThermalGrid t, float* ax, float* ay, float* az, float t_ref,
-                              float beta, float gx, float gy, float gz, cudaStream_t s);
+// temperature = sum_d g[d] (written), then a += -beta (T - t_ref) * gravity, in one pass.
+cudaError_t launch_thermal_boussinesq(const float* g, ThermalGrid t, float* temperature, float* ax, float* ay,
+                                     float* az, float t_ref, float beta, float gx, float gy, float gz,
+                                     cudaStream_t s);
 // FP64 sum of the 7 * cells populations into out[0] (partials: `blocks` doubles of scratch).
 cudaError_t launch_thermal_total(const float* g, ThermalGrid t, double* partials, int blocks, double* out,
                                  cudaStream_t s);
