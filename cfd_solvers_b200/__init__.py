@@ -15,6 +15,7 @@ from .lbm import (
     InPlaceLbmConfig,
     MacroscopicFields,
     cavity_flags,
+    release_scratch,
     smagorinsky_k,
     trt_tau_minus,
 )
@@ -34,6 +35,7 @@ __all__ = [
     "InPlaceLbmConfig",
     "MacroscopicFields",
     "cavity_flags",
+    "release_scratch",
     "smagorinsky_k",
     "trt_tau_minus",
     "DistributedEsotericPullSolver",

@@ -213,6 +213,7 @@ SIGNATURES = {
     "cfdx_diagnostics_info": (_i, [_vp, ctypes.POINTER(_sz)]),
     "cfdx_lbm_debug_slot_audit": (_i, [_H, _i, ctypes.POINTER(cfdx_slot_audit)]),
     "cfdx_debug_audit_classify": (_i, [ctypes.c_uint32] * 5 + [ctypes.POINTER(ctypes.c_uint)]),
+    "cfdx_release_scratch": (_i, [_i]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
 }
 

@@ -26,6 +26,7 @@
 #include "voxelize.h"
 #include "export.h"
 #include "resident.h"
+#include "scratch_pool.h"
 #include "slot_audit.h"
 #include "thermal.h"
 
@@ -1195,10 +1196,10 @@ CFDX_API int cfdx_lbm_macroscopic_f64(cfdx_lbm* h, double* rho, double* ux, doub
             h->d2h += 4U * bytes;
             h->sync();
         } catch (...) {
-            device_free(s);
+            scratch_free(s, h->stream);
             throw;
         }
-        device_free(s);
+        scratch_free(s, h->stream);
     });
 }
 
@@ -1872,7 +1873,9 @@ CFDX_API int cfdx_q_criterion(const double* velocity, std::size_t nx, std::size_
             const double* u = velocity;
             double* out = q;
             if (where == CFDX_HOST) {
-                staging = static_cast<double*>(device_alloc(4 * n * sizeof(double), "Q-criterion staging"));
+                void* p = nullptr;
+                check_cuda(scratch_alloc(&p, 4 * n * sizeof(double), s), "Q-criterion staging");
+                staging = static_cast<double*>(p);
                 check_cuda(cudaMemcpyAsync(staging, velocity, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s),
                            "cudaMemcpyAsync (velocity)");
                 u = staging;
@@ -1885,11 +1888,11 @@ CFDX_API int cfdx_q_criterion(const double* velocity, std::size_t nx, std::size_
                            "cudaMemcpyAsync (Q)");
             check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
         } catch (...) {
-            device_free(staging);
+            scratch_free(staging, s);
             cudaStreamDestroy(s);
             throw;
         }
-        device_free(staging);
+        scratch_free(staging, s);
         cudaStreamDestroy(s);
     });
 }
@@ -1903,8 +1906,10 @@ CFDX_API int cfdx_lbm_q_criterion(cfdx_lbm* h, double dx, double dy, double dz, 
         require(where == CFDX_HOST || where == CFDX_DEVICE, "where must be CFDX_HOST or CFDX_DEVICE");
         const std::size_t n = h->N;
         // rho | ux | uy | uz as cfdx_lbm_macroscopic_f64 reports them, then Q
-        double* s = static_cast<double*>(device_alloc((where == CFDX_HOST ? 5 : 4) * n * sizeof(double),
-                                                      "Q-criterion staging"));
+        void* p = nullptr;
+        check_cuda(scratch_alloc(&p, (where == CFDX_HOST ? 5 : 4) * n * sizeof(double), h->stream),
+                   "Q-criterion staging");
+        double* s = static_cast<double*>(p);
         try {
             check_cuda(launch_macro(h->key, h->args(), s, s + n, s + 2 * n, s + 3 * n, true, h->grid(), h->block(),
                                     h->stream),
@@ -2544,6 +2549,18 @@ CFDX_API int cfdx_debug_audit_classify(uint32_t reads, uint32_t writes, uint32_t
     return guarded([&] {
         require(classes != nullptr, "null output");
         *classes = audit_classify(reads, writes, lowest_reader, highest_reader, writer);
+    });
+}
+
+CFDX_API int cfdx_release_scratch(int device) {
+    return guarded([&] {
+        int devices = 0;
+        if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+            fail(CFDX_ERR_CUDA, "no CUDA device is available (the B200 engine has no CPU fallback)");
+        require(device >= 0 && device < devices, "device ordinal out of range");
+        check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        check_cuda(scratch_release(device), "cudaMemPoolTrimTo");
     });
 }
 

@@ -25,8 +25,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
-#include <mutex>
 
+#include "scratch_pool.h"
 #include "voxelize.h"
 
 namespace cfdx {
@@ -172,44 +172,8 @@ __global__ void __launch_bounds__(128) k_vox_cells(const Tri* tris, Grid g, cons
     out[n] = (hits & 1U) ? value : (base ? base[n] : std::uint8_t(0));
 }
 
-// Scratch of a call comes from a memory pool the library keeps per device
-// (stream-ordered cudaMallocFromPoolAsync / cudaFreeAsync), so repeated calls
-// -- a moving body re-voxelized every few steps -- reuse memory instead of
-// mapping it anew and synchronising the device in cudaFree each time.  The
-// pool keeps up to kScratchKeep bytes between calls (a 512^3 grid with 3e5
-// triangles uses about 70 MB).
-constexpr std::uint64_t kScratchKeep = 1ULL << 30;
-constexpr int kMaxDevices = 64;
-
-cudaError_t scratch_pool(cudaMemPool_t* pool) {
-    static std::mutex guard;
-    static cudaMemPool_t pools[kMaxDevices] = {};
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess) return e;
-    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-    const std::lock_guard<std::mutex> lock(guard);
-    if (!pools[device]) {
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = device;
-        cudaMemPool_t created = nullptr;
-        e = cudaMemPoolCreate(&created, &props);
-        if (e != cudaSuccess) return e;
-        std::uint64_t keep = kScratchKeep;
-        e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep);
-        if (e != cudaSuccess) {
-            cudaMemPoolDestroy(created);
-            return e;
-        }
-        pools[device] = created;
-    }
-    *pool = pools[device];
-    return cudaSuccess;
-}
-
-// Pool memory released on the call's stream when the buffer goes out of scope.
+// Scratch from the library's per-device pool (scratch_pool.cu), released on
+// the call's stream when the buffer goes out of scope.
 struct DeviceBuffer {
     void* p = nullptr;
     cudaStream_t s = nullptr;
@@ -217,14 +181,9 @@ struct DeviceBuffer {
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
     ~DeviceBuffer() {
-        if (p) cudaFreeAsync(p, s);
+        scratch_free(p, s);
     }
-    cudaError_t alloc(std::size_t bytes) {
-        cudaMemPool_t pool = nullptr;
-        const cudaError_t e = scratch_pool(&pool);
-        if (e != cudaSuccess) return e;
-        return cudaMallocFromPoolAsync(&p, std::max<std::size_t>(bytes, 16), pool, s);
-    }
+    cudaError_t alloc(std::size_t bytes) { return scratch_alloc(&p, bytes, s); }
 };
 
 } // namespace

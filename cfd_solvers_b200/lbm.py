@@ -538,6 +538,14 @@ class EsotericPullCudaSolver:
         return self._lib
 
 
+def release_scratch(device: int = 0, library=None):
+    """Return the unused memory of the library's per-device scratch pool to the driver
+    (cfdx_release_scratch).  The voxelizer and the Q-criterion take their temporary buffers from
+    that pool, which keeps up to 8 GiB mapped between calls."""
+    lib = library or B.load()
+    lib.call("cfdx_release_scratch", int(device))
+
+
 def smagorinsky_k(cs: float) -> float:
     """Smagorinsky coefficient K = 18 sqrt(2) Cs^2 of tau_eff = (tau + sqrt(tau^2 + K sqrt(Q)/rho)) / 2."""
     return 18.0 * math.sqrt(2.0) * cs * cs

@@ -550,6 +550,14 @@ CFDX_API int cfdx_diagnostics_q_criterion(cfdx_diagnostics* diagnostics, const f
                                           const float* uz, float** q);
 CFDX_API int cfdx_diagnostics_info(cfdx_diagnostics* diagnostics, size_t* resident_bytes);
 
+/* Temporary buffers of single calls (cfdx_voxelize / cfdx_lbm_set_flags_surface
+ * scratch, cfdx_q_criterion / cfdx_lbm_q_criterion staging) come from a
+ * stream-ordered memory pool the library keeps per device, which keeps up to
+ * 8 GiB mapped between calls so that repeated calls do not map memory anew or
+ * synchronise the device in cudaFree.  This returns the pool's unused memory on
+ * `device` to the driver (after synchronising the device). */
+CFDX_API int cfdx_release_scratch(int device);
+
 /* ---- Slot-ownership audit (a test hook standing in for a race detector).
  * In-place streaming is race-free because, within a step, every population
  * slot is loaded and then stored by exactly one cell.  The audit runs the

@@ -102,3 +102,15 @@ def test_cli_json_record(case):
         assert key in rec
     assert rec["schema"] == "cfd_solvers.benchmark.v1" and rec["backend"] == "cuda" and rec["q"] == 19
     assert rec["mlups"] > 0 and rec["mass_error_rel"] < 1e-3
+
+
+def test_release_scratch_without_device_fails_loudly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    import cfd_solvers_b200 as cs
+    from cfd_solvers_b200.bindings import CudaError
+
+    with pytest.raises(CudaError):
+        cs.release_scratch(0)

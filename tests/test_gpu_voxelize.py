@@ -161,3 +161,27 @@ def test_slabs_voxelize_their_own_planes(engine):
     finally:
         for s in ss:
             s.close()
+
+
+def test_repeated_calls_reuse_scratch_and_release(engine):
+    """The voxelizer's and the Q-criterion's temporary buffers come from the library's per-device
+    pool: repeated calls give the same mask, and release_scratch hands the pool's memory back
+    without disturbing later calls."""
+    from cfd_solvers_b200 import geometry as G
+
+    cs = engine
+    t = G.icosphere((0.5, 0.5, 0.5), 0.3, 3)
+    grid = G.VoxelGrid3D(48, 40, 32)
+    first = G.voxelize_surface(t, grid)
+    for _ in range(4):
+        assert np.array_equal(G.voxelize_surface(t, grid), first)
+    cs.release_scratch(0)
+    assert np.array_equal(G.voxelize_surface(t, grid), first)
+    with cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(nx=24, ny=20, nz=16, tau=0.7)) as s:
+        s.initialize_taylor_green(0.03)
+        s.step(3)
+        q0 = s.q_criterion()
+        cs.release_scratch(0)
+        assert np.array_equal(s.q_criterion(), q0)
+    with pytest.raises(ValueError):
+        cs.release_scratch(1 << 20)
