@@ -86,6 +86,11 @@ __device__ __forceinline__ float3 tension_cell(const Nb& p, float kappa, float s
     return make_float3(__fmul_rn(c, gx), __fmul_rn(c, gy), __fmul_rn(c, gz));
 }
 
+// Q = (|Omega|^2 - |S|^2) / 2 with the sums over (i, j) in row order, as the
+// reference adds them.  Terms that are equal in IEEE arithmetic are computed
+// once: s_ji = s_ij (addition commutes), o_ji = -o_ij (so o_ji^2 = o_ij^2),
+// s_ii = g_ii (0.5 (a + a) = a) and o_ii = +0, whose square adds nothing to the
+// non-negative o2.  The result is bit for bit the nine-term loop's.
 __device__ __forceinline__ float q_cell(const Nb& ux, const Nb& uy, const Nb& uz) {
     const Nb* u[3] = {&ux, &uy, &uz};
     float g[3][3];
@@ -95,14 +100,24 @@ __device__ __forceinline__ float q_cell(const Nb& ux, const Nb& uy, const Nb& uz
         g[i][1] = half_diff(u[i]->yp, u[i]->ym);
         g[i][2] = half_diff(u[i]->zp, u[i]->zm);
     }
+    float ss[3][3], oo[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        ss[i][i] = __fmul_rn(g[i][i], g[i][i]);
+#pragma unroll
+        for (int j = i + 1; j < 3; ++j) {
+            const float sij = half_sum(g[i][j], g[j][i]), oij = half_diff(g[i][j], g[j][i]);
+            ss[i][j] = ss[j][i] = __fmul_rn(sij, sij);
+            oo[i][j] = oo[j][i] = __fmul_rn(oij, oij);
+        }
+    }
     float s2 = 0.0F, o2 = 0.0F;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const float sij = half_sum(g[i][j], g[j][i]), oij = half_diff(g[i][j], g[j][i]);
-            s2 = __fadd_rn(s2, __fmul_rn(sij, sij));
-            o2 = __fadd_rn(o2, __fmul_rn(oij, oij));
+            s2 = __fadd_rn(s2, ss[i][j]);
+            if (i != j) o2 = __fadd_rn(o2, oo[i][j]);
         }
     return __fmul_rn(0.5F, __fsub_rn(o2, s2));
 }
@@ -298,15 +313,73 @@ __global__ void __launch_bounds__(128) k_surface_tension4(const float* phi, cons
     st4(az, r.c, c);
 }
 
-__global__ void __launch_bounds__(128) k_resident_q4(const float* ux, const float* uy, const float* uz, ThermalGrid t,
-                                                     float* q) {
-    Rows r;
-    if (!rows_of(t, r)) return;
-    const Quad<true, true> u(ux, r), v(uy, r), w(uz, r);
-    float o[4];
+// The Q-criterion needs all six neighbours of three fields.  A thread takes
+// four x-adjacent cells through kQPlanes z-planes, carrying each field's rows
+// z-1, z and z+1 in registers: per plane it loads the z+1 row, the two y
+// neighbour rows and the segment's two x-edge values instead of the five rows
+// of the one-plane form.
+constexpr u32 kQPlanes = 8U;
+
+struct QColumn {
+    float4 below, cur, above; // rows z-1, z, z+1 of the segment
+    float xl, xr;             // row z at x0 - 1 and x0 + 4
+};
+
+__device__ __forceinline__ Nb q_nb(const QColumn& col, float4 yp, float4 ym, int k) {
+    Nb n;
+    n.c = lane(col.cur, k);
+    n.xm = k == 0 ? col.xl : lane(col.cur, k - 1);
+    n.xp = k == 3 ? col.xr : lane(col.cur, k + 1);
+    n.yp = lane(yp, k);
+    n.ym = lane(ym, k);
+    n.zp = lane(col.above, k);
+    n.zm = lane(col.below, k);
+    return n;
+}
+
+__global__ void __launch_bounds__(128) k_resident_q4z(const float* ux, const float* uy, const float* uz, ThermalGrid t,
+                                                      float* q) {
+    const u32 x0 = 4U * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (x0 >= t.nx) return;
+    const u32 y = blockIdx.y, z0 = blockIdx.z * kQPlanes;
+    const u32 z_end = min(z0 + kQPlanes, t.nz);
+    const u32 yp = shp(y, t.ny), ym = shm(y, t.ny);
+    const u32 xl = x0 == 0U ? t.nx - 1U : x0 - 1U, xr = x0 + 4U == t.nx ? 0U : x0 + 4U;
+    const float* f[3] = {ux, uy, uz};
+    QColumn col[3];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) o[k] = q_cell(u.at(k), v.at(k), w.at(k));
-    st4(q, r.c, make_float4(o[0], o[1], o[2], o[3]));
+    for (int c = 0; c < 3; ++c) {
+        col[c].below = ld4(f[c], at(x0, y, shm(z0, t.nz), t));
+        col[c].cur = ld4(f[c], at(x0, y, z0, t));
+        col[c].above = ld4(f[c], at(x0, y, shp(z0, t.nz), t));
+        col[c].xl = f[c][at(xl, y, z0, t)];
+        col[c].xr = f[c][at(xr, y, z0, t)];
+    }
+    for (u32 z = z0; z < z_end; ++z) {
+        float4 yps[3], yms[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            yps[c] = ld4(f[c], at(x0, yp, z, t));
+            yms[c] = ld4(f[c], at(x0, ym, z, t));
+        }
+        float o[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            o[k] = q_cell(q_nb(col[0], yps[0], yms[0], k), q_nb(col[1], yps[1], yms[1], k),
+                          q_nb(col[2], yps[2], yms[2], k));
+        st4(q, at(x0, y, z, t), make_float4(o[0], o[1], o[2], o[3]));
+        if (z + 1U < z_end) {
+            const u32 zn = z + 1U, znp = shp(zn, t.nz);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                col[c].below = col[c].cur;
+                col[c].cur = col[c].above;
+                col[c].above = ld4(f[c], at(x0, y, znp, t));
+                col[c].xl = f[c][at(xl, y, zn, t)];
+                col[c].xr = f[c][at(xr, y, zn, t)];
+            }
+        }
+    }
 }
 
 __global__ void __launch_bounds__(256) k_sum_floats(const float* v, std::size_t count, double* partials) {
@@ -492,7 +565,8 @@ cudaError_t launch_particles_advance(float* state, std::uint32_t count, ThermalG
 cudaError_t launch_resident_q(const float* ux, const float* uy, const float* uz, ThermalGrid t, float* q,
                               cudaStream_t s) {
     if (quads(t, ux, uy, uz, q))
-        k_resident_q4<<<quad_grid(t), 128, 0, s>>>(ux, uy, uz, t, q);
+        k_resident_q4z<<<dim3((t.nx / 4U + 127U) / 128U, t.ny, (t.nz + kQPlanes - 1U) / kQPlanes), 128, 0, s>>>(
+            ux, uy, uz, t, q);
     else
         k_resident_q<<<cell_grid3(t), 128, 0, s>>>(ux, uy, uz, t, q);
     return cudaGetLastError();

@@ -146,7 +146,7 @@ def test_resident_q_matches_oracle(engine, oracle_mod, nx):
     from cfd_solvers_b200.multiphysics import ResidentFlowDiagnostics3D
 
     cs = engine
-    ny, nz = 10, 8
+    ny, nz = 10, 19  # z-marching kernel: chunks of 8 planes, the last one partial
     with cavity(cs, nx, ny, nz) as flow, ResidentFlowDiagnostics3D(flow) as diag:
         macro = flow.refresh_device_macroscopic()
         f = flow.compute_macroscopic()
