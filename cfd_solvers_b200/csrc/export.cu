@@ -84,12 +84,27 @@ template <class T> __device__ __forceinline__ double load_d(const void* p, std::
     return double(static_cast<const T*>(p)[i]);
 }
 
+// Divisor 2 d of one axis.  When it is a power of two, x / (2 d) and
+// x * (1 / (2 d)) are correctly rounded values of the same real number, so the
+// kernel multiplies (one instruction instead of a division sequence).
+struct Spacing {
+    double d2, inv;
+    int pow2;
+};
+
+__device__ __forceinline__ double by_spacing(double x, const Spacing& s) {
+    return s.pow2 ? __dmul_rn(x, s.inv) : __ddiv_rn(x, s.d2);
+}
+
 // The reference's central-difference gradient and Q = (|Omega|^2 - |S|^2)/2,
 // operand for operand in FP64 without contraction; the outer layer of the grid is 0.
+// Terms that are equal in IEEE arithmetic are computed once (s_ji = s_ij,
+// o_ji^2 = o_ij^2, s_ii = g_ii, o_ii = +0 adds nothing), with the reference's
+// order of additions kept, so the result is the nine-term loop's bit for bit.
 template <class T>
 __global__ void __launch_bounds__(128) k_q_criterion(const void* ux, const void* uy, const void* uz,
                                                      std::size_t stride, std::uint32_t nx, std::uint32_t ny,
-                                                     std::uint32_t nz, double dx2, double dy2, double dz2, double* q) {
+                                                     std::uint32_t nz, Spacing hx, Spacing hy, Spacing hz, double* q) {
     const std::uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
     if (x >= nx) return;
     const std::size_t n = (std::size_t(z) * ny + y) * nx + x;
@@ -102,21 +117,41 @@ __global__ void __launch_bounds__(128) k_q_criterion(const void* ux, const void*
     double g[3][3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        g[c][0] = __ddiv_rn(__dsub_rn(load_d<T>(u[c], (n + sx) * stride), load_d<T>(u[c], (n - sx) * stride)), dx2);
-        g[c][1] = __ddiv_rn(__dsub_rn(load_d<T>(u[c], (n + sy) * stride), load_d<T>(u[c], (n - sy) * stride)), dy2);
-        g[c][2] = __ddiv_rn(__dsub_rn(load_d<T>(u[c], (n + sz) * stride), load_d<T>(u[c], (n - sz) * stride)), dz2);
+        g[c][0] = by_spacing(__dsub_rn(load_d<T>(u[c], (n + sx) * stride), load_d<T>(u[c], (n - sx) * stride)), hx);
+        g[c][1] = by_spacing(__dsub_rn(load_d<T>(u[c], (n + sy) * stride), load_d<T>(u[c], (n - sy) * stride)), hy);
+        g[c][2] = by_spacing(__dsub_rn(load_d<T>(u[c], (n + sz) * stride), load_d<T>(u[c], (n - sz) * stride)), hz);
+    }
+    double ss[3][3], oo[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        ss[i][i] = __dmul_rn(g[i][i], g[i][i]);
+#pragma unroll
+        for (int j = i + 1; j < 3; ++j) {
+            const double sij = __dmul_rn(0.5, __dadd_rn(g[i][j], g[j][i]));
+            const double oij = __dmul_rn(0.5, __dsub_rn(g[i][j], g[j][i]));
+            ss[i][j] = ss[j][i] = __dmul_rn(sij, sij);
+            oo[i][j] = oo[j][i] = __dmul_rn(oij, oij);
+        }
     }
     double s2 = 0.0, o2 = 0.0;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const double sij = __dmul_rn(0.5, __dadd_rn(g[i][j], g[j][i]));
-            const double oij = __dmul_rn(0.5, __dsub_rn(g[i][j], g[j][i]));
-            s2 = __dadd_rn(s2, __dmul_rn(sij, sij));
-            o2 = __dadd_rn(o2, __dmul_rn(oij, oij));
+            s2 = __dadd_rn(s2, ss[i][j]);
+            if (i != j) o2 = __dadd_rn(o2, oo[i][j]);
         }
     q[n] = __dmul_rn(0.5, __dsub_rn(o2, s2));
+}
+
+Spacing spacing(double d) {
+    Spacing s{2 * d, 0.0, 0}; // 2 * d as the reference writes it: exact for every finite d
+    int e = 0;
+    if (std::isfinite(s.d2) && s.d2 > 0.0 && std::frexp(s.d2, &e) == 0.5) {
+        s.inv = std::ldexp(1.0, 1 - e); // 2 d = 2^(e-1)
+        s.pow2 = std::isnormal(s.inv) ? 1 : 0;
+    }
+    return s;
 }
 
 } // namespace
@@ -198,13 +233,13 @@ cudaError_t launch_q_criterion(const void* ux, const void* uy, const void* uz, b
                                std::size_t nx, std::size_t ny, std::size_t nz, double dx, double dy, double dz,
                                double* q, cudaStream_t s) {
     const dim3 grid(static_cast<unsigned>((nx + 127) / 128), static_cast<unsigned>(ny), static_cast<unsigned>(nz));
-    // 2 * d as the reference writes it: exact for every finite d
+    const Spacing hx = spacing(dx), hy = spacing(dy), hz = spacing(dz);
     if (f64)
         k_q_criterion<double><<<grid, 128, 0, s>>>(ux, uy, uz, stride, std::uint32_t(nx), std::uint32_t(ny),
-                                                   std::uint32_t(nz), 2 * dx, 2 * dy, 2 * dz, q);
+                                                   std::uint32_t(nz), hx, hy, hz, q);
     else
         k_q_criterion<float><<<grid, 128, 0, s>>>(ux, uy, uz, stride, std::uint32_t(nx), std::uint32_t(ny),
-                                                  std::uint32_t(nz), 2 * dx, 2 * dy, 2 * dz, q);
+                                                  std::uint32_t(nz), hx, hy, hz, q);
     return cudaGetLastError();
 }
 

@@ -36,6 +36,18 @@ def test_q_matches_reference(engine):
         E.q_criterion_3d(2, 6, 5, np.zeros((60, 3)))
 
 
+@pytest.mark.parametrize("spacing", [(1.0, 0.5, 2.0), (0.3, 0.7, 1.1), (1.0, 0.3, 0.125)])
+def test_q_spacings_match_oracle(engine, oracle_mod, spacing):
+    """Power-of-two spacings take the multiply path, others the division path (mixed in the last
+    case); both equal the FP64 restatement of the reference's q_criterion_3d bit for bit."""
+    from cfd_solvers_b200 import export as E
+
+    nx, ny, nz = 11, 9, 8
+    v = np.random.default_rng(4).normal(0, 0.05, (nx * ny * nz, 3))
+    q = E.q_criterion_3d(nx, ny, nz, v, *spacing)
+    assert np.array_equal(q, oracle_mod.q_criterion(v, nx, ny, nz, *spacing))
+
+
 def run_solver(cs, storage, lattice):
     cfg = cs.InPlaceLbmConfig(nx=14, ny=12, nz=10, tau=0.6, storage=storage, lattice=lattice, collision="trt",
                               acceleration_x=1e-4)
