@@ -784,16 +784,22 @@ def slab_main(args, torch, cs, rank, world, local_rank):
     e2e = None
     if not args.no_e2e:
         flags_host = torch.from_numpy(local_flags).pin_memory()
+        d = build()  # the solver is created outside the timed job, as in the single-GPU e2e
+        # rho/u of the local planes (ghosts included) into pinned host memory through the C ABI, as
+        # the single-GPU e2e downloads; the rank's own planes are a contiguous range of them
+        out = [torch.empty(d.solver.cells(), dtype=torch.float32).pin_memory() for _ in range(4)]
+        lib = d.solver.library
+        d.solver.wait()
         dist.barrier()
         t0 = time.perf_counter()
-        d = build()
         try:
-            d.solver.library.check(d.solver.library.raw.cfdx_lbm_set_flags(
-                d.solver.handle, ctypes.c_void_p(flags_host.data_ptr()), cs.bindings.HOST))
+            lib.check(lib.raw.cfdx_lbm_set_flags(d.solver.handle, ctypes.c_void_p(flags_host.data_ptr()),
+                                                 cs.bindings.HOST))
             d.set_wall_velocity(2, 0.1, 0.0, 0.0)
             d.initialize_uniform()
             d.step(args.steps)
-            d.compute_macroscopic()
+            lib.check(lib.raw.cfdx_lbm_macroscopic(d.solver.handle, *[ctypes.c_void_p(o.data_ptr()) for o in out],
+                                                   cs.bindings.HOST))
             d.reduce()
             t1 = time.perf_counter()
             stats = d.solver.transfer_stats()
