@@ -1044,11 +1044,12 @@ std::uint64_t step_graphs(cfdx_lbm* h, LbmArgs& a, dim3 g, dim3 b, std::uint64_t
     }
     cudaGraph_t graph = nullptr;
     const cudaError_t ended = cudaStreamEndCapture(h->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t made =
+        launched == cudaSuccess && ended == cudaSuccess ? cudaGraphInstantiate(&exec, graph, 0) : cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
     check_cuda(launched, "step kernel (graph capture)");
     check_cuda(ended, "cudaStreamEndCapture");
-    cudaGraphExec_t exec = nullptr;
-    const cudaError_t made = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
     check_cuda(made, "cudaGraphInstantiate");
     cudaError_t e = cudaSuccess;
     std::uint64_t run = 0;
