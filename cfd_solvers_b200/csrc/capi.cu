@@ -1060,6 +1060,34 @@ std::uint64_t step_graphs(cfdx_lbm* h, LbmArgs& a, dim3 g, dim3 b, std::uint64_t
     return run * kGraphSteps;
 }
 
+// Enqueues `launches` (returning the first launch error) on the handle's stream,
+// inside one captured CUDA graph when the stream is not already being captured:
+// the adjoint's segments are a hundred-odd dependent launches each, and a graph
+// shortens the gaps between them.  A capture is always ended before an error
+// is reported, so the stream never stays in capture mode.
+extern "C++" template <class F> void enqueue_captured(cfdx_lbm* h, const char* what, F&& launches) {
+    cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &status) != cudaSuccess || status != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        check_cuda(launches(), what);
+        return;
+    }
+    check_cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    const cudaError_t launched = launches();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ended = cudaStreamEndCapture(h->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t made =
+        launched == cudaSuccess && ended == cudaSuccess ? cudaGraphInstantiate(&exec, graph, 0) : cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    check_cuda(launched, what);
+    check_cuda(ended, "cudaStreamEndCapture");
+    check_cuda(made, "cudaGraphInstantiate");
+    const cudaError_t e = cudaGraphLaunch(exec, h->stream);
+    cudaGraphExecDestroy(exec);
+    check_cuda(e, "cudaGraphLaunch");
+}
+
 } // namespace
 
 CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
@@ -1725,19 +1753,24 @@ CFDX_API int cfdx_lbm_adjoint_backward(cfdx_lbm* h, const float* g_rho, const fl
             const std::uint64_t ts = A.t0 + s * A.interval;
             const std::uint64_t len = std::min<std::uint64_t>(A.interval, A.t0 + A.steps - ts);
             const int P = static_cast<int>(A.t0 & 1U); // every checkpoint and frame keeps the layout of t0
-            for (std::uint64_t k = 1; k < len; ++k) {
-                LbmArgs src = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
-                src.round_seed = h->round_seed(ts + k - 1U); // the forward's step at this time
-                check_cuda(launch_step_oop(h->key, src, h->args_at(adjoint_frame(h, s, k), es, P ^ 1), g, b,
-                                           h->stream),
-                           "adjoint recompute kernel");
-            }
-            for (std::uint64_t k = len; k >= 1U; --k) {
-                X.f = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
-                X.l = h->args_at(A.lam, lam_es, static_cast<int>(parity & 1U));
-                check_cuda(launch_adjoint_step(h->key, X, g, b, h->stream), "adjoint step kernel");
-                ++parity;
-            }
+            // the segment's recompute and adjoint steps as one graph
+            enqueue_captured(h, "adjoint segment kernels", [&]() -> cudaError_t {
+                for (std::uint64_t k = 1; k < len; ++k) {
+                    LbmArgs src = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
+                    src.round_seed = h->round_seed(ts + k - 1U); // the forward's step at this time
+                    const cudaError_t e =
+                        launch_step_oop(h->key, src, h->args_at(adjoint_frame(h, s, k), es, P ^ 1), g, b, h->stream);
+                    if (e != cudaSuccess) return e;
+                }
+                for (std::uint64_t k = len; k >= 1U; --k) {
+                    X.f = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
+                    X.l = h->args_at(A.lam, lam_es, static_cast<int>(parity & 1U));
+                    const cudaError_t e = launch_adjoint_step(h->key, X, g, b, h->stream);
+                    if (e != cudaSuccess) return e;
+                    ++parity;
+                }
+                return cudaSuccess;
+            });
         }
         check_cuda(launch_sum_partials(A.tau_partials, blocks, A.tau_out, h->stream), "adjoint tau reduction");
         if (grad_ns) {

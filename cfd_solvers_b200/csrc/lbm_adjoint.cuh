@@ -222,8 +222,20 @@ __device__ __forceinline__ void block_accumulate(double v, double* partials) {
 // Out-of-place forward step for the segment recompute: gather from f (parity
 // P tables, source frame), collide exactly as k_step does, scatter through s
 // (parity P ^ 1 tables, destination frame).
+// Resident blocks per SM of the out-of-place recompute step.  It carries two
+// argument blocks, and at the one-cell step's cap for D3Q19 (12 blocks, 40
+// registers) its forms spilled up to 152 bytes.  Measured on B200, 128^3 FP32
+// gray TRT channel, reverse sweep per step: 12 blocks 191 us, 10 blocks (48
+// registers) 172 us, 8 blocks (64 registers) 173 us.
+#ifndef CFDX_OOP_MIN_BLOCKS_Q19
+#define CFDX_OOP_MIN_BLOCKS_Q19 10
+#endif
+template <class L, class S> constexpr int oop_min_blocks() {
+    return L::Q == 19 && sizeof(typename S::T) != 8 ? CFDX_OOP_MIN_BLOCKS_Q19 : step_min_blocks<L, S>();
+}
+
 template <class L, class S, bool FLAGS, bool GRAY>
-__global__ void __launch_bounds__(128, step_min_blocks<L, S>()) k_step_oop(const __grid_constant__ LbmArgs f,
+__global__ void __launch_bounds__(128, oop_min_blocks<L, S>()) k_step_oop(const __grid_constant__ LbmArgs f,
                                                                           const __grid_constant__ LbmArgs s) {
     using R = typename S::R;
     const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
