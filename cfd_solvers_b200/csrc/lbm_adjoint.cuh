@@ -230,12 +230,12 @@ __device__ __forceinline__ void block_accumulate(double v, double* partials) {
 #ifndef CFDX_OOP_MIN_BLOCKS_Q19
 #define CFDX_OOP_MIN_BLOCKS_Q19 10
 #endif
-template <class L, class S> constexpr int oop_min_blocks() {
-    return L::Q == 19 && sizeof(typename S::T) != 8 ? CFDX_OOP_MIN_BLOCKS_Q19 : step_min_blocks<L, S>();
+template <class L, class S, bool GRAY> constexpr int oop_min_blocks() {
+    return L::Q == 19 && sizeof(typename S::T) != 8 ? CFDX_OOP_MIN_BLOCKS_Q19 : step_min_blocks<L, S, GRAY>();
 }
 
 template <class L, class S, bool FLAGS, bool GRAY>
-__global__ void __launch_bounds__(128, oop_min_blocks<L, S>()) k_step_oop(const __grid_constant__ LbmArgs f,
+__global__ void __launch_bounds__(128, oop_min_blocks<L, S, GRAY>()) k_step_oop(const __grid_constant__ LbmArgs f,
                                                                           const __grid_constant__ LbmArgs s) {
     using R = typename S::R;
     const u32 x = blockIdx.x * blockDim.x + threadIdx.x;

@@ -1035,16 +1035,34 @@ __device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, V* h) {
 #ifndef CFDX_PAIR_MIN_BLOCKS
 #define CFDX_PAIR_MIN_BLOCKS 8
 #endif
+// Gray-LBM forms (partial bounce-back) keep the solid fraction and the
+// pre-collision populations alive through the collision and spilled up to
+// 112 (D3Q19 FP32) and 368 (D3Q27 FP16) bytes per thread at the caps above.
+// Measured on B200, gray TRT channel forward step: D3Q27 FP16 256^3 at 8
+// blocks (64 registers) 548 us vs 744 us at 10; D3Q19 FP32 128^3 at 8 blocks
+// 63.7 us vs 65.9 us at 12 (10 blocks, 48 registers, keeps 24 bytes of spill).
+#ifndef CFDX_STEP_MIN_BLOCKS_Q19_GRAY
+#define CFDX_STEP_MIN_BLOCKS_Q19_GRAY 10
+#endif
+#ifndef CFDX_STEP_MIN_BLOCKS_Q27_F16_GRAY
+#define CFDX_STEP_MIN_BLOCKS_Q27_F16_GRAY 8
+#endif
 
-template <class L, class S> constexpr int step_min_blocks() {
-    return sizeof(typename S::T) == 8 ? 1
-         : (L::Q == 19 ? CFDX_STEP_MIN_BLOCKS_Q19
-                       : (sizeof(typename S::T) == 2 ? CFDX_STEP_MIN_BLOCKS_Q27_F16 : CFDX_STEP_MIN_BLOCKS_Q27_F32));
+template <class L, class S, bool GRAY = false> constexpr int step_min_blocks() {
+    if constexpr (sizeof(typename S::T) == 8) {
+        return 1;
+    } else if constexpr (L::Q == 19) {
+        return GRAY ? CFDX_STEP_MIN_BLOCKS_Q19_GRAY : CFDX_STEP_MIN_BLOCKS_Q19;
+    } else if constexpr (sizeof(typename S::T) == 2) {
+        return GRAY ? CFDX_STEP_MIN_BLOCKS_Q27_F16_GRAY : CFDX_STEP_MIN_BLOCKS_Q27_F16;
+    } else {
+        return CFDX_STEP_MIN_BLOCKS_Q27_F32;
+    }
 }
 template <class S> constexpr int pair_min_blocks() { return sizeof(typename S::T) == 8 ? 1 : CFDX_PAIR_MIN_BLOCKS; }
 
 template <class L, class S, bool LES, bool FLAGS, bool GRAY, int CPT, bool NARROW>
-__global__ void __launch_bounds__(128, step_min_blocks<L, S>()) k_step(const __grid_constant__ LbmArgs a) {
+__global__ void __launch_bounds__(128, step_min_blocks<L, S, GRAY>()) k_step(const __grid_constant__ LbmArgs a) {
     using R = typename S::R;
     const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
