@@ -58,7 +58,17 @@ void* device_alloc(std::size_t bytes, const char* what) {
         fail(CFDX_ERR_OOM, std::string(what) + ": injected allocation failure (cudaErrorMemoryAllocation)");
     }
     void* p = nullptr;
-    check_cuda(cudaMalloc(&p, bytes), what);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        // the scratch pool may hold idle memory from earlier voxelizer / Q-criterion
+        // calls: return it to the driver and try once more
+        cudaGetLastError();
+        int device = 0;
+        if (cudaGetDevice(&device) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+            scratch_release(device) == cudaSuccess)
+            e = cudaMalloc(&p, bytes);
+    }
+    check_cuda(e, what);
     return p;
 }
 
