@@ -49,6 +49,10 @@ def parse_args(argv=None):
     p.add_argument("--n", type=int, default=512, help="cavity edge (cells)")
     p.add_argument("--lattice", choices=["d3q19", "d3q27"], default="d3q19")
     p.add_argument("--storage", choices=["fp32", "fp16s"], default="fp32")
+    p.add_argument("--variant", type=int, default=0,
+                   help="step kernel of the headline lattice: 0 automatic, 1 one cell per thread, 2 paired cells, "
+                        "3 / 4 wall-aware FP16 pairs with / without shared-memory prefetch")
+    p.add_argument("--planes", type=int, default=0, help="z-planes per thread of variants 3 and 4 (0: default)")
     p.add_argument("--no-variants", action="store_true", help="skip the FP16S / D3Q27 side measurements")
     p.add_argument("--slabs", action="store_true",
                    help="run the z-slab path (used for N > 1) also on one GPU: one slab that is the whole ring")
@@ -154,10 +158,13 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- our engine
-def make_cavity(cs, n, lattice="d3q19", storage="fp32", device=0):
+def make_cavity(cs, n, lattice="d3q19", storage="fp32", device=0, variant=0, planes=0):
     s = cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(
         nx=n, ny=n, nz=n, tau=0.51, lattice=lattice, collision="trt", trt_magic=3.0 / 16.0, smagorinsky_les=True,
         smagorinsky_cs=0.1, storage=storage, device=device))
+    if variant or planes:
+        s.set_launch_shape(0, 0, variant)
+        s.set_step_planes(planes)
     return s
 
 
@@ -886,7 +893,8 @@ def main(argv=None):
 
     n = args.n
     q = 19 if args.lattice == "d3q19" else 27
-    s = make_cavity(cs, n, lattice=args.lattice, storage=args.storage, device=local_rank)
+    s = make_cavity(cs, n, lattice=args.lattice, storage=args.storage, device=local_rank, variant=args.variant,
+                    planes=args.planes)
     setup_cavity(s, cs, n)
     time_steps(torch, s, args.warmup)
 

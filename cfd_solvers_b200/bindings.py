@@ -151,6 +151,7 @@ SIGNATURES = {
     "cfdx_lbm_stream": (_i, [_H, ctypes.POINTER(_vp)]),
     "cfdx_lbm_raw_populations": (_i, [_H, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
     "cfdx_lbm_set_launch_shape": (_i, [_H, _i, _i, _i]),
+    "cfdx_lbm_set_step_planes": (_i, [_H, _i]),
     "cfdx_lbm_reduce_noalloc": (_i, [_H, ctypes.POINTER(ctypes.c_double)]),
     "cfdx_lbm_set_tau": (_i, [_H, ctypes.c_float]),
     "cfdx_lbm_checkpoint_save": (_i, [_H, ctypes.c_char_p]),
@@ -215,6 +216,7 @@ SIGNATURES = {
     "cfdx_debug_audit_classify": (_i, [ctypes.c_uint32] * 5 + [ctypes.POINTER(ctypes.c_uint)]),
     "cfdx_release_scratch": (_i, [_i]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
+    "cfdx_debug_retry_allocations": (_i, [_i, ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 
 

@@ -37,6 +37,8 @@ using namespace cfdx;
 thread_local std::string g_error;
 thread_local int g_error_status = CFDX_OK;
 std::atomic<int> g_fail_allocations{0};
+std::atomic<int> g_retry_allocations{0};           // test hook: first attempts that report out-of-memory
+std::atomic<unsigned long long> g_allocation_retries{0};
 
 struct CfdxError : std::runtime_error {
     int status;
@@ -58,14 +60,23 @@ void* device_alloc(std::size_t bytes, const char* what) {
         fail(CFDX_ERR_OOM, std::string(what) + ": injected allocation failure (cudaErrorMemoryAllocation)");
     }
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes);
+    cudaError_t e;
+    if (g_retry_allocations.load() > 0) {
+        g_retry_allocations.fetch_sub(1);
+        e = cudaErrorMemoryAllocation; // test hook: the first attempt reports out-of-memory
+    } else {
+        e = cudaMalloc(&p, bytes);
+    }
     if (e == cudaErrorMemoryAllocation) {
-        // the scratch pool may hold idle memory from earlier voxelizer / Q-criterion
-        // calls: return it to the driver and try once more
+        // The scratch pool may hold idle memory from earlier voxelizer / Q-criterion
+        // calls: return it to the driver and try once more.  No synchronisation:
+        // the trim releases what the pool holds idle now, and pool memory whose
+        // stream-ordered free has not run yet stays mapped (waiting for every
+        // stream of the device would stall other handles and other libraries).
         cudaGetLastError();
+        ++g_allocation_retries;
         int device = 0;
-        if (cudaGetDevice(&device) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
-            scratch_release(device) == cudaSuccess)
+        if (cudaGetDevice(&device) == cudaSuccess && scratch_release(device) == cudaSuccess)
             e = cudaMalloc(&p, bytes);
     }
     check_cuda(e, what);
@@ -167,7 +178,11 @@ struct cfdx_lbm {
     float wall_u[kMaxWallIds][3]{};
     float scale[27]{};
     LaunchShape shape{};
-    int variant = 0; // step kernel: 0 auto, 1 one cell per thread, 2 paired cells
+    // step kernel: 0 auto, 1 one cell per thread, 2 paired cells, 3 / 4 the
+    // wall-aware z-marching FP16 pair kernel with / without its cp.async pipeline
+    int variant = 0;
+    std::uint32_t planes = 0; // z-planes per thread of that kernel (0: kDefaultPlanes)
+    static constexpr std::uint32_t kDefaultPlanes = 8;
     // Automatic choice between the one-cell and the paired-cell kernel, from
     // B200 measurements (GLUPS, FP16 D3Q19, one-cell vs two-cell): pairs win
     // only on lattices without flags (BGK periodic 512^3: 64.3 vs 55.6).  With
@@ -247,6 +262,7 @@ struct cfdx_lbm {
         a.wall_mask = key.flags ? wall_mask : nullptr;
         a.near_list = key.flags ? near_list : nullptr;
         a.near_count = key.flags ? near_count : 0U;
+        a.planes = planes == 0U ? kDefaultPlanes : planes;
         a.ax_field = local_a;
         a.ay_field = local_a ? local_a + N : nullptr;
         a.az_field = local_a ? local_a + 2 * N : nullptr;
@@ -315,11 +331,29 @@ struct cfdx_lbm {
                static_cast<unsigned long long>(key.q) * N < (1ULL << 32) &&
                (shape.block_x == 0 || shape.block_x % 32 == 0);
     }
+    // The wall-aware FP16 pair kernel needs FP16 storage, an even nx and
+    // element offsets that fit 32 bits.
+    bool w2_eligible() const {
+        return key.storage == kStoreF16S && cfg.nx % 2U == 0U &&
+               static_cast<unsigned long long>(key.q) * N < (1ULL << 32) &&
+               (shape.block_x == 0 || shape.block_x * shape.block_y == 128);
+    }
     void choose_variant() {
         key.narrow = static_cast<unsigned long long>(key.q) * N < (1ULL << 32);
-        key.paired = variant == 2 || (variant == 0 && paired_eligible() && paired_default(key.storage, key.q, key.flags));
+        key.w2 = (variant == 3 || variant == 4) && w2_eligible();
+        key.w2_pipe = variant != 4;
+        key.paired = !key.w2 && (variant == 2 || (variant == 0 && paired_eligible() &&
+                                                  paired_default(key.storage, key.q, key.flags)));
     }
     dim3 step_block() const {
+        if (key.w2) {
+            // 128 threads as one warp along x in each of four rows: the warps of
+            // a block cover the same x-segment, so a block's warps meet the same
+            // walls (a row's end pairs hold its x-walls) and finish together
+            if (shape.block_x > 0 && shape.block_y > 0)
+                return dim3(static_cast<unsigned>(shape.block_x), static_cast<unsigned>(shape.block_y), 1U);
+            return dim3(32U, 4U, 1U);
+        }
         if (!key.paired) return block();
         int bx = shape.block_x, by = shape.block_y;
         if (bx <= 0 || by <= 0) {
@@ -1413,7 +1447,8 @@ CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* h, void** ptr, std::size_t* byte
 CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int variant) {
     return guarded([&] {
         checked(h);
-        require(variant >= 0 && variant <= 2, "step kernel variant must be 0 (auto), 1 (one cell) or 2 (paired)");
+        require(variant >= 0 && variant <= 4,
+                "step kernel variant must be 0 (auto), 1 (one cell), 2 (paired) or 3 / 4 (wall-aware FP16 pairs)");
         if (bx == 0 && by == 0) {
             h->shape = LaunchShape{};
         } else {
@@ -1427,9 +1462,21 @@ CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* h, int bx, int by, int variant)
             require(h->paired_eligible(),
                     "the paired-cell kernel needs FP32/FP16 storage, an even nx, q*cells < 2^32 and block_x a "
                     "multiple of 32");
+        if (variant == 3 || variant == 4)
+            require(h->w2_eligible(),
+                    "the wall-aware paired kernel needs FP16 storage, an even nx, q*cells < 2^32 and 128-thread "
+                    "blocks");
 
         h->choose_variant();
         refresh_near_list(h, false);
+    });
+}
+
+CFDX_API int cfdx_lbm_set_step_planes(cfdx_lbm* h, int planes) {
+    return guarded([&] {
+        checked(h);
+        require(planes >= 0 && planes <= 4096, "planes per thread must be in [0, 4096] (0: default)");
+        h->planes = static_cast<std::uint32_t>(planes);
     });
 }
 
@@ -2663,6 +2710,12 @@ CFDX_API int cfdx_release_scratch(int device) {
 
 CFDX_API int cfdx_debug_fail_allocations(int count) {
     g_fail_allocations.store(count > 0 ? count : 0);
+    return CFDX_OK;
+}
+
+CFDX_API int cfdx_debug_retry_allocations(int count, unsigned long long* retries) {
+    if (count >= 0) g_retry_allocations.store(count);
+    if (retries) *retries = g_allocation_retries.load();
     return CFDX_OK;
 }
 

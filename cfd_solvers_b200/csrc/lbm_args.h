@@ -83,6 +83,8 @@ struct LbmArgs {
     // with a wall or a near-wall cell), in cell order; k_step_list steps them.
     const std::uint32_t* near_list;
     std::uint32_t near_count;
+    // z-planes each thread of the z-marching pair kernel (k_step_w2) steps.
+    std::uint32_t planes;
 };
 
 // Parameters of the adjoint kernels (lbm_adjoint.cuh).

@@ -25,6 +25,8 @@ struct KernelKey {
     bool gray;
     int cells_per_thread; // reserved (one cell per thread)
     bool paired;          // use the paired-cell step kernel (two adjacent x cells per thread)
+    bool w2;              // FP16: the wall-aware z-marching pair kernel (k_step_w2)
+    bool w2_pipe;         // k_step_w2 with its cp.async shared-memory pipeline
     bool narrow;          // 32-bit slot offsets (q * cells < 2^32)
 };
 

@@ -2,12 +2,14 @@
 // one storage type.  Included by lbm_kernels_{f32,f16s,f64}.cu only.
 #pragma once
 
+#include <algorithm>
 #include <type_traits>
 
 #include "lbm_adjoint.cuh"
 #include "lbm_device.cuh"
 #include "lbm_launch.h"
 #include "lbm_step_h2.cuh"
+#include "lbm_step_w2.cuh"
 #include "lbm_step_x2.cuh"
 
 namespace cfdx {
@@ -65,8 +67,43 @@ cudaError_t step_paired(const LbmArgs& a, dim3 b, cudaStream_t s) {
     }
 }
 
+// Wall-aware z-marching pair kernel (FP16 storage): grid over pairs, rows and
+// chunks of a.planes planes; the pipelined form stages two planes of words
+// per thread in shared memory.  Its shared-memory carveout is set once so that
+// the blocks its register cap allows fit on an SM.
+template <class K> cudaError_t w2_carveout(K kernel, unsigned smem_bytes, int blocks) {
+    static cudaError_t done = [&] {
+        const unsigned need = (smem_bytes + 1024U) * static_cast<unsigned>(blocks); // + per-block reservation
+        const int pct = static_cast<int>(std::min(100U, (need * 100U + 228U * 1024U - 1U) / (228U * 1024U)));
+        return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    }();
+    return done;
+}
+
+template <class L, class S, bool LES, bool FL, bool GR>
+cudaError_t step_w2(const KernelKey& k, const LbmArgs& a, dim3 b, cudaStream_t s) {
+    if constexpr (sizeof(typename S::T) != 2) {
+        return cudaErrorInvalidValue;
+    } else {
+        if (b.x * b.y != kW2Threads || b.z != 1U) return cudaErrorInvalidValue;
+        const unsigned pairs = a.nx / 2U;
+        const unsigned planes = a.planes == 0U ? 1U : a.planes;
+        dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, (a.nz + planes - 1U) / planes);
+        if (k.w2_pipe) {
+            const cudaError_t e =
+                w2_carveout(k_step_w2<L, LES, FL, GR, true>, w2_smem_bytes<L>(), w2_min_blocks<L>());
+            if (e != cudaSuccess) return e;
+            k_step_w2<L, LES, FL, GR, true><<<g, b, w2_smem_bytes<L>(), s>>>(a);
+        } else {
+            k_step_w2<L, LES, FL, GR, false><<<g, b, 0, s>>>(a);
+        }
+        return cudaGetLastError();
+    }
+}
+
 template <class L, class S, bool LES, bool FL>
 cudaError_t step_gray(const KernelKey& k, const LbmArgs& a, dim3 g, dim3 b, cudaStream_t s) {
+    if (k.w2) return k.gray ? step_w2<L, S, LES, FL, true>(k, a, b, s) : step_w2<L, S, LES, FL, false>(k, a, b, s);
     if (k.paired)
         return k.gray ? step_paired<L, S, LES, FL, true>(a, b, s) : step_paired<L, S, LES, FL, false>(a, b, s);
     return k.gray ? step_single<L, S, LES, FL, true>(k.narrow, a, g, b, s)

@@ -1,0 +1,403 @@
+// Wall-aware two-cell step kernel for FP16-shifted storage (sm_100a).
+//
+// A thread owns the cells x0 = 2t and x0 + 1 of an x-row (nx even) and
+// marches through `planes` consecutive z-planes.  Every FP16 slot pair
+// (x0, x0+1) is one aligned 32-bit word, so a pair of cells costs one word
+// access per direction where the one-cell kernel spends two 16-bit ones, and
+// both cells relax together in packed f32x2 arithmetic (collide_scaled with
+// V = float2).
+//
+// Loads.  Per plane a thread reads the rest word, the pb words at its own
+// cells and the pa words at the neighbours n + c_j: aligned rows where
+// c_x(j) = 0, and two aligned words spliced by one byte permute where the row
+// is shifted by one element (the neighbouring thread reads the same words,
+// so the second access hits L1).  In the pipelined form (PIPE) the words of
+// plane z + 1 are copied into the thread's own shared-memory slots with
+// 4-byte cp.async while plane z is relaxed, so loads stay in flight through
+// the collision without holding registers; each thread reads back only what
+// it copied itself, so no block barrier is involved (cp.async.wait_group
+// makes a thread's own copies visible to it).
+//
+// Walls (half-way bounce-back in place, as the one-cell kernel's gather).  A
+// wall link only changes which slot a load takes: the source's other slot at
+// the same address.  The kernel loads the plain words for every pair and, for
+// the few cells with wall links (a nonzero wall-link mask), replaces the
+// bounced halves with 16-bit loads of the partner slots; a cell next to a
+// moving wall gets the one-cell kernel's correction lane by lane.  Stores are
+// the same slots with or without walls; a pair holding a wall cell stores its
+// fluid cell's halves alone (wall cells hold no populations of their own).
+// Warps without near-wall cells skip all of this on uniform branches, so
+// there is no near-wall cell list and no second launch.
+//
+// Results equal the one-cell kernel's bit for bit: the same loads, the same
+// explicitly rounded collision (collide_scaled), the moving-wall correction
+// by the same function, and the same stochastic rounding bits per (cell,
+// direction).
+//
+// In-place safety of the prefetch: within a step every slot is read and
+// written by exactly one cell, so the words of plane z + 1 that a thread
+// copies early are slots no other cell writes in this step.  The only other
+// data in those words are the unused halves of shifted words (another cell's
+// slot), which are discarded.
+#pragma once
+
+#include "lbm_step_h2.cuh"
+
+namespace cfdx {
+
+// Word slots of one thread's pair of cells, in issue order: 0 the rest word,
+// 1 + p the pb word of pair p, then the pa words of each pair (two for a pair
+// whose neighbour direction j has c_x(j) != 0).
+template <class L> struct W2Words {
+    __host__ __device__ static constexpr bool shifted(int p) { return L::cx(2 * p + 2) != 0; }
+    __host__ __device__ static constexpr int pa_slot(int p) {
+        int k = 1 + L::PAIRS;
+        for (int q = 0; q < p; ++q) k += shifted(q) ? 2 : 1;
+        return k;
+    }
+    static constexpr int count = pa_slot(L::PAIRS);
+    // pair of pa word slot k (k > PAIRS)
+    __host__ __device__ static constexpr int pa_pair(int k) {
+        int p = 0;
+        while (p + 1 < L::PAIRS && pa_slot(p + 1) <= k) ++p;
+        return p;
+    }
+};
+
+// Per-thread indices; n0 / nl / nr (the plane's row index plus x0 / xl / xr)
+// change with the plane, the rest does not.
+struct W2Ctx {
+    u32 x0, xl, xr, y, z; // xl / xr: x of the aligned words left / right of x0 (periodic)
+    u32 n0, nl, nr;
+    u32 oy[3], oz[3];     // row offsets of the y / z neighbours (periodic), [c + 1]
+};
+
+__device__ __forceinline__ void w2_thread(const LbmArgs& a, u32 x0, u32 y, W2Ctx& c) {
+    c.x0 = x0;
+    c.y = y;
+    c.xl = x0 == 0U ? a.nx - 2U : x0 - 2U;
+    c.xr = x0 + 2U == a.nx ? 0U : x0 + 2U;
+    c.oy[0] = y == 0 ? (a.ny - 1U) * a.nx : 0U - a.nx;
+    c.oy[1] = 0U;
+    c.oy[2] = y == a.ny - 1U ? 0U - (a.ny - 1U) * a.nx : a.nx;
+}
+
+__device__ __forceinline__ void w2_plane(const LbmArgs& a, u32 z, W2Ctx& c) {
+    c.z = z;
+    const u32 row = (z * a.ny + c.y) * a.nx;
+    c.n0 = row + c.x0;
+    c.nl = row + c.xl;
+    c.nr = row + c.xr;
+    const u32 plane = a.nx * a.ny;
+    c.oz[0] = z == 0 ? (a.nz - 1U) * plane : 0U - plane;
+    c.oz[1] = 0U;
+    c.oz[2] = z == a.nz - 1U ? 0U - (a.nz - 1U) * plane : plane;
+}
+
+// Offset from a cell's row to the row of its neighbour n + c_D (periodic in y and z).
+template <class L, int D> __device__ __forceinline__ u32 w2_dyz(const W2Ctx& c) {
+    return c.oy[L::cy(D) + 1] + c.oz[L::cz(D) + 1];
+}
+
+// Slot tables as pointers: a slot address is a table pointer (uniform across
+// the launch, built from the kernel parameters) plus one 32-bit per-thread
+// index.  Measured on B200 against widening a 32-bit sum of table offset and
+// index per access: +10 % on the 512^3 FP16 cavity.
+__device__ __forceinline__ __half* w2_tab(const LbmArgs& a, u32 off) { return static_cast<__half*>(a.base) + off; }
+
+// Address of word slot K.
+template <class L, int K> __device__ __forceinline__ const __half* w2_word_ptr(const LbmArgs& a, const W2Ctx& c) {
+    if constexpr (K == 0) {
+        return w2_tab(a, a.rest_off) + c.n0;
+    } else if constexpr (K <= L::PAIRS) {
+        return w2_tab(a, a.pb_off[K - 1]) + c.n0;
+    } else {
+        constexpr int p = W2Words<L>::pa_pair(K);
+        constexpr int second = K - W2Words<L>::pa_slot(p);
+        constexpr int j = 2 * p + 2, s = L::cx(j);
+        const u32 dyz = w2_dyz<L, j>(c);
+        const __half* t = w2_tab(a, a.pa_off[p]);
+        if constexpr (s == 0) return t + (c.n0 + dyz);
+        else if constexpr (s > 0) return t + ((second ? c.nr : c.n0) + dyz); // elements x0+1, x0+2
+        else return t + ((second ? c.n0 : c.nl) + dyz);                      // elements x0-1, x0
+    }
+}
+
+// Calls f(std::integral_constant<int, k>, address) for every word slot k.
+template <class L, int K = 0, class F> __device__ __forceinline__ void w2_words(const LbmArgs& a, const W2Ctx& c, F&& f) {
+    if constexpr (K < W2Words<L>::count) {
+        f(std::integral_constant<int, K>{}, w2_word_ptr<L, K>(a, c));
+        w2_words<L, K + 1>(a, c, f);
+    }
+}
+
+// Pair words (low half: cell x0, high half: cell x0 + 1) of every direction
+// from the raw words, as if the pair had no walls.
+template <class L> __device__ __forceinline__ void w2_assemble(const u32* raw, u32* pw) {
+    pw[0] = raw[0];
+    static_for_pairs<L>([&](auto PP) {
+        constexpr int p = decltype(PP)::value;
+        constexpr int i = 2 * p + 1, j = i + 1;
+        constexpr int k = W2Words<L>::pa_slot(p);
+        pw[j] = raw[1 + p];
+        if constexpr (W2Words<L>::shifted(p))
+            pw[i] = splice(raw[k], raw[k + 1]);
+        else
+            pw[i] = raw[k];
+    });
+}
+
+__device__ __forceinline__ u32 ld_u16(const __half* p) { return *reinterpret_cast<const unsigned short*>(p); }
+__device__ __forceinline__ u32 with_lo(u32 w, u32 h) { return (w & 0xffff0000U) | h; }
+__device__ __forceinline__ u32 with_hi(u32 w, u32 h) { return (w & 0x0000ffffU) | (h << 16); }
+
+// Index, within the cell's own row plane, of the source element of cell
+// x0 + C for a direction with c_x = S (the halves of the shifted words of
+// w2_words; periodic in x).  Add w2_dyz for the neighbour's row.
+template <int S, int C> __device__ __forceinline__ u32 w2_src(const W2Ctx& c) {
+    if constexpr (S == 0) return c.n0 + C;
+    else if constexpr (S > 0) return C == 0 ? c.n0 + 1U : c.nr;
+    else return C == 0 ? c.nl + 1U : c.n0;
+}
+
+// Half-way bounce-back of the cells with wall links (masks m0, m1; the
+// one-cell gather_walls rule): direction i = 2p+1 whose source n + c_j is a
+// wall reads the pb slot at that source; direction j whose source n + c_i is a
+// wall reads the pa slot at the cell.
+
+template <class L>
+__device__ __forceinline__ void w2_bounce(const LbmArgs& a, const W2Ctx& c, u32 m0, u32 m1, u32* pw) {
+    const u32 m = m0 | m1;
+    static_for_pairs<L>([&](auto PP) {
+        constexpr int p = decltype(PP)::value;
+        constexpr int i = 2 * p + 1, j = i + 1, s = L::cx(j);
+        constexpr u32 bi = 1U << (2 * p), bj = 2U << (2 * p);
+        if (m & bi) {
+            const u32 dyz = w2_dyz<L, j>(c);
+            if (m0 & bi) pw[i] = with_lo(pw[i], ld_u16(w2_tab(a, a.pb_off[p]) + (w2_src<s, 0>(c) + dyz)));
+            if (m1 & bi) pw[i] = with_hi(pw[i], ld_u16(w2_tab(a, a.pb_off[p]) + (w2_src<s, 1>(c) + dyz)));
+        }
+        if (m & bj) {
+            if (m0 & bj) pw[j] = with_lo(pw[j], ld_u16(w2_tab(a, a.pa_off[p]) + c.n0));
+            if (m1 & bj) pw[j] = with_hi(pw[j], ld_u16(w2_tab(a, a.pa_off[p]) + (c.n0 + 1U)));
+        }
+    });
+}
+
+// Moving-wall correction of one lane (cell x0 + C) with the one-cell kernel's function.
+template <class L, int C>
+__device__ __noinline__ void w2_moving_lane(const LbmArgs& a, const W2Ctx c, std::uint8_t flag, float2* f) {
+    float h[L::Q];
+#pragma unroll
+    for (int d = 0; d < L::Q; ++d) h[d] = C ? f[d].y : f[d].x;
+    gather_fixup_scaled<L>(a, c.n0 + C, make_nbr(a, c.x0 + C, c.y, c.z), flag, h);
+#pragma unroll
+    for (int d = 0; d < L::Q; ++d) {
+        if (C)
+            f[d].y = h[d];
+        else
+            f[d].x = h[d];
+    }
+}
+
+// Stores: aligned words where the slot pair is aligned, two 16-bit stores
+// where the pa row is shifted (h2_stores' rule).
+// MERGE (a warp holding a pair with a wall cell): a wall cell is not stepped,
+// and its slots must keep their bits.  Its half of each aligned word is the
+// word's loaded value (raw(k), word slot k; byte selector sel: 0x3210 keeps
+// the stepped word, 0x3254 takes the low half, 0x7610 the high half from
+// raw), and its shifted halves are not stored (live0 / live1).  Writing the
+// loaded bits back is exact: no cell writes a wall cell's slots within a step
+// and the cells that read them (bounce-back) read the same bits either way.
+template <class L, bool MERGE, class Raw>
+__device__ __forceinline__ void w2_stores(const LbmArgs& a, const W2Ctx& c, const float2* f, u32 h0, u32 h1, u32 sel,
+                                          bool live0, bool live1, Raw&& raw) {
+    const auto merged = [&](u32 w, auto K) {
+        if constexpr (MERGE)
+            return __byte_perm(w, raw(K), sel);
+        else
+            return w;
+    };
+    st_word(w2_tab(a, a.rest_off) + c.n0,
+            merged(f16x2_rs(f[0].y, f[0].x, lo_halves(round_bits(a, h0, 0), round_bits(a, h1, 0))),
+                   std::integral_constant<int, 0>{}));
+    static_for_pairs<L>([&](auto PP) {
+        constexpr int p = decltype(PP)::value;
+        constexpr int i = 2 * p + 1, j = i + 1, s = L::cx(j);
+        constexpr int k = W2Words<L>::pa_slot(p);
+        const u32 k0 = round_bits(a, h0, p + 1), k1 = round_bits(a, h1, p + 1);
+        st_word(w2_tab(a, a.pb_off[p]) + c.n0,
+                merged(f16x2_rs(f[i].y, f[i].x, lo_halves(k0, k1)), std::integral_constant<int, 1 + p>{}));
+        const u32 wj = f16x2_rs(f[j].y, f[j].x, hi_halves(k0, k1));
+        __half* t = w2_tab(a, a.pa_off[p]);
+        const u32 dyz = w2_dyz<L, j>(c);
+        if constexpr (s == 0) {
+            st_word(t + (c.n0 + dyz), merged(wj, std::integral_constant<int, k>{}));
+        } else if constexpr (MERGE) {
+            if (live0) st_half(t + (w2_src<s, 0>(c) + dyz), wj);
+            if (live1) st_half(t + (w2_src<s, 1>(c) + dyz), wj >> 16);
+        } else {
+            st_half(t + (w2_src<s, 0>(c) + dyz), wj);
+            st_half(t + (w2_src<s, 1>(c) + dyz), wj >> 16);
+        }
+    });
+}
+
+// One pair of cells from its raw words.  fl2: the two internal flag bytes
+// (cell x0 in the low byte).  raw(k): word slot k as loaded (for MERGE stores).
+// The moving-wall correction is a call, not inlined code: inlined, its
+// per-lane arrays raised the register demand of the whole kernel and the
+// interior path spilled.  It gets a copy of the populations (tmp), since an
+// array whose address reaches a call lives in local memory on every path.
+// The bounce-back loads stay inline: they run in every warp that holds a
+// near-wall pair (on a cavity, the first and last warp of each row), and a
+// call there saved and restored the live registers through local memory.
+template <class L, bool LES, bool FLAGS, bool GRAY, class Raw>
+__device__ __forceinline__ void w2_cell_pair(const LbmArgs& a, const W2Ctx& c, const u32* raw_words, unsigned fl2,
+                                             Raw&& raw) {
+    u32 pw[L::Q];
+    w2_assemble<L>(raw_words, pw);
+    constexpr unsigned kNearWall2 = kFlagNearWall * 0x0101U;
+    constexpr unsigned kNearMoving2 = kFlagNearMoving * 0x0101U;
+    constexpr unsigned kType2 = kFlagTypeMask * 0x0101U;
+    if constexpr (FLAGS) {
+        if (fl2 & kNearWall2) {
+            // wall cells have empty masks; a fluid cell's mask is loaded only when it has links
+            const u32 m0 = (fl2 & kFlagNearWall) ? a.wall_mask[c.n0] : 0U;
+            const u32 m1 = (fl2 & (kFlagNearWall << 8)) ? a.wall_mask[c.n0 + 1U] : 0U;
+            w2_bounce<L>(a, c, m0, m1, pw);
+        }
+    }
+    float2 f[L::Q];
+#pragma unroll
+    for (int d = 0; d < L::Q; ++d) f[d] = unpack(pw[d]);
+    if constexpr (FLAGS) {
+        if (fl2 & kNearMoving2) {
+            float2 tmp[L::Q];
+#pragma unroll
+            for (int d = 0; d < L::Q; ++d) tmp[d] = f[d];
+            w2_moving_lane<L, 0>(a, c, static_cast<std::uint8_t>(fl2), tmp);
+            w2_moving_lane<L, 1>(a, c, static_cast<std::uint8_t>(fl2 >> 8), tmp);
+#pragma unroll
+            for (int d = 0; d < L::Q; ++d) f[d] = tmp[d];
+        }
+    }
+    if (a.has_force)
+        collide_scaled<L, LES, GRAY, true>(a, c.n0, f);
+    else
+        collide_scaled<L, LES, GRAY, false>(a, c.n0, f);
+    const u32 h0 = round_hash(a, c.n0), h1 = round_hash(a, c.n0 + 1U);
+    if constexpr (FLAGS) {
+        const bool wall0 = (fl2 & kFlagTypeMask) != 0U, wall1 = (fl2 & (kFlagTypeMask << 8)) != 0U;
+        // warp-uniform choice: the merging stores cost every thread of the warp the same
+        if (__any_sync(__activemask(), (fl2 & kType2) != 0U)) {
+            const u32 sel = wall0 ? 0x3254U : (wall1 ? 0x7610U : 0x3210U);
+            w2_stores<L, true>(a, c, f, h0, h1, sel, !wall0, !wall1, raw);
+            return;
+        }
+    }
+    w2_stores<L, false>(a, c, f, h0, h1, 0x3210U, true, true, raw);
+}
+
+// ---------------------------------------------------------------- cp.async
+template <int OFF> __device__ __forceinline__ void cp_async4(u32 smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0+%2], [%1], 4;\n" ::"r"(smem), "l"(gmem), "n"(OFF) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Resident 128-thread blocks per SM (register cap 65536 / (128 * blocks)).
+// The macros exist for tuning builds.
+#ifndef CFDX_W2_MIN_BLOCKS
+#define CFDX_W2_MIN_BLOCKS 6
+#endif
+#ifndef CFDX_W2_MIN_BLOCKS_Q27
+#define CFDX_W2_MIN_BLOCKS_Q27 5
+#endif
+template <class L> constexpr int w2_min_blocks() { return L::Q == 27 ? CFDX_W2_MIN_BLOCKS_Q27 : CFDX_W2_MIN_BLOCKS; }
+
+// Threads per block of k_step_w2 (the shared-memory slots of the pipelined
+// form are laid out for it, so their offsets are immediates).
+constexpr unsigned kW2Threads = 128;
+
+// Shared memory of the pipelined form: two stages of the word slots per thread.
+template <class L> constexpr unsigned w2_smem_bytes() {
+    return 2U * static_cast<unsigned>(W2Words<L>::count) * kW2Threads * 4U;
+}
+
+// Grid: x over pairs (blockDim.x threads, nx/2 pairs), y over rows
+// (blockDim.x * blockDim.y == kW2Threads), z over chunks of a.planes planes.
+template <class L, bool LES, bool FLAGS, bool GRAY, bool PIPE>
+__global__ void __launch_bounds__(kW2Threads, w2_min_blocks<L>()) k_step_w2(const __grid_constant__ LbmArgs a) {
+    constexpr int W = W2Words<L>::count;
+    const u32 x0 = 2U * (blockIdx.x * blockDim.x + threadIdx.x);
+    const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x0 >= a.nx || y >= a.ny) return;
+    const u32 zb = blockIdx.z * a.planes;
+    const u32 ze = min(a.nz, zb + a.planes);
+    W2Ctx c;
+    w2_thread(a, x0, y, c);
+    const auto flags_of = [&](const W2Ctx& cc) -> unsigned {
+        if constexpr (FLAGS)
+            return *reinterpret_cast<const unsigned short*>(a.flags + cc.n0);
+        else
+            return 0U;
+    };
+    // both cells walls: nothing to step
+    const auto both_walls = [](unsigned fl2) {
+        return FLAGS && (fl2 & kFlagTypeMask) != 0U && (fl2 & (kFlagTypeMask << 8)) != 0U;
+    };
+    if constexpr (!PIPE) {
+        for (u32 z = zb; z < ze; ++z) {
+            w2_plane(a, z, c);
+            const unsigned fl2 = flags_of(c);
+            if (both_walls(fl2)) continue;
+            u32 raw[W];
+            w2_words<L>(a, c, [&](auto K, const __half* p) { raw[decltype(K)::value] = ld_word(p); });
+            // merging stores reload a wall cell's words (no other cell writes them in this step)
+            w2_cell_pair<L, LES, FLAGS, GRAY>(a, c, raw, fl2, [&](auto K) {
+                return ld_word(w2_word_ptr<L, decltype(K)::value>(a, c));
+            });
+        }
+    } else {
+        // word k of stage st: w2_stage[(st * W + k) * kW2Threads + tid]
+        extern __shared__ u32 w2_stage[];
+        const u32 tid = threadIdx.y * blockDim.x + threadIdx.x;
+        const u32* mine = w2_stage + tid;
+        const u32 sbase = static_cast<u32>(__cvta_generic_to_shared(mine));
+        constexpr u32 kStageBytes = W * kW2Threads * 4U;
+        const auto issue = [&](u32 z, u32 st) -> unsigned {
+            W2Ctx cn = c;
+            w2_plane(a, z, cn);
+            const u32 s0 = sbase + st * kStageBytes;
+            w2_words<L>(a, cn, [&](auto K, const __half* p) {
+                cp_async4<decltype(K)::value * kW2Threads * 4>(s0, p);
+            });
+            return flags_of(cn);
+        };
+        unsigned fl_next = issue(zb, 0U);
+        cp_async_commit();
+        for (u32 z = zb; z < ze; ++z) {
+            const unsigned fl2 = fl_next;
+            const u32 st = (z - zb) & 1U;
+            if (z + 1U < ze) fl_next = issue(z + 1U, st ^ 1U);
+            cp_async_commit();
+            cp_async_wait<1>();
+            if (both_walls(fl2)) continue;
+            const u32* words = mine + st * (W * kW2Threads);
+            u32 raw[W];
+#pragma unroll
+            for (int k = 0; k < W; ++k) raw[k] = words[k * kW2Threads];
+            w2_plane(a, z, c);
+            // merging stores re-read the words from the stage, intact until the next issue
+            w2_cell_pair<L, LES, FLAGS, GRAY>(a, c, raw, fl2,
+                                              [&](auto K) { return words[decltype(K)::value * kW2Threads]; });
+        }
+        cp_async_wait_all();
+    }
+}
+
+} // namespace cfdx

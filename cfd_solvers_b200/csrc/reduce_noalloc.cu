@@ -14,12 +14,12 @@
 // other allocating routine; the caller passes the lattice (a handle created
 // beforehand) and a host output buffer of CFDX_REDUCE_COUNT doubles.
 //
-// Scratch: the reduction runs nz blocks (block b sums every nz-th x-row,
-// starting at row b), each writing its 7 partial sums; a final block combines
-// them in a fixed order and writes the 7 results.  The array holds the
-// partials of at most 4096 blocks, so lattices with more than 4096 cells in z
-// are rejected.  Every GPU that loads this library holds the array (229,432
-// bytes) until the process exits.
+// Scratch: the reduction runs min(ny*nz, 4096) blocks over the ny*nz x-rows
+// (block b sums rows b, b + blocks, ...), each writing its 7 partial sums; a
+// final block combines them in a fixed order and writes the 7 results.  The
+// array holds the partials of those at most 4096 blocks plus the results, so
+// any lattice size is accepted.  Every GPU that loads this library holds the
+// array (229,432 bytes) until the process exits.
 #include "cfdx_lbm.h"
 
 #include <cuda_runtime.h>
@@ -34,11 +34,11 @@ namespace {
 
 using namespace cfdx;
 
-constexpr unsigned kMaxPlanes = 4096;
+constexpr unsigned kMaxBlocks = 4096;
 constexpr int kMaxDevices = 64;
-constexpr std::size_t kScratchDoubles = (static_cast<std::size_t>(kMaxPlanes) + 1U) * kReduceFields;
+constexpr std::size_t kScratchDoubles = (static_cast<std::size_t>(kMaxBlocks) + 1U) * kReduceFields;
 
-// Partial sums of up to kMaxPlanes blocks followed by the 7 final values.
+// Partial sums of up to kMaxBlocks blocks followed by the 7 final values.
 static __device__ __align__(256) double g_reduce_scratch[kScratchDoubles];
 
 std::mutex g_setup_mutex;
@@ -46,7 +46,10 @@ void* g_scratch_address[kMaxDevices] = {};
 
 // Device address of g_reduce_scratch on `device`, which must be current.  In
 // host code the array's name is only a host-side stand-in; the address comes
-// from cudaGetSymbolAddress, once per device, on the first call there.
+// from cudaGetSymbolAddress, once per device, on the first call there.  The
+// cached address belongs to the device's primary context as it was then: a
+// process that resets the device (cudaDeviceReset) must not call this entry
+// point again afterwards.
 int scratch_address(int device, double** out) {
     if (device < 0 || device >= kMaxDevices) return record_error(CFDX_ERR_INVALID, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -88,22 +91,20 @@ extern "C" CFDX_API int cfdx_lbm_reduce_noalloc(cfdx_lbm* lbm, double* out) {
     int rc = handle_reduce_view(lbm, &v);
     if (rc != CFDX_OK) return rc;
     if (!out) return record_error(CFDX_ERR_INVALID, "null output buffer");
-    const unsigned planes = v.args.nz;
-    if (planes > kMaxPlanes)
-        return record_error(CFDX_ERR_INVALID,
-                            "cfdx_lbm_reduce_noalloc: lattice has more than 4096 cells in z (its static scratch holds "
-                            "the partial sums of at most 4096 blocks, one block per z extent); use cfdx_lbm_reduce");
+    // a fixed block count for every lattice shape, so thin lattices reduce on many SMs
+    const unsigned long long rows = static_cast<unsigned long long>(v.args.ny) * v.args.nz;
+    const unsigned blocks = static_cast<unsigned>(rows < kMaxBlocks ? rows : kMaxBlocks);
     double* scratch = nullptr;
     rc = scratch_address(v.device, &scratch);
     if (rc != CFDX_OK) return rc;
-    double* result = scratch + static_cast<std::size_t>(kMaxPlanes) * kReduceFields;
+    double* result = scratch + static_cast<std::size_t>(kMaxBlocks) * kReduceFields;
     // Every block writes all of its partial slots and the final block writes
     // every result slot, so nothing left by an earlier call is read.
     cudaError_t e;
     switch (v.key.storage) {
-    case kStoreF32: e = launch_storage<StF32>(v, scratch, planes, result); break;
-    case kStoreF64: e = launch_storage<StF64>(v, scratch, planes, result); break;
-    case kStoreF16S: e = launch_storage<StF16>(v, scratch, planes, result); break;
+    case kStoreF32: e = launch_storage<StF32>(v, scratch, blocks, result); break;
+    case kStoreF64: e = launch_storage<StF64>(v, scratch, blocks, result); break;
+    case kStoreF16S: e = launch_storage<StF16>(v, scratch, blocks, result); break;
     default: e = cudaErrorInvalidValue; break;
     }
     if (e == cudaSuccess)

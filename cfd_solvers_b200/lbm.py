@@ -454,8 +454,13 @@ class EsotericPullCudaSolver:
         self._call("cfdx_lbm_set_storage_scale", ctypes.c_void_p(s.ctypes.data))
 
     def set_launch_shape(self, block_x: int = 0, block_y: int = 0, variant: int = 0):
-        """Threads per block and step-kernel variant (0 auto, 1 one cell, 2 paired cells)."""
+        """Threads per block and step-kernel variant (0 auto, 1 one cell, 2 paired cells,
+        3 / 4 the wall-aware FP16 pair kernel with / without its shared-memory prefetch)."""
         self._call("cfdx_lbm_set_launch_shape", int(block_x), int(block_y), int(variant))
+
+    def set_step_planes(self, planes: int = 0):
+        """z-planes per thread of the z-marching FP16 pair kernel (0: default)."""
+        self._call("cfdx_lbm_set_step_planes", int(planes))
 
     def save_checkpoint(self, path):
         """CFDCHK3 checkpoint of the current state (reference DistributedPullSolver::save_checkpoint)."""

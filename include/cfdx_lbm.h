@@ -235,11 +235,19 @@ CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* lbm, void** device_ptr, size_t* 
 
 /* Launch shape of the cell kernels: threads per block (x, y) and the step
  * kernel variant: 0 automatic, 1 one cell per thread, 2 two adjacent x cells
- * per thread (FP32/FP16 storage, even nx).  Both variants give bitwise equal
+ * per thread (FP32/FP16 storage, even nx), 3 / 4 the wall-aware FP16 pair
+ * kernel that marches along z, with / without its shared-memory prefetch of
+ * the next plane (FP16 storage, even nx).  All variants give bitwise equal
  * results.  Automatic: two cells for D3Q19 FP16 on lattices without flags,
- * one cell otherwise (measured: with walls the one-cell kernel is faster).
- * Zeros restore the defaults. */
+ * one cell otherwise.  Zeros restore the defaults.
+ * Reference: no counterpart (the OpenMP loop of step_once,
+ * esoteric_pull.hpp:494-515, has no launch shape). */
 CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, int variant);
+
+/* z-planes each thread of the z-marching pair kernel (variants 3 and 4)
+ * steps, in [1, 4096]; 0 restores the default.  Results do not depend on it.
+ * Reference: no counterpart. */
+CFDX_API int cfdx_lbm_set_step_planes(cfdx_lbm* lbm, int planes);
 
 /* The reduction of cfdx_lbm_reduce() without any allocation: no
  * cudaMalloc, cudaFree or other allocating routine, for callers that cannot
@@ -250,11 +258,12 @@ CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, 
  * `out` is host memory for CFDX_REDUCE_COUNT doubles, same layout and status
  * codes as cfdx_lbm_reduce().  Scratch is a fixed static device array
  * (229,432 bytes on every GPU that loads the library, held until exit) with
- * partial sums for nz reduction blocks: lattices with nz > 4096 are rejected
- * with CFDX_ERR_INVALID.  The first call on each device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture.  All calls share the array: calls whose work overlaps on
- * the GPU (different handles' streams, or threads) race and must be
+ * the partial sums of min(ny*nz, 4096) reduction blocks, so every lattice
+ * size is accepted.  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress) and keeps it; make that first call
+ * before any stream capture, and do not call this entry point again after
+ * resetting the device.  All calls share the array: calls whose work overlaps
+ * on the GPU (different handles' streams, or threads) race and must be
  * serialised by the caller. */
 CFDX_API int cfdx_lbm_reduce_noalloc(cfdx_lbm* lbm, double* out);
 
@@ -596,6 +605,13 @@ CFDX_API int cfdx_debug_audit_classify(uint32_t reads, uint32_t writes, uint32_t
  * cudaErrorMemoryAllocation (0 disables).  Used to test CFDX_ERR_OOM paths
  * without exhausting the device. */
 CFDX_API int cfdx_debug_fail_allocations(int count);
+
+/* Test hook of the out-of-memory retry: the next `count` device allocations
+ * (count >= 0; < 0 leaves it unchanged) see out-of-memory from their first
+ * attempt, return the idle scratch-pool memory to the driver and try again.
+ * *retries (may be NULL) receives the number of retries taken so far in
+ * this process. */
+CFDX_API int cfdx_debug_retry_allocations(int count, unsigned long long* retries);
 
 #ifdef __cplusplus
 }

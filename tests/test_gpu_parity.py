@@ -391,6 +391,24 @@ def test_allocation_failure_is_reported_and_recoverable(engine):
         assert s.mass() == pytest.approx(512.0, rel=1e-6)
 
 
+def test_out_of_memory_retry_releases_the_scratch_pool(engine):
+    """A first allocation attempt that runs out of memory returns the idle scratch pool and retries."""
+    import ctypes
+
+    lib = engine.load()
+    before, after = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)
+    lib.raw.cfdx_debug_retry_allocations(-1, ctypes.byref(before))
+    lib.raw.cfdx_debug_retry_allocations(1, None)
+    try:
+        with make(engine, 19, 8, 8, 8) as s:
+            lib.raw.cfdx_debug_retry_allocations(-1, ctypes.byref(after))
+            assert after.value == before.value + 1
+            s.step(2)
+            assert s.mass() == pytest.approx(512.0, rel=1e-6)
+    finally:
+        lib.raw.cfdx_debug_retry_allocations(0, None)
+
+
 def test_argument_errors(engine):
     with make(engine, 19, 8, 8, 8) as s:
         with pytest.raises(IndexError):

@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 SHAPES = [(18, 15, 13), (130, 6, 5), (2, 6, 4), (64, 9, 7)]
 
 
-def run(cs, variant, q, shape, storage, flags_kind, gray, steps, seed=11):
+def run(cs, variant, q, shape, storage, flags_kind, gray, steps, seed=11, planes=0):
     nx, ny, nz = shape
     n = nx * ny * nz
     rng = np.random.default_rng(seed)
@@ -27,6 +27,7 @@ def run(cs, variant, q, shape, storage, flags_kind, gray, steps, seed=11):
                               acceleration_x=1e-5, fp16_rounding=rounding or "stochastic")
     with cs.EsotericPullCudaSolver(cfg) as s:
         s.set_launch_shape(0, 0, variant)
+        s.set_step_planes(planes)
         if flags_kind == "random":
             fl = (rng.random(n) < 0.2).astype(np.uint8)
             fl[rng.random(n) < 0.05] = 3
@@ -64,3 +65,35 @@ def test_paired_variant_requires_even_nx(engine):
         s.set_launch_shape(0, 0, 0)  # automatic falls back to one cell per thread
         s.step(3)
 
+
+
+# The wall-aware FP16 pair kernel (variants 3 and 4) marches along z; plane
+# counts that do not divide nz leave a short last chunk, and rows of 256 cells
+# span more than one warp.
+W2_SHAPES = SHAPES + [(256, 5, 9)]
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("storage", ["fp16s", "fp16s:nearest"])
+@pytest.mark.parametrize("shape", W2_SHAPES, ids=[f"{a}x{b}x{c}" for a, b, c in W2_SHAPES])
+@pytest.mark.parametrize("flags_kind, gray", [(None, False), ("random", False), ("random", True),
+                                              ("cavity", False), ("cavity", True)])
+@pytest.mark.parametrize("variant, planes", [(3, 0), (3, 3), (4, 1), (4, 5)])
+def test_wall_aware_pairs_match_single_bitwise(engine, q, storage, shape, flags_kind, gray, variant, planes):
+    steps = 5
+    a_log, a_red = run(engine, 1, q, shape, storage, flags_kind, gray, steps)
+    b_log, b_red = run(engine, variant, q, shape, storage, flags_kind, gray, steps, planes=planes)
+    assert np.array_equal(a_log.view(np.uint32), b_log.view(np.uint32))
+    assert a_red["mass"] == b_red["mass"]
+
+
+def test_wall_aware_pairs_need_fp16_and_even_nx(engine):
+    cs = engine
+    with cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(nx=16, ny=4, nz=4)) as s:
+        with pytest.raises(ValueError, match="wall-aware"):
+            s.set_launch_shape(0, 0, 3)
+        with pytest.raises(ValueError, match="planes"):
+            s.set_step_planes(-1)
+    with cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(nx=17, ny=4, nz=4, storage="fp16s")) as s:
+        with pytest.raises(ValueError, match="wall-aware"):
+            s.set_launch_shape(0, 0, 4)
