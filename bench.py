@@ -537,6 +537,95 @@ def cpu_reference_sample(n, warmup, steps, threads=0):
     return mlups, seconds, O.ref_threads()
 
 
+# The reference CPU sample of the cavity workload, shared by cpu_baseline and
+# the --impl reference arm: the 3-pass solid step at SOLID_SAMPLE_N^3 (about
+# 1.5 s per step on 16 host threads).
+SOLID_SAMPLE_N = 384
+CPU_SAMPLE_SECONDS = 20.0
+
+
+def cpu_solid_baseline(max_seconds=CPU_SAMPLE_SECONDS):
+    """cpu_baseline of the cavity line: the shared sample, timed steps sized to about max_seconds."""
+    n = SOLID_SAMPLE_N
+    _, per_step, _ = cpu_reference_sample(n, 0, 1)
+    steps = max(2, int(max_seconds / max(per_step, 1e-3)))
+    mlups, secs, cores = cpu_reference_sample(n, 1, steps)
+    return {
+        "value": mlups / 1e3, "unit": "GLUPS", "cores": cores, "kind": "reference",
+        "sample": f"reference EsotericPullSolver<D3Q19> BGK+Smagorinsky, cavity as static solid mask (its 3-pass "
+                  f"solid step), {n}^3, 1 warmup + {steps} timed steps ({secs:.1f} s), all host threads",
+    }
+
+
+def cpu_inplace_sample(n, seconds=CPU_SAMPLE_SECONDS, warmup=10):
+    """The reference's own benchmark CLI on its plain in-place path (apps/cfd-bench.cpp:173-191):
+    D3Q19 periodic BGK Taylor-Green, cfd-bench --streaming in-place, all host threads, timed steps
+    sized to about `seconds`.  Returns the parsed cfd_solvers.benchmark.v1 record."""
+    import subprocess
+
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+
+    def cli(w, k):
+        out = subprocess.run([str(O.REF_CLI), "--lattice", "d3q19", "--nx", str(n), "--ny", str(n), "--nz", str(n),
+                              "--warmup", str(w), "--steps", str(k), "--streaming", "in-place", "--threads",
+                              str(threads), "--json"], capture_output=True, text=True, check=True).stdout
+        return json.loads(out.strip().splitlines()[-1])
+
+    probe = cli(1, 2)
+    per_step = probe["seconds"] / 2
+    steps = max(3, int(seconds / max(per_step, 1e-6)))
+    rec = cli(min(warmup, steps), steps)
+    rec["threads"] = threads
+    return rec
+
+
+def cpu_inplace_baselines():
+    """cfd-bench in-place at the plain-method size (64^3) and at 512^3, one sample length each."""
+    out = {}
+    for n in (64, 512):
+        r = cpu_inplace_sample(n)
+        out[f"in_place_periodic_{n}"] = {
+            "value": r["mlups"] / 1e3, "unit": "GLUPS", "cores": r["threads"], "kind": "reference",
+            "sample": f"reference cfd-bench --lattice d3q19 --nx {n} --ny {n} --nz {n} --streaming in-place "
+                      f"--threads {r['threads']} (periodic BGK, Taylor-Green), {r['steps']} timed steps "
+                      f"({r['seconds']:.1f} s)",
+        }
+    return out
+
+
+def c1_plain_method(torch, cs, device, warmup=10, steps=100):
+    """The plain-method configuration on the GPU: D3Q19 BGK, 64^3 periodic, tau 0.6, Taylor-Green A = 0.05,
+    FP32, 10 warmup + 100 timed steps; fields and checksum against the reference's own dump of the same run
+    (tests/golden/reference_fixtures, made by the reference CPU build)."""
+    root = os.path.dirname(os.path.abspath(__file__))
+    data = np.load(os.path.join(root, "tests", "golden", "reference_fixtures.npz"))
+    meta = json.load(open(os.path.join(root, "tests", "golden", "reference_fixtures.json")))["c1_d3q19_tg64"]
+    n = 64
+    s = cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(nx=n, ny=n, nz=n, tau=0.6, device=device))
+    try:
+        s.initialize_taylor_green(0.05)
+        ms_warm = time_steps(torch, s, warmup)
+        ms = time_steps(torch, s, steps)
+        got = [np.asarray(a)[:: meta["stride"]] for a in s.compute_macroscopic()]
+        checksum = s.checksum()
+    finally:
+        s.close()
+    ref = [data[f"c1_d3q19_tg64_{k}"] for k in ("rho", "ux", "uy", "uz")]
+    err = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(got, ref))
+    return {
+        "workload": "D3Q19 BGK 64^3 periodic, tau 0.6, Taylor-Green A 0.05 (k = 2 pi / 64), FP32, "
+                    f"{warmup} warmup + {steps} timed steps",
+        "glups": n ** 3 * steps / (ms / 1e3) / 1e9, "ms_per_step": ms / steps, "warmup_ms": ms_warm,
+        "l2": "lattice 19.9 MB < 126 MB L2 (L2-resident, as the configuration is)",
+        "parity": {"max_abs_rho_u_vs_reference": err, "gate": 2e-5, "checksum": checksum,
+                   "reference_checksum": meta["checksum"], "checksum_rel": abs(checksum - meta["checksum"]) /
+                   abs(meta["checksum"]), "pass": err < 2e-5 and abs(checksum - meta["checksum"]) <
+                   1e-6 * abs(meta["checksum"])},
+    }
+
+
 def voxelizer_measure(torch, device, n=512, subdivisions=7, cpu_sample=True):
     """The device voxelizer on a closed sphere of 20*4^s triangles over an n^3 grid.
 
@@ -700,27 +789,30 @@ def resident_coupling_measure(torch, cs, n, device, particles=1 << 20, reps=5):
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's own CPU path for the cavity workload on the host cores: the same lattice as
+    cpu_baseline (SOLID_SAMPLE_N^3, 3-pass solid step, Smagorinsky), smaller only when W + K steps of
+    it would not end within about two minutes."""
     if rank != 0:
         return 0
-    from oracle import oracle as O
-
-    # Calibrate a per-step sample so that warmup + steps end within ~2 minutes.
-    probe_n = 96
-    mlups, secs, cores = cpu_reference_sample(probe_n, 1, 2)
-    rate = mlups * 1e6
+    _, per_step, _ = cpu_reference_sample(SOLID_SAMPLE_N, 0, 1)
     budget = 110.0
-    edge = int((rate * budget / max(1, args.steps + args.warmup)) ** (1.0 / 3.0))
-    edge = max(48, min(args.n, edge))
+    edge = SOLID_SAMPLE_N
+    if per_step * (args.steps + args.warmup) > budget:
+        edge = int(SOLID_SAMPLE_N * (budget / (per_step * (args.steps + args.warmup))) ** (1.0 / 3.0))
+        edge = max(48, edge)
     mlups, secs, cores = cpu_reference_sample(edge, args.warmup, args.steps)
     glups = mlups / 1e3
-    sample = (f"reference EsotericPullSolver<D3Q19> BGK+Smagorinsky, cavity as static solid mask, "
-              f"{edge}^3 cells per step, {args.warmup} warmup + {args.steps} timed steps (3-pass solid path)")
+    sample = (f"reference EsotericPullSolver<D3Q19> BGK+Smagorinsky, cavity as static solid mask (its 3-pass "
+              f"solid step), {edge}^3, {args.warmup} warmup + {args.steps} timed steps ({secs:.1f} s), "
+              f"all host threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"D3Q19 lid-driven cavity {args.n}^3 (reference CPU sample {edge}^3)",
-                   "lattice": "d3q19", "n": args.n, "sample_n": edge},
+                   "lattice": "d3q19", "n": args.n, "sample_n": edge,
+                   "convention": "GLUPS = all cells (walls included) x steps / time, the reference's MLUPS "
+                                 "convention (apps/cfd-bench.cpp:109-112)"},
         "cpu_baseline": {"value": glups, "unit": "GLUPS", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": glups, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
@@ -935,6 +1027,10 @@ def main(argv=None):
                 "l2": f"populations {cells * q * (4 if args.storage == 'fp32' else 2) / 1e9:.1f} GB > 126 MB L2 "
                       "(no flush needed)",
                 "fluid_cells": cavity_fluid_cells(n),
+                "glups_fluid": cavity_fluid_cells(n) * args.steps * world / (ms_max / 1e3) / 1e9,
+                "convention": "value = all cells (walls included) x steps / time, the reference's MLUPS "
+                              "convention (apps/cfd-bench.cpp:109-112); glups_fluid counts fluid cells only, "
+                              "as roofline.achieved's bytes do",
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
@@ -963,6 +1059,7 @@ def main(argv=None):
     if rank == 0 and not args.no_variants and world == 1:
         vs = max(20, args.steps // 2)
         if args.storage == "fp32" and args.lattice == "d3q19":
+            variants["c1_plain_method_64"] = c1_plain_method(torch, cs, local_rank)
             f16 = measure_variant(torch, cs, n, "d3q19", "fp16s", vs, local_rank)
             f16["speedup_vs_fp32"] = f16["glups"] / value
             f16["roofline_frac"] = f16["achieved_gbs"] / hbm_peak()[0]
@@ -986,13 +1083,8 @@ def main(argv=None):
             line["variants"] = variants
             line["targets"] = target_summary(line, variants)
         if not args.no_cpu_baseline and world == 1:
-            edge = min(n, 256)
-            mlups, secs, cores = cpu_reference_sample(edge, 1, 5)
-            line["cpu_baseline"] = {
-                "value": mlups / 1e3, "unit": "GLUPS", "cores": cores, "kind": "reference",
-                "sample": f"reference EsotericPullSolver<D3Q19> BGK+Smagorinsky, cavity as static solid mask, "
-                          f"{edge}^3, 1 warmup + 5 timed steps ({secs:.1f} s), all host threads",
-            }
+            line["cpu_baseline"] = cpu_solid_baseline()
+            line["cpu_baseline_in_place"] = cpu_inplace_baselines()
         print(json.dumps(line), flush=True)
 
     if dist is not None:

@@ -216,6 +216,7 @@ SIGNATURES = {
     "cfdx_debug_audit_classify": (_i, [ctypes.c_uint32] * 5 + [ctypes.POINTER(ctypes.c_uint)]),
     "cfdx_release_scratch": (_i, [_i]),
     "cfdx_debug_fail_allocations": (_i, [_i]),
+    "cfdx_lbm_debug_force_wide_slots": (_i, [_H, _i]),
     "cfdx_debug_retry_allocations": (_i, [_i, ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 

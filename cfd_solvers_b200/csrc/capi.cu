@@ -327,19 +327,22 @@ struct cfdx_lbm {
     // The paired-cell step kernel needs FP32/FP16 storage, an even nx and
     // element offsets that fit 32 bits.
     bool paired_eligible() const {
-        return key.storage != kStoreF64 && cfg.nx % 2U == 0U &&
-               static_cast<unsigned long long>(key.q) * N < (1ULL << 32) &&
+        return key.storage != kStoreF64 && cfg.nx % 2U == 0U && offsets_fit() &&
                (shape.block_x == 0 || shape.block_x % 32 == 0);
     }
+    // Element offsets of every slot fit 32 bits (q * cells < 2^32), unless the
+    // test hook cfdx_debug_force_wide_slots sends a small lattice through the
+    // 64-bit slot-pointer kernels that larger lattices use.
+    bool force_wide = false;
+    bool offsets_fit() const { return !force_wide && static_cast<unsigned long long>(key.q) * N < (1ULL << 32); }
     // The wall-aware FP16 pair kernel needs FP16 storage, an even nx and
     // element offsets that fit 32 bits.
     bool w2_eligible() const {
-        return key.storage == kStoreF16S && cfg.nx % 2U == 0U &&
-               static_cast<unsigned long long>(key.q) * N < (1ULL << 32) &&
+        return key.storage == kStoreF16S && cfg.nx % 2U == 0U && offsets_fit() &&
                (shape.block_x == 0 || shape.block_x * shape.block_y == 128);
     }
     void choose_variant() {
-        key.narrow = static_cast<unsigned long long>(key.q) * N < (1ULL << 32);
+        key.narrow = offsets_fit();
         key.w2 = (variant == 3 || variant == 4) && w2_eligible();
         key.w2_pipe = variant != 4;
         key.paired = !key.w2 && (variant == 2 || (variant == 0 && paired_eligible() &&
@@ -2711,6 +2714,16 @@ CFDX_API int cfdx_release_scratch(int device) {
 CFDX_API int cfdx_debug_fail_allocations(int count) {
     g_fail_allocations.store(count > 0 ? count : 0);
     return CFDX_OK;
+}
+
+CFDX_API int cfdx_lbm_debug_force_wide_slots(cfdx_lbm* h, int wide) {
+    return guarded([&] {
+        checked(h);
+        h->force_wide = wide != 0;
+        if (h->force_wide) h->variant = h->variant == 1 ? 1 : 0; // the paired kernels need 32-bit offsets
+        h->choose_variant();
+        refresh_near_list(h, false);
+    });
 }
 
 CFDX_API int cfdx_debug_retry_allocations(int count, unsigned long long* retries) {

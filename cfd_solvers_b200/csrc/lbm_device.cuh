@@ -379,7 +379,9 @@ __device__ __forceinline__ void bounce_fixup(const LbmArgs& a, const typename S:
 }
 
 // Moving-wall correction for values held in FP16 storage units: the
-// correction 6 w_k rho (c_k . u_wall) is scaled by s_k.
+// correction 6 w_k rho (c_k . u_wall) is scaled by s_k.  Explicitly rounded
+// operations: the paired kernels call this out of line, the one-cell kernel
+// inline, and both must round alike.
 template <class L, int P = 0>
 __device__ __forceinline__ void moving_wall_pairs_scaled(const LbmArgs& a, u32 n, const Nbr& o, float rw, float* h) {
     if constexpr (P < L::PAIRS) {
@@ -387,12 +389,12 @@ __device__ __forceinline__ void moving_wall_pairs_scaled(const LbmArgs& a, u32 n
         const int idb = a.flags[n + nbr_off<L, j>(o)] & kFlagTypeMask;
         if (idb >= 2) {
             const float cu = cdot<L, i, float>(a.wall_u[idb][0], a.wall_u[idb][1], a.wall_u[idb][2]);
-            h[i] += a.scale[i] * (6.0F * float(L::w(i)) * rw * cu);
+            h[i] = __fmaf_rn(a.scale[i], __fmul_rn(__fmul_rn(6.0F * float(L::w(i)), rw), cu), h[i]);
         }
         const int idf = a.flags[n + nbr_off<L, i>(o)] & kFlagTypeMask;
         if (idf >= 2) {
             const float cu = cdot<L, j, float>(a.wall_u[idf][0], a.wall_u[idf][1], a.wall_u[idf][2]);
-            h[j] += a.scale[j] * (6.0F * float(L::w(j)) * rw * cu);
+            h[j] = __fmaf_rn(a.scale[j], __fmul_rn(__fmul_rn(6.0F * float(L::w(j)), rw), cu), h[j]);
         }
         moving_wall_pairs_scaled<L, P + 1>(a, n, o, rw, h);
     }
@@ -404,7 +406,7 @@ __device__ __forceinline__ void gather_fixup_scaled(const LbmArgs& a, u32 n, con
     if (flag & kFlagNearMoving) {
         float rho0 = 1.0F;
 #pragma unroll
-        for (int d = 0; d < L::Q; ++d) rho0 += h[d] * a.inv_scale[d];
+        for (int d = 0; d < L::Q; ++d) rho0 = __fmaf_rn(h[d], a.inv_scale[d], rho0);
         const float rw = rho0 > 1.0e-8F ? rho0 : 1.0e-8F;
         moving_wall_pairs_scaled<L>(a, n, o, rw, h);
     }
@@ -866,7 +868,7 @@ __device__ __forceinline__ V scaled_moment2(const V* v, const float* inv, V init
 // sqrt for the Smagorinsky rate: hardware reciprocal square root (2 ulp);
 // the eddy viscosity needs no correctly rounded square root, and FP16
 // storage rounding is far larger.  x >= 0; x = 0 gives 0.
-__device__ __forceinline__ float les_sqrt(float x) { return x * rsqrtf(fmaxf(x, 1.0e-30F)); }
+__device__ __forceinline__ float les_sqrt(float x) { return __fmul_rn(x, rsqrtf(fmaxf(x, 1.0e-30F))); }
 
 // n: the first cell of V's lanes (lane k is cell n + k).
 template <class L, bool LES, bool GRAY, bool FORCE, class V>
@@ -928,7 +930,10 @@ __device__ __forceinline__ void collide_scaled(const LbmArgs& a, u32 n, V* h) {
         const float tau0 = a.tau_f, kles = a.les_k_f;
         V tau = v_map(q, [&](float qq, int k) {
             const float r = v_lane(rho, k);
-            return r > 0.0F ? 0.5F * (tau0 + les_sqrt(tau0 * tau0 + kles * les_sqrt(qq) * v_lane(irho, k))) : tau0;
+            // tau0/2 + sqrt(tau0^2 + K sqrt(Q) / rho) / 2, every operation explicitly rounded: the
+            // same bits in every kernel, whatever the compiler hoists out of a loop around it
+            const float t = __fmul_rn(__fmul_rn(kles, les_sqrt(qq)), v_lane(irho, k));
+            return r > 0.0F ? __fmul_rn(0.5F, __fadd_rn(tau0, les_sqrt(__fmaf_rn(tau0, tau0, t)))) : tau0;
         });
         omega = v_map(tau, [](float t, int) { return rcp(t); });
         omega_m = v_map(tau, [&](float t, int k) { return omega_minus_of<float>(a, t, v_lane(omega, k)); });

@@ -312,7 +312,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Resident 128-thread blocks per SM (register cap 65536 / (128 * blocks)).
 // The macros exist for tuning builds.
 #ifndef CFDX_W2_MIN_BLOCKS
-#define CFDX_W2_MIN_BLOCKS 6
+#define CFDX_W2_MIN_BLOCKS 5
 #endif
 #ifndef CFDX_W2_MIN_BLOCKS_Q27
 #define CFDX_W2_MIN_BLOCKS_Q27 5
@@ -323,10 +323,10 @@ template <class L> constexpr int w2_min_blocks() { return L::Q == 27 ? CFDX_W2_M
 // form are laid out for it, so their offsets are immediates).
 constexpr unsigned kW2Threads = 128;
 
-// Shared memory of the pipelined form: two stages of the word slots per thread.
-template <class L> constexpr unsigned w2_smem_bytes() {
-    return 2U * static_cast<unsigned>(W2Words<L>::count) * kW2Threads * 4U;
-}
+// Shared memory of the pipelined form: two stages of the word slots per
+// thread, in groups of four words so that one 16-byte load reads four.
+template <class L> constexpr unsigned w2_groups() { return (static_cast<unsigned>(W2Words<L>::count) + 3U) / 4U; }
+template <class L> constexpr unsigned w2_smem_bytes() { return 2U * w2_groups<L>() * kW2Threads * 16U; }
 
 // Grid: x over pairs (blockDim.x threads, nx/2 pairs), y over rows
 // (blockDim.x * blockDim.y == kW2Threads), z over chunks of a.planes planes.
@@ -363,18 +363,20 @@ __global__ void __launch_bounds__(kW2Threads, w2_min_blocks<L>()) k_step_w2(cons
             });
         }
     } else {
-        // word k of stage st: w2_stage[(st * W + k) * kW2Threads + tid]
-        extern __shared__ u32 w2_stage[];
+        // word k of stage st: component k % 4 of w2_stage[(st * G + k / 4) * kW2Threads + tid]
+        constexpr u32 G = w2_groups<L>();
+        extern __shared__ uint4 w2_stage[];
         const u32 tid = threadIdx.y * blockDim.x + threadIdx.x;
-        const u32* mine = w2_stage + tid;
+        const uint4* mine = w2_stage + tid;
         const u32 sbase = static_cast<u32>(__cvta_generic_to_shared(mine));
-        constexpr u32 kStageBytes = W * kW2Threads * 4U;
+        constexpr u32 kStageBytes = G * kW2Threads * 16U;
         const auto issue = [&](u32 z, u32 st) -> unsigned {
             W2Ctx cn = c;
             w2_plane(a, z, cn);
             const u32 s0 = sbase + st * kStageBytes;
             w2_words<L>(a, cn, [&](auto K, const __half* p) {
-                cp_async4<decltype(K)::value * kW2Threads * 4>(s0, p);
+                constexpr int k = decltype(K)::value;
+                cp_async4<(k / 4) * kW2Threads * 16 + (k % 4) * 4>(s0, p);
             });
             return flags_of(cn);
         };
@@ -387,14 +389,22 @@ __global__ void __launch_bounds__(kW2Threads, w2_min_blocks<L>()) k_step_w2(cons
             cp_async_commit();
             cp_async_wait<1>();
             if (both_walls(fl2)) continue;
-            const u32* words = mine + st * (W * kW2Threads);
-            u32 raw[W];
+            const uint4* groups = mine + st * (G * kW2Threads);
+            u32 raw[4 * G];
 #pragma unroll
-            for (int k = 0; k < W; ++k) raw[k] = words[k * kW2Threads];
+            for (u32 g = 0; g < G; ++g) {
+                const uint4 v = groups[g * kW2Threads];
+                raw[4 * g] = v.x;
+                raw[4 * g + 1] = v.y;
+                raw[4 * g + 2] = v.z;
+                raw[4 * g + 3] = v.w;
+            }
             w2_plane(a, z, c);
             // merging stores re-read the words from the stage, intact until the next issue
-            w2_cell_pair<L, LES, FLAGS, GRAY>(a, c, raw, fl2,
-                                              [&](auto K) { return words[decltype(K)::value * kW2Threads]; });
+            w2_cell_pair<L, LES, FLAGS, GRAY>(a, c, raw, fl2, [&](auto K) {
+                constexpr int k = decltype(K)::value;
+                return reinterpret_cast<const u32*>(groups + (k / 4) * kW2Threads)[k % 4];
+            });
         }
         cp_async_wait_all();
     }

@@ -606,6 +606,15 @@ CFDX_API int cfdx_debug_audit_classify(uint32_t reads, uint32_t writes, uint32_t
  * without exhausting the device. */
 CFDX_API int cfdx_debug_fail_allocations(int count);
 
+/* Test hook: with wide != 0 the handle addresses slots through 64-bit
+ * per-parity pointers, the form every kernel uses when q * cells >= 2^32
+ * (e.g. D3Q27 above about 542^3), instead of 32-bit element offsets, so that
+ * small lattices test that path; the paired-cell kernels, which need the
+ * offsets, are not used then, and the adjoint refuses the handle as it
+ * refuses such lattices.  Reference: no counterpart (esoteric_pull.hpp:304-310
+ * indexes with size_t throughout). */
+CFDX_API int cfdx_lbm_debug_force_wide_slots(cfdx_lbm* lbm, int wide);
+
 /* Test hook of the out-of-memory retry: the next `count` device allocations
  * (count >= 0; < 0 leaves it unchanged) see out-of-memory from their first
  * attempt, return the idle scratch-pool memory to the driver and try again.

@@ -27,9 +27,13 @@ def fields_err(a, b):
     return max(maxabs(x, y) for x, y in zip(a, b))
 
 
-def make(cs, q, nx, ny, nz, **kw):
+def make(cs, q, nx, ny, nz, wide=False, **kw):
+    """A solver; `wide` sends it through the 64-bit slot-pointer kernels of lattices with q*cells >= 2^32."""
     lattice = {19: "d3q19", 27: "d3q27"}[q]
-    return cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(nx=nx, ny=ny, nz=nz, lattice=lattice, **kw))
+    s = cs.EsotericPullCudaSolver(cs.InPlaceLbmConfig(nx=nx, ny=ny, nz=nz, lattice=lattice, **kw))
+    if wide:
+        s.library.call("cfdx_lbm_debug_force_wide_slots", s.handle, 1)
+    return s
 
 
 # ------------------------------------------------------------ vs reference
@@ -156,16 +160,17 @@ def case_inputs(kind, gray, local, nx, ny, nz, seed=7):
     return flags, wall_u, ns, la
 
 
+@pytest.mark.parametrize("wide", [False, True], ids=["offsets32", "pointers64"])
 @pytest.mark.parametrize("q", [19, 27])
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
-def test_oracle_feature_matrix(engine, oracle_mod, q, case):
+def test_oracle_feature_matrix(engine, oracle_mod, q, case, wide):
     name, kw, _, kind, gray, local = case
     nx, ny, nz = 17, 15, 13
     kw = dict(tau=0.62, **kw)
     flags, wall_u, ns, la = case_inputs(kind, gray, local, nx, ny, nz)
     L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, q, nx, ny, nz, kw), flags=flags, wall_u=wall_u,
                                  solid_fraction=ns, local_a=la)
-    with make(engine, q, nx, ny, nz, **kw) as s:
+    with make(engine, q, nx, ny, nz, wide=wide, **kw) as s:
         if flags is not None:
             s.set_flags(flags)
             if wall_u is not None:
@@ -191,14 +196,15 @@ def test_oracle_feature_matrix(engine, oracle_mod, q, case):
         assert got["kinetic_energy"] == pytest.approx(ref["kinetic_energy"], rel=1e-3, abs=1e-9)
 
 
+@pytest.mark.parametrize("wide", [False, True], ids=["offsets32", "pointers64"])
 @pytest.mark.parametrize("q", [19, 27])
-def test_fp64_storage_matches_fp64_oracle(engine, oracle_mod, q):
+def test_fp64_storage_matches_fp64_oracle(engine, oracle_mod, q, wide):
     nx, ny, nz = 17, 15, 13
     kw = dict(tau=0.62, storage="fp64", collision="trt", smagorinsky_les=True, smagorinsky_cs=0.1,
               acceleration_x=1e-5)
     flags = (np.random.default_rng(3).random(nx * ny * nz) < 0.1).astype(np.uint8)
     L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, q, nx, ny, nz, kw), storage="f64", flags=flags)
-    with make(engine, q, nx, ny, nz, **kw) as s:
+    with make(engine, q, nx, ny, nz, wide=wide, **kw) as s:
         s.set_flags(flags)
         s.initialize_taylor_green(0.04)
         L.init_taylor_green(0.04)
@@ -207,8 +213,9 @@ def test_fp64_storage_matches_fp64_oracle(engine, oracle_mod, q):
         assert fields_err(s.compute_macroscopic(), L.macroscopic()) < 1e-12
 
 
+@pytest.mark.parametrize("wide", [False, True], ids=["offsets32", "pointers64"])
 @pytest.mark.parametrize("q", [19, 27])
-def test_fp16_storage_matches_fp16_oracle(engine, oracle_mod, q):
+def test_fp16_storage_matches_fp16_oracle(engine, oracle_mod, q, wide):
     nx, ny, nz = 17, 15, 13
     # nearest rounding: the oracle's FP16 codec rounds to nearest (ties to even;
     # the GPU's nearest mode rounds ties away from zero, a 1-ulp difference
@@ -218,13 +225,50 @@ def test_fp16_storage_matches_fp16_oracle(engine, oracle_mod, q):
     scale = np.array([2.0 ** round(np.log2(1 / w)) for w in oracle_weights(q)], np.float32)
     L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, q, nx, ny, nz, kw), storage="f16s", flags=flags,
                                  scale=scale)
-    with make(engine, q, nx, ny, nz, **kw) as s:
+    with make(engine, q, nx, ny, nz, wide=wide, **kw) as s:
         s.set_flags(flags)
         s.initialize_taylor_green(0.04)
         L.init_taylor_green(0.04)
         s.step(9)
         L.step(9)
         assert fields_err(s.compute_macroscopic(), L.macroscopic()) < 5e-5
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("storage", ["fp32", "fp16s", "fp64"])
+def test_wide_slot_pointers_equal_offsets_bitwise(engine, q, storage):
+    """Lattices with q*cells >= 2^32 address slots through 64-bit pointers: same bits as 32-bit offsets."""
+    nx, ny, nz = 18, 15, 13
+    n = nx * ny * nz
+    rng = np.random.default_rng(5)
+    flags = (rng.random(n) < 0.15).astype(np.uint8)
+    flags[rng.random(n) < 0.04] = 2
+    ns = rng.uniform(0, 0.2, n).astype(np.float32)
+    out = []
+    for wide in (False, True):
+        with make(engine, q, nx, ny, nz, wide=wide, tau=0.6, storage=storage, collision="trt",
+                  smagorinsky_les=True, smagorinsky_cs=0.1, acceleration_x=1e-5) as s:
+            s.set_flags(flags)
+            s.set_wall_velocity(2, 0.05, 0.0, -0.02)
+            s.set_solid_fraction(ns)
+            s.initialize_taylor_green(0.04)
+            s.step(9)
+            out.append((s.logical_populations(), s.compute_macroscopic(), s.reduce()))
+    (la, ma, ra), (lb, mb, rb) = out
+    assert np.array_equal(la.view(np.uint32), lb.view(np.uint32))
+    for a, b in zip(ma, mb):
+        assert np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
+    assert ra == rb
+
+
+def test_adjoint_refuses_wide_slot_lattices(engine):
+    """The adjoint kernels address slots by 32-bit offsets only: lattices beyond them are refused."""
+    nx = ny = nz = 12
+    with make(engine, 19, nx, ny, nz, wide=True, tau=0.6, collision="trt", acceleration_x=1e-5) as s:
+        s.set_solid_fraction(np.full(nx * ny * nz, 0.05, np.float32))
+        s.initialize_uniform()
+        with pytest.raises(ValueError, match="2\\^32"):
+            s.adjoint_forward(8, 4)
 
 
 def oracle_weights(q):
