@@ -182,7 +182,7 @@ struct cfdx_lbm {
     // wall-aware z-marching FP16 pair kernel with / without its cp.async pipeline
     int variant = 0;
     std::uint32_t planes = 0; // z-planes per thread of that kernel (0: kDefaultPlanes)
-    static constexpr std::uint32_t kDefaultPlanes = 8;
+    static constexpr std::uint32_t kDefaultPlanes = 4; // measured: 4 > 8 > 16 on the 512^3 cavity
     // Automatic choice between the one-cell and the paired-cell kernel, from
     // B200 measurements (GLUPS, FP16 D3Q19, one-cell vs two-cell): pairs win
     // only on lattices without flags (BGK periodic 512^3: 64.3 vs 55.6).  With
@@ -194,6 +194,15 @@ struct cfdx_lbm {
     // registers than the kernel can hold).
     static bool paired_default(int storage, int q, bool flags) {
         return storage == kStoreF16S && q == 19 && !flags;
+    }
+    // The wall-aware z-marching pair kernel (k_step_w2, cp.async pipeline, 4
+    // planes per thread) against the one-cell kernel, B200, FP16, GLUPS:
+    // D3Q19 TRT + Smagorinsky cavity 512^3 50.6 vs 48.6; without Smagorinsky
+    // 51.9 vs 52.0; D3Q27 Smagorinsky cavity 29.6 vs 34.1; gray channels (D3Q27
+    // 256^3, D3Q19 128^3) 15.7 vs 30.7 and 29.2 vs 36.4; 512x256x256 sphere pack
+    // 40.8 vs 45.6.  Automatic choice: where it wins.
+    static bool w2_default(int storage, int q, bool flags, bool les, bool gray) {
+        return storage == kStoreF16S && q == 19 && flags && les && !gray;
     }
     double les_k = 0.0;
     std::uint64_t h2d = 0, d2h = 0, syncs = 0;
@@ -343,7 +352,9 @@ struct cfdx_lbm {
     }
     void choose_variant() {
         key.narrow = offsets_fit();
-        key.w2 = (variant == 3 || variant == 4) && w2_eligible();
+        key.w2 = (variant == 3 || variant == 4 ||
+                  (variant == 0 && w2_default(key.storage, key.q, key.flags, key.les, key.gray))) &&
+                 w2_eligible();
         key.w2_pipe = variant != 4;
         key.paired = !key.w2 && (variant == 2 || (variant == 0 && paired_eligible() &&
                                                   paired_default(key.storage, key.q, key.flags)));

@@ -66,7 +66,6 @@ def test_paired_variant_requires_even_nx(engine):
         s.step(3)
 
 
-
 # The wall-aware FP16 pair kernel (variants 3 and 4) marches along z; plane
 # counts that do not divide nz leave a short last chunk, and rows of 256 cells
 # span more than one warp.
