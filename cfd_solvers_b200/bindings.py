@@ -42,6 +42,8 @@ WALL = 1
 MAX_WALL_IDS = 16
 REDUCE_COUNT = 7
 SIDE_LOWER = 0
+STEP_EDGES = 1     # CFDX_STEP_EDGES: a slab's edge planes (the cells its halo messages carry)
+STEP_INTERIOR = 2  # CFDX_STEP_INTERIOR: the remaining planes of that step
 SIDE_UPPER = 1
 
 
@@ -152,6 +154,7 @@ SIGNATURES = {
     "cfdx_lbm_raw_populations": (_i, [_H, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
     "cfdx_lbm_set_launch_shape": (_i, [_H, _i, _i, _i]),
     "cfdx_lbm_set_step_planes": (_i, [_H, _i]),
+    "cfdx_lbm_step_phase": (_i, [_H, _i]),
     "cfdx_lbm_reduce_noalloc": (_i, [_H, ctypes.POINTER(ctypes.c_double)]),
     "cfdx_lbm_set_tau": (_i, [_H, ctypes.c_float]),
     "cfdx_lbm_checkpoint_save": (_i, [_H, ctypes.c_char_p]),

@@ -216,6 +216,7 @@ struct cfdx_lbm {
         std::uint32_t z_begin = 0, z_extent = 0, nz_global = 0;
         std::uint8_t due = 0; // sides (bit 0 lower, bit 1 upper) whose message of the last step is not yet in
         bool fresh = false;   // a step ran since the last initialisation or checkpoint load
+        bool interior_due = false; // a two-phase step ran its edge planes; its interior is still to run
         bool whole_ring() const { return on && z_extent == nz_global; }
     } slab;
     cudaEvent_t event = nullptr; // ordering point between two slabs' streams (cfdx_lbm_halo_exchange)
@@ -280,6 +281,8 @@ struct cfdx_lbm {
         a.ny = static_cast<std::uint32_t>(cfg.ny);
         a.nz = static_cast<std::uint32_t>(cfg.nz);
         a.N = static_cast<std::uint32_t>(N);
+        a.z_first = 0U; // step launches cover every plane unless a two-phase step narrows them
+        a.z_end = a.nz;
         a.has_force = (cfg.acceleration_x != 0.0F || cfg.acceleration_y != 0.0F || cfg.acceleration_z != 0.0F ||
                        local_a != nullptr)
                           ? 1
@@ -395,8 +398,12 @@ void require(bool ok, const char* message) {
     if (!ok) throw std::invalid_argument(message);
 }
 
-cfdx_lbm* checked(cfdx_lbm* h) {
+// mid_step: the call may come between the two phases of a slab's step
+// (cfdx_lbm_step_phase); every other call needs whole steps.
+cfdx_lbm* checked(cfdx_lbm* h, bool mid_step = false) {
     if (!h) throw std::invalid_argument("null cfdx_lbm handle");
+    if (!mid_step && h->slab.interior_due)
+        throw std::invalid_argument("the slab's two-phase step is half done: run its CFDX_STEP_INTERIOR phase first");
     h->set_device();
     return h;
 }
@@ -452,6 +459,7 @@ void init_state(cfdx_lbm* h, const InitSpec& in) {
     // Every slot a step reads now holds its own cell's state: no message is due.
     h->slab.due = 0;
     h->slab.fresh = false;
+    h->slab.interior_due = false;
 }
 
 void ensure_reduce(cfdx_lbm* h) {
@@ -1029,7 +1037,7 @@ int last_step_plan(const cfdx_lbm* h, int side, HaloEntry* send, HaloEntry* recv
 }
 
 cfdx_lbm* checked_slab(cfdx_lbm* h) {
-    checked(h);
+    checked(h, true); // halo messages travel while the interior of the step runs
     require(h->slab.on, "not a slab handle (cfdx_lbm_create_slab)");
     return h;
 }
@@ -1174,6 +1182,43 @@ CFDX_API int cfdx_lbm_step(cfdx_lbm* h, std::uint64_t count) {
     });
 }
 
+// Planes [z0, z1) of the step that starts at h->t (whole-lattice arguments otherwise).
+void launch_planes(cfdx_lbm* h, std::uint64_t ts, std::uint32_t z0, std::uint32_t z1) {
+    LbmArgs a = h->args();
+    h->set_step(a, ts);
+    a.z_first = z0;
+    a.z_end = z1;
+    dim3 g = h->grid();
+    g.z = z1 - z0;
+    check_cuda(launch_step(h->key, a, g, h->step_block(), h->stream), "step kernel");
+}
+
+CFDX_API int cfdx_lbm_step_phase(cfdx_lbm* h, int phase) {
+    return guarded([&] {
+        checked(h, true);
+        require(h->slab.on, "the two-phase step is for slab handles (cfdx_lbm_create_slab)");
+        require(phase == CFDX_STEP_EDGES || phase == CFDX_STEP_INTERIOR,
+                "phase must be CFDX_STEP_EDGES or CFDX_STEP_INTERIOR");
+        const std::uint32_t ze = h->slab.z_extent; // own planes 1..ze; 0 and ze + 1 are ghosts
+        if (phase == CFDX_STEP_EDGES) {
+            require(!h->slab.interior_due, "the interior phase of the previous step has not run");
+            require(h->slab.due == 0, "the halo messages of the slab's previous step have not all been received");
+            h->adj.ready = false;
+            launch_planes(h, h->t, 1U, 2U);
+            if (ze > 1U) launch_planes(h, h->t, ze, ze + 1U);
+            ++h->t;
+            h->slab.due = 3;
+            h->slab.fresh = true;
+            h->slab.interior_due = true;
+            if (h->slab.whole_ring()) exchange_cut(h, h);
+        } else {
+            require(h->slab.interior_due, "no interior is due: run CFDX_STEP_EDGES first");
+            if (ze > 2U) launch_planes(h, h->t - 1U, 2U, ze); // slabs of one or two planes are all edges
+            h->slab.interior_due = false;
+        }
+    });
+}
+
 CFDX_API int cfdx_lbm_slab_info(cfdx_lbm* h, std::uint32_t* z_begin, std::uint32_t* z_extent, std::uint32_t* nz_global) {
     return guarded([&] {
         require(h != nullptr && z_begin != nullptr && z_extent != nullptr && nz_global != nullptr,
@@ -1280,7 +1325,7 @@ CFDX_API int cfdx_lbm_halo_exchange(cfdx_lbm* lower, cfdx_lbm* upper) {
 
 CFDX_API int cfdx_lbm_synchronize(cfdx_lbm* h) {
     return guarded([&] {
-        checked(h);
+        checked(h, true);
         h->sync();
     });
 }

@@ -85,6 +85,11 @@ struct LbmArgs {
     std::uint32_t near_count;
     // z-planes each thread of the z-marching pair kernel (k_step_w2) steps.
     std::uint32_t planes;
+    // Planes [z_first, z_end) a step launch covers (0 and nz for a whole step;
+    // a slab's two-phase step launches its edge planes and its interior
+    // separately).  Honoured by every step kernel (k_step, k_step_w2, k_step_h2,
+    // k_step_x2); the other kernels cover the whole lattice.
+    std::uint32_t z_first, z_end;
 };
 
 // Parameters of the adjoint kernels (lbm_adjoint.cuh).

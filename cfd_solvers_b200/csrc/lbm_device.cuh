@@ -1071,7 +1071,7 @@ __global__ void __launch_bounds__(128, step_min_blocks<L, S, GRAY>()) k_step(con
     using R = typename S::R;
     const u32 x = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
-    const u32 z0 = blockIdx.z * CPT;
+    const u32 z0 = a.z_first + blockIdx.z * CPT;
     if (x >= a.nx || y >= a.ny) return;
     R fin[CPT][L::Q];
     std::uint8_t flag[CPT];
@@ -1080,7 +1080,7 @@ __global__ void __launch_bounds__(128, step_min_blocks<L, S, GRAY>()) k_step(con
     for (int c = 0; c < CPT; ++c) {
         const u32 z = z0 + c;
         const u32 n = (z * a.ny + y) * a.nx + x;
-        live[c] = z < a.nz;
+        live[c] = z < a.z_end;
         flag[c] = 0;
         if constexpr (FLAGS) {
             if (live[c]) {

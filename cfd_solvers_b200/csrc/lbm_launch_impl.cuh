@@ -49,7 +49,7 @@ cudaError_t step_paired(const LbmArgs& a, dim3 b, cudaStream_t s) {
         return cudaErrorInvalidValue;
     } else {
         const unsigned pairs = (a.nx + 1U) / 2U;
-        dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, a.nz);
+        dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, a.z_end - a.z_first);
         if constexpr (sizeof(typename S::T) == 2) {
             // interior pairs two cells per thread, then the pairs with walls one cell per thread
             k_step_h2<L, LES, FL, GR><<<g, b, 0, s>>>(a);
@@ -88,7 +88,8 @@ cudaError_t step_w2(const KernelKey& k, const LbmArgs& a, dim3 b, cudaStream_t s
         if (b.x * b.y != kW2Threads || b.z != 1U) return cudaErrorInvalidValue;
         const unsigned pairs = a.nx / 2U;
         const unsigned planes = a.planes == 0U ? 1U : a.planes;
-        dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, (a.nz + planes - 1U) / planes);
+        const unsigned span = a.z_end - a.z_first;
+        dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, (span + planes - 1U) / planes);
         if (k.w2_pipe) {
             const cudaError_t e =
                 w2_carveout(k_step_w2<L, LES, FL, GR, true>, w2_smem_bytes<L>(), w2_min_blocks<L>());

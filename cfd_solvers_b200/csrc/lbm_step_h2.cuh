@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(128, LES ? CFDX_H2_MIN_BLOCKS_LES : CFDX_H2_MI
     H2Ctx c;
     c.x0 = 2U * (blockIdx.x * blockDim.x + threadIdx.x);
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
-    const u32 z = blockIdx.z;
+    const u32 z = a.z_first + blockIdx.z;
     if (c.x0 >= a.nx || y >= a.ny) return;
     c.row = (z * a.ny + y) * a.nx;
     c.n0 = c.row + c.x0;
@@ -186,6 +186,7 @@ __global__ void __launch_bounds__(128, step_min_blocks<L, S>()) k_step_list(cons
     const u32 n = a.near_list[k];
     const u32 plane = a.nx * a.ny;
     const u32 z = n / plane;
+    if (z < a.z_first || z >= a.z_end) return; // outside this launch's planes
     const u32 r = n - z * plane;
     const u32 y = r / a.nx;
     const u32 x = r - y * a.nx;

@@ -329,15 +329,16 @@ template <class L> constexpr unsigned w2_groups() { return (static_cast<unsigned
 template <class L> constexpr unsigned w2_smem_bytes() { return 2U * w2_groups<L>() * kW2Threads * 16U; }
 
 // Grid: x over pairs (blockDim.x threads, nx/2 pairs), y over rows
-// (blockDim.x * blockDim.y == kW2Threads), z over chunks of a.planes planes.
+// (blockDim.x * blockDim.y == kW2Threads), z over chunks of a.planes planes
+// of [a.z_first, a.z_end).
 template <class L, bool LES, bool FLAGS, bool GRAY, bool PIPE>
 __global__ void __launch_bounds__(kW2Threads, w2_min_blocks<L>()) k_step_w2(const __grid_constant__ LbmArgs a) {
     constexpr int W = W2Words<L>::count;
     const u32 x0 = 2U * (blockIdx.x * blockDim.x + threadIdx.x);
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x0 >= a.nx || y >= a.ny) return;
-    const u32 zb = blockIdx.z * a.planes;
-    const u32 ze = min(a.nz, zb + a.planes);
+    const u32 zb = a.z_first + blockIdx.z * a.planes;
+    const u32 ze = min(a.z_end, zb + a.planes);
     W2Ctx c;
     w2_thread(a, x0, y, c);
     const auto flags_of = [&](const W2Ctx& cc) -> unsigned {

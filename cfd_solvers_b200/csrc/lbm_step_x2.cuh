@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(128, pair_min_blocks<S>()) k_step_x2(const __g
     c.lane = threadIdx.x & 31U;
     c.x0 = 2U * (blockIdx.x * blockDim.x + threadIdx.x);
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
-    const u32 z = blockIdx.z;
+    const u32 z = a.z_first + blockIdx.z;
     if (y >= a.ny) return; // warp-uniform: a warp never spans rows
     c.valid = c.x0 < a.nx;
     c.row = (z * a.ny + y) * a.nx;

@@ -37,6 +37,8 @@ from .lbm import EsotericPullCudaSolver, InPlaceLbmConfig, MacroscopicFields, _L
 
 SIDE_LOWER = B.SIDE_LOWER
 SIDE_UPPER = B.SIDE_UPPER
+STEP_EDGES = B.STEP_EDGES
+STEP_INTERIOR = B.STEP_INTERIOR
 
 
 def partition_axis(extent: int, coordinate: int, partitions: int) -> tuple[int, int]:
@@ -172,6 +174,11 @@ class SlabSolver(EsotericPullCudaSolver):
 
         return torch.empty(self._halo_bytes, dtype=torch.uint8, device=f"cuda:{self._config.device}")
 
+    def step_phase(self, phase: int):
+        """One phase of a two-phase step: STEP_EDGES (the edge planes, after which the messages can be
+        packed) or STEP_INTERIOR (the rest of that step); equal to step(1) bit for bit."""
+        self._call("cfdx_lbm_step_phase", int(phase))
+
     def pack(self, side: int, buffer):
         """Writes the message of `side` for the step just taken into `buffer` (device, stream-ordered)."""
         self._check_buffer(buffer)
@@ -267,6 +274,12 @@ class DistributedEsotericPullSolver:
         self._exchanger = SlabExchanger(g, group)
         self._buffers = None if ranks == 1 else [self.solver.message_buffer() for _ in range(4)]
         self._stream = self.solver.torch_stream() if hasattr(self.solver, "torch_stream") else None
+        # The exchange runs on a stream of its own while the slab's stream steps the interior.
+        self._comm_stream = None
+        if self._buffers is not None and self._stream is not None and hasattr(self.solver, "step_phase"):
+            import torch
+
+            self._comm_stream = torch.cuda.Stream(device=f"cuda:{config.device}")
 
     # ------------------------------------------------------------ lifecycle
     def close(self):
@@ -335,10 +348,38 @@ class DistributedEsotericPullSolver:
 
     # ------------------------------------------------------------ stepping
     def step(self, count: int = 1):
+        """`count` steps, each followed by its halo exchange.
+
+        With a CUDA slab on more than one rank every step runs in two phases
+        (reference distributed_pull.hpp:97-116, interior overlapped with the
+        boundary exchange): the edge planes, then the messages are packed and
+        sent on a communication stream while the slab's stream steps the
+        interior planes; the unpacks wait for both.
+        """
         for _ in range(int(count)):
+            if self._comm_stream is not None:
+                self._overlapped_step()
+                continue
             self.solver.step(1)
             if self._buffers is not None:
                 self._exchange()
+
+    def _overlapped_step(self):
+        import torch
+
+        s = self.solver
+        send_lo, send_up, recv_lo, recv_up = self._buffers
+        s.step_phase(STEP_EDGES)
+        s.pack(SIDE_LOWER, send_lo)
+        s.pack(SIDE_UPPER, send_up)
+        comm = self._comm_stream
+        comm.wait_stream(self._stream)
+        with torch.cuda.stream(comm):
+            self._exchanger.exchange(send_lo, send_up, recv_lo, recv_up)
+        s.step_phase(STEP_INTERIOR)
+        self._stream.wait_stream(comm)
+        s.unpack(SIDE_LOWER, recv_lo)
+        s.unpack(SIDE_UPPER, recv_up)
 
     def _exchange(self):
         s = self.solver
@@ -465,9 +506,20 @@ def virtual_exchange(slabs: Sequence[SlabSolver]):
         s.exchange_with(slabs[(r + 1) % len(slabs)])
 
 
-def virtual_step(slabs: Sequence[SlabSolver], count: int = 1):
-    """`count` steps of all slabs with an exchange after each (reference virtual_step)."""
+def virtual_step(slabs: Sequence[SlabSolver], count: int = 1, phases: bool = False):
+    """`count` steps of all slabs with an exchange after each (reference virtual_step).
+
+    With `phases` every slab steps its edge planes, the cuts exchange, and then
+    the slabs step their interiors (the order of the overlapped multi-process
+    step); the results are the same bits."""
     for _ in range(int(count)):
+        if phases:
+            for s in slabs:
+                s.step_phase(STEP_EDGES)
+            virtual_exchange(slabs)
+            for s in slabs:
+                s.step_phase(STEP_INTERIOR)
+            continue
         for s in slabs:
             s.step(1)
         virtual_exchange(slabs)

@@ -373,6 +373,21 @@ CFDX_API int cfdx_halo_plan(int lattice, int odd, int side, uint32_t z_extent, c
 /* Bytes of one message (chunks * nx * ny * storage bytes). */
 CFDX_API int cfdx_lbm_halo_bytes(cfdx_lbm* lbm, size_t* bytes);
 
+/* One time step of a slab in two launches, so that its halo exchange can
+ * overlap the interior of the step.  CFDX_STEP_EDGES steps the slab's first
+ * and last own planes -- the cells whose stores the messages carry -- and
+ * counts the time step: from then on the messages of the step can be packed
+ * (cfdx_lbm_halo_pack) and sent.  CFDX_STEP_INTERIOR steps the remaining
+ * planes.  The arriving messages may be unpacked before or after the
+ * interior phase (they fill slots no cell of the slab touches during the
+ * step), but before the next step.  Between the phases only the halo calls,
+ * cfdx_lbm_synchronize and cfdx_lbm_stream are accepted.  Results equal
+ * cfdx_lbm_step's bit for bit.  Reference: the interior / boundary-shell
+ * split of DistributedPullBlock (distributed_pull.hpp:97-116). */
+#define CFDX_STEP_EDGES 1
+#define CFDX_STEP_INTERIOR 2
+CFDX_API int cfdx_lbm_step_phase(cfdx_lbm* lbm, int phase);
+
 /* Copies the message for `side` of the step just taken into device memory
  * `buffer` (this device's or a peer's), stream-ordered after the step. */
 CFDX_API int cfdx_lbm_halo_pack(cfdx_lbm* lbm, int side, void* device_buffer);

@@ -83,6 +83,29 @@ def sliced(cfg, inputs, ranks, steps, mode="direct", variant=0):
             prepare(s, inputs, local=lambda a, k=1, g=s.slab: g.local(a, k))
         if mode == "direct":
             S.virtual_step(ss, steps)
+        elif mode == "phases":
+            S.virtual_step(ss, steps, phases=True)
+        elif mode == "phases_buffers":
+            # the overlapped multi-process order: edges, pack, interior, unpack
+            buffers = [(s.message_buffer(), s.message_buffer()) for s in ss]
+            for _ in range(steps):
+                for s in ss:
+                    s.step_phase(S.STEP_EDGES)
+                if ranks > 1:
+                    for s, (lo, up) in zip(ss, buffers):
+                        s.pack(S.SIDE_LOWER, lo)
+                        s.pack(S.SIDE_UPPER, up)
+                for s in ss:
+                    s.step_phase(S.STEP_INTERIOR)
+                if ranks == 1:
+                    continue
+                for s in ss:
+                    s.wait()
+                for r, s in enumerate(ss):
+                    s.unpack(S.SIDE_LOWER, buffers[(r - 1) % ranks][1])
+                    s.unpack(S.SIDE_UPPER, buffers[(r + 1) % ranks][0])
+                for s in ss:
+                    s.wait()
         else:
             buffers = [(s.message_buffer(), s.message_buffer()) for s in ss]
             for _ in range(steps):
@@ -137,6 +160,49 @@ def test_exchange_paths_and_thin_slabs(engine, mode, ranks):
     """13 planes over 5 slabs: slabs of 3 and 2 planes; over 13: one-plane slabs."""
     cfg, inputs = setup(engine, q=27, storage="fp16s", gray=True)
     check(engine, cfg, inputs, ranks, steps=5, mode=mode)
+
+
+@pytest.mark.parametrize("mode", ["phases", "phases_buffers"])
+@pytest.mark.parametrize("q, storage, variant", [(19, "fp32", 0), (27, "fp16s", 0), (19, "fp16s", 0),
+                                                 (19, "fp16s", 2), (19, "fp32", 2), (19, "fp16s", 3)])
+@pytest.mark.parametrize("ranks", [1, 2, 3, 5])
+def test_two_phase_step_matches_whole_lattice(engine, mode, q, storage, variant, ranks):
+    """Edge planes, exchange, interior (the overlapped order): the same bits as whole steps, for every
+    step kernel, with slabs of 5, 4, 3 and 2 planes (13 planes over up to 5 ranks)."""
+    cfg, inputs = setup(engine, q=q, shape=(16, 9, 13), storage=storage, les=True, gray=variant != 3,
+                        local_force=True)
+    check(engine, cfg, inputs, ranks, steps=5, mode=mode, variant=variant)
+
+
+def test_two_phase_step_order_is_enforced(engine):
+    from cfd_solvers_b200 import slabs as S
+
+    cfg, inputs = setup(engine, q=19, shape=(12, 10, 13))
+    ss = S.virtual_slabs(cfg, 2)
+    try:
+        for s in ss:
+            prepare(s, inputs, local=lambda a, k=1, g=s.slab: g.local(a, k))
+        with pytest.raises(ValueError, match="EDGES first"):
+            ss[0].step_phase(S.STEP_INTERIOR)
+        ss[0].step_phase(S.STEP_EDGES)
+        with pytest.raises(ValueError, match="half done"):
+            ss[0].reduce()
+        with pytest.raises(ValueError, match="half done"):
+            ss[0].step(1)
+        with pytest.raises(ValueError, match="interior phase of the previous step"):
+            ss[0].step_phase(S.STEP_EDGES)
+        ss[1].step_phase(S.STEP_EDGES)
+        ss[0].exchange_with(ss[1])  # halo calls are accepted between the phases
+        ss[1].exchange_with(ss[0])
+        for s in ss:
+            s.step_phase(S.STEP_INTERIOR)
+        ss[0].reduce()
+    finally:
+        for s in ss:
+            s.close()
+    with engine.EsotericPullCudaSolver(engine.InPlaceLbmConfig(nx=8, ny=8, nz=8)) as s:
+        with pytest.raises(ValueError, match="slab handles"):
+            s.library.call("cfdx_lbm_step_phase", s.handle, S.STEP_EDGES)
 
 
 @pytest.mark.parametrize("coll, les", [("bgk", False), ("trt", True)])
