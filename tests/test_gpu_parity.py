@@ -196,17 +196,22 @@ def test_oracle_feature_matrix(engine, oracle_mod, q, case, wide):
         assert got["kinetic_energy"] == pytest.approx(ref["kinetic_energy"], rel=1e-3, abs=1e-9)
 
 
+CAVITY_SHAPES = [(96, 96, 96), (256, 48, 40)]
+
+
+@pytest.mark.parametrize("shape", CAVITY_SHAPES, ids=[f"{a}x{b}x{c}" for a, b, c in CAVITY_SHAPES])
 @pytest.mark.parametrize("q", [19, 27])
-def test_cavity_trt_les_96_matches_oracle(engine, oracle_mod, q):
-    """The plain-method-at-scale shape on a lattice the oracle runs in seconds: 96^3 lid-driven cavity,
+def test_cavity_trt_les_96_matches_oracle(engine, oracle_mod, q, shape):
+    """The plain-method-at-scale shape on lattices the oracle runs in seconds: a lid-driven cavity,
     TRT (magic 3/16) + Smagorinsky Cs 0.1, tau 0.51, lid (0.1, 0, 0), FP32, from rest.  Rows of 96
-    cells span several warps and every row has long near-wall runs; 10 and 11 steps cover both
-    parities (the reference's in-place vs SYCL gate, tests/test_main.cpp:587-615, is 2e-5)."""
-    n = 96
+    cells span several warps, rows of 256 cells two 128-thread blocks, and every row has long
+    near-wall runs; 10 and 11 steps cover both parities (the reference's in-place vs SYCL gate,
+    tests/test_main.cpp:587-615, is 2e-5)."""
+    nx, ny, nz = shape
     kw = dict(tau=0.51, collision="trt", trt_magic=3.0 / 16.0, smagorinsky_les=True, smagorinsky_cs=0.1)
-    flags, wall_u, _, _ = case_inputs("cavity", False, False, n, n, n)
-    L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, q, n, n, n, kw), flags=flags, wall_u=wall_u)
-    with make(engine, q, n, n, n, **kw) as s:
+    flags, wall_u, _, _ = case_inputs("cavity", False, False, nx, ny, nz)
+    L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, q, nx, ny, nz, kw), flags=flags, wall_u=wall_u)
+    with make(engine, q, nx, ny, nz, **kw) as s:
         s.set_flags(flags)
         s.set_wall_velocity(2, *wall_u[2])
         s.initialize_uniform()
