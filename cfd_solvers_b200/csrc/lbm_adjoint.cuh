@@ -75,7 +75,8 @@ template <class R> struct CellState {
     R rho, irho, utx, uty, utz, ux, uy, uz, ax, ay, az;
 };
 
-template <class L, class R>
+// x: absolute populations, or deviations f - w when DELTA.
+template <class L, class R, bool DELTA = false>
 __device__ __forceinline__ CellState<R> cell_state(const LbmArgs& a, u32 n, const R* x, bool force) {
     CellState<R> c;
     R r = x[0], jx = R(0), jy = R(0), jz = R(0);
@@ -90,8 +91,8 @@ __device__ __forceinline__ CellState<R> cell_state(const LbmArgs& a, u32 n, cons
         if constexpr (L::cz(i) > 0) jz += d;
         if constexpr (L::cz(i) < 0) jz -= d;
     });
-    c.rho = r;
-    c.irho = rcp_unbiased(r);
+    c.rho = DELTA ? r + R(1) : r;
+    c.irho = rcp_unbiased(c.rho);
     c.utx = jx * c.irho;
     c.uty = jy * c.irho;
     c.utz = jz * c.irho;
@@ -104,13 +105,15 @@ __device__ __forceinline__ CellState<R> cell_state(const LbmArgs& a, u32 n, cons
 }
 
 // One cell of the adjoint step: nin are the gathered adjoint values
-// (nin_k = mu_{opp k}), x the forward's incoming populations (absolute).
-// Writes the flipped result nout (nout_i = lambda_{opp i}) and this cell's
-// dJ/dn_s and dJ/dtau contributions.
-template <class L, class R>
+// (nin_k = mu_{opp k}), x the forward's incoming populations (absolute, or
+// the deviations f - w when DELTA: FP16-shifted frames, whose deviations are
+// what the loads decode and which keep the non-equilibrium differences below
+// free of the weights' cancellation).  Writes the flipped result nout
+// (nout_i = lambda_{opp i}) and this cell's dJ/dn_s and dJ/dtau contributions.
+template <class L, class R, bool DELTA>
 __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x, const R* nin, R* nout, bool force,
                                              R dwp, R dwm, double& g_ns, double& g_tau) {
-    const CellState<R> c = cell_state<L, R>(a, n, x, force);
+    const CellState<R> c = cell_state<L, R, DELTA>(a, n, x, force);
     const R tau = p_tau<R>(a);
     const R wp = rcp(tau);
     const R wm = omega_minus_of<R>(a, tau, wp);
@@ -124,13 +127,18 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
     // rest direction: forward pieces and adjoint moments
     constexpr R w0 = R(L::w(0));
     const R mu0 = nin[0];
-    const R neq0 = x[0] - w0 * c.rho * base;
+    // x_0 - w0 rho base; with deviations x_0 - w0 (rho base - 1)
+    const R neq0 = DELTA ? x[0] - w0 * (c.rho * base - R(1)) : x[0] - w0 * c.rho * base;
     const R F0 = -R(3) * w0 * uF;
-    const R fs0 = x[0] - wp * neq0 + gp * F0;
-    R gns = mu0 * (x[0] - fs0);
-    R gtp = mu0 * (-neq0 - R(0.5) * F0);
-    R gtm = R(0);
-    R m0 = w0 * mu0, mx = R(0), my = R(0), mz = R(0);
+    // Pair sums for dC/dn_s and dC/dtau: with s, d the pair sum and
+    // difference of x and sneq = s - 2 w rho (base + 4.5 (c.u)^2),
+    // dneq = d - 6 w rho c.u their non-equilibrium parts,
+    //   SA = sum sigma sneq,  SB = sum delta dneq,  SD = sum delta d.
+    // The pairs' Guo terms sF = 2 w (9 (c.u)(c.F) - 3 u.F), dF = 6 w c.F enter
+    // only through sum sigma sF = 18 u.M.F - 6 u.F m0' and sum delta dF = 6 m.F,
+    // with m0' = m0 - w0 mu0 the pairs' share of m0, so no per-pair force term.
+    R SA = R(0), SB = R(0), SD = R(0);
+    R m0p = R(0), mx = R(0), my = R(0), mz = R(0);
     R Mxx = R(0), Myy = R(0), Mzz = R(0), Mxy = R(0), Mxz = R(0), Myz = R(0);
     R ms[L::PAIRS], md[L::PAIRS];
     static_for<0, L::PAIRS>([&](auto PP) {
@@ -144,7 +152,7 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
         ms[p] = sg;
         md[p] = dl;
         const R ws = w * sg, wd = w * dl;
-        m0 += ws;
+        m0p += ws;
         mx += signed_sum<cx, 0, 0>(wd, R(0), R(0));
         my += signed_sum<cy, 0, 0>(wd, R(0), R(0));
         mz += signed_sum<cz, 0, 0>(wd, R(0), R(0));
@@ -154,23 +162,17 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
         Mxy += signed_sum<cx * cy, 0, 0>(ws, R(0), R(0));
         Mxz += signed_sum<cx * cz, 0, 0>(ws, R(0), R(0));
         Myz += signed_sum<cy * cz, 0, 0>(ws, R(0), R(0));
-        // forward pair quantities for dC/dn_s and dC/dtau
         const R s = x[i] + x[j], d = x[i] - x[j];
         const R cu = cdot<L, i>(ux, uy, uz);
-        const R cF = cdot<L, i>(Fx, Fy, Fz);
-        const R sneq = s - R(2) * w * c.rho * (base + R(4.5) * cu * cu);
-        const R dneq = d - R(6) * w * c.rho * cu;
-        const R sF = R(2) * w * (R(9) * cu * cF - R(3) * uF);
-        const R dF = R(6) * w * cF;
-        const R sst = s - wp * sneq + gp * sF;
-        const R dst = d - wm * dneq + gm * dF;
-        gns += R(0.5) * (sg * (s - sst) - dl * (d + dst));
-        gtp += R(0.5) * sg * (-sneq - R(0.5) * sF);
-        gtm += R(0.5) * dl * (-dneq - R(0.5) * dF);
+        const R t = base + R(4.5) * cu * cu;
+        // s - 2 w rho t, with deviations s - 2 w (rho t - 1); d has no weight part
+        const R sneq = DELTA ? s - (R(2) * w) * (c.rho * t - R(1)) : s - (R(2) * w * c.rho) * t;
+        const R dneq = d - (R(6) * w * c.rho) * cu;
+        SA += sg * sneq;
+        SB += dl * dneq;
+        SD += dl * d;
     });
-    g_ns = double(gns);
-    g_tau = double((R(1) - ns) * (dwp * gtp + dwm * gtm));
-
+    const R m0 = w0 * mu0 + m0p;
     const R ax = c.ax, ay = c.ay, az = c.az;
     const R Mux = Mxx * ux + Mxy * uy + Mxz * uz;
     const R Muy = Mxy * ux + Myy * uy + Myz * uz;
@@ -178,10 +180,22 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
     const R Max = Mxx * ax + Mxy * ay + Mxz * az;
     const R May = Mxy * ax + Myy * ay + Myz * az;
     const R Maz = Mxz * ax + Myz * ay + Mzz * az;
+    // F = rho a: u.M.F = rho u.M.a, m.F = rho m.a
+    const R uMa = ux * Max + uy * May + uz * Maz;
+    const R ma = mx * ax + my * ay + mz * az;
+    const R SF = R(18) * c.rho * uMa - R(6) * uF * m0p;
+    const R DF = R(6) * c.rho * ma;
+    // x_0 - C_0 = wp neq0 - gp F0, and per pair s - sst = wp sneq - gp sF,
+    // d + dst = 2 d - wm dneq + gm dF
+    const R gns = mu0 * (wp * neq0 - gp * F0) + R(0.5) * (wp * SA - gp * SF - R(2) * SD + wm * SB - gm * DF);
+    const R gtp = mu0 * (-neq0 - R(0.5) * F0) - R(0.5) * SA - R(0.25) * SF;
+    const R gtm = -R(0.5) * SB - R(0.25) * DF;
+    g_ns = double(gns);
+    g_tau = double((R(1) - ns) * (dwp * gtp + dwm * gtm));
+
     const R P = wp * (m0 * base + R(4.5) * (ux * Mux + uy * Muy + uz * Muz)) +
                 R(3) * wm * (mx * ux + my * uy + mz * uz) +
-                gp * (R(9) * (ux * Max + uy * May + uz * Maz) - R(3) * m0 * (ux * ax + uy * ay + uz * az)) +
-                R(3) * gm * (mx * ax + my * ay + mz * az);
+                gp * (R(9) * uMa - R(3) * m0 * (ux * ax + uy * ay + uz * az)) + R(3) * gm * ma;
     const R vx = wp * ux + gp * ax, vy = wp * uy + gp * ay, vz = wp * uz + gp * az;
     const R Vx = R(9) * (wp * Mux + gp * Max) - R(3) * m0 * vx + R(3) * wm * mx;
     const R Vy = R(9) * (wp * Muy + gp * May) - R(3) * m0 * vy + R(3) * wm * my;
@@ -189,15 +203,20 @@ __device__ __forceinline__ void adjoint_cell(const LbmArgs& a, u32 n, const R* x
     const R Vu = Vx * c.utx + Vy * c.uty + Vz * c.utz;
     const R keep = R(1) - ns;
     nout[0] = keep * (mu0 * (R(1) - wp) + P - Vu) + ns * mu0;
-    const R even0 = R(2) * (P - Vu);
+    // Per pair, with ls = keep (sigma (1 - wp) + 2 (P - Vu)) + ns sigma and
+    // ld = keep (delta (1 - wm) + 2 V.c_i) - ns delta: lambda_i = (ls + ld) / 2
+    // is stored in slot j (flipped), lambda_j = (ls - ld) / 2 in slot i.  The
+    // halves fold into per-cell coefficients.
+    const R as = R(0.5) * (keep * (R(1) - wp) + ns), bs = keep * (P - Vu);
+    const R ad = R(0.5) * (keep * (R(1) - wm) - ns);
+    const R kVx = keep * Vx, kVy = keep * Vy, kVz = keep * Vz;
     static_for<0, L::PAIRS>([&](auto PP) {
         constexpr int p = decltype(PP)::value;
         constexpr int i = 2 * p + 1, j = i + 1;
-        const R ls = keep * (ms[p] * (R(1) - wp) + even0) + ns * ms[p];
-        const R ld = keep * (md[p] * (R(1) - wm) + R(2) * cdot<L, i>(Vx, Vy, Vz)) - ns * md[p];
-        // lambda_i = (ls + ld) / 2 is stored in slot j (flipped), lambda_j in slot i
-        nout[i] = R(0.5) * (ls - ld);
-        nout[j] = R(0.5) * (ls + ld);
+        const R hs = ms[p] * as + bs;
+        const R hd = md[p] * ad + cdot<L, i>(kVx, kVy, kVz);
+        nout[i] = hs - hd;
+        nout[j] = hs + hd;
     });
 }
 
@@ -346,9 +365,8 @@ __global__ void __launch_bounds__(128, adjoint_min_blocks<L, S>()) k_adjoint_ste
             R xin[L::Q], nin[L::Q], nout[L::Q];
             gather_loads<L, S, FLAGS, true, false>(f, n, o, flag, xin);
             gather_loads<L, LS, FLAGS, true, false>(A.l, n, o, flag, nin);
-            to_absolute<L, S>(xin);
             double g_ns = 0.0;
-            adjoint_cell<L, R>(f, n, xin, nin, nout, f.has_force != 0, R(A.dwp), R(A.dwm), g_ns, g_tau);
+            adjoint_cell<L, R, S::delta>(f, n, xin, nin, nout, f.has_force != 0, R(A.dwp), R(A.dwm), g_ns, g_tau);
             scatter<L, LS, true, false>(A.l, n, o, nout, 0U);
             A.grad_ns[n] += g_ns;
         }
