@@ -330,14 +330,15 @@ __global__ void __launch_bounds__(128) k_adjoint_seed(const __grid_constant__ Ad
 // Resident blocks per SM the reverse step is compiled for (register cap
 // 65536 / (128 * blocks)).  Measured on B200 (adjoint step alone): D3Q19 at 8
 // blocks (64 registers) 0.098 ms vs 0.125 uncapped at 128^3 FP32 (reverse sweep
-// per step 173.4 us, against 174.0 at 7 blocks and 183.8 at 6, which spill less);
-// D3Q27 at 5 (96 registers) 1.24 ms vs 1.43 uncapped at 256^3 FP16 (reverse sweep
-// 1753 us, against 1785 at 6 blocks and 1972 at 4).
+// per step 173.4 us, against 174.0 at 7 blocks and 183.8 at 6, which spill less;
+// with the moment form of the gradient terms 160.5 us at 8, 164.9 at 7, 175.4 at 6);
+// D3Q27 FP16 at 256^3, reverse sweep per step: 1597 us at 6 blocks (80 registers,
+// no spill once the gradient terms came from the moments), 1654 at 5, 1670 at 7.
 #ifndef CFDX_ADJOINT_MIN_BLOCKS_Q19
 #define CFDX_ADJOINT_MIN_BLOCKS_Q19 8
 #endif
 #ifndef CFDX_ADJOINT_MIN_BLOCKS_Q27
-#define CFDX_ADJOINT_MIN_BLOCKS_Q27 5
+#define CFDX_ADJOINT_MIN_BLOCKS_Q27 6
 #endif
 template <class L, class S> constexpr int adjoint_min_blocks() {
     return sizeof(typename S::T) == 8 ? 1 : (L::Q == 19 ? CFDX_ADJOINT_MIN_BLOCKS_Q19 : CFDX_ADJOINT_MIN_BLOCKS_Q27);
