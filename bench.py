@@ -60,6 +60,8 @@ def parse_args(argv=None):
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-differentiation", action="store_true",
                    help="skip the adjoint workloads (128^3 D3Q19 FP32 and 256^3 D3Q27 FP16 gray TRT)")
+    p.add_argument("--subinterval", type=int, default=0,
+                   help="--case adjoint: sub-checkpoint interval of the reverse sweep (0: one level)")
     p.add_argument("--case", choices=["cavity", "adjoint", "precision"], default="cavity",
                    help="cavity: the headline line (default); adjoint / precision: only that workload at --n "
                         "(adjoint: gray TRT --lattice/--storage, --steps steps; precision: n x n/2 x n/2 sphere "
@@ -330,7 +332,7 @@ def misfit(s, ns, fluid, target, steps):
     return 0.5 * float(np.sum(r * r))
 
 
-def adjoint_gradient(torch, s, ns, fluid, target, steps, interval):
+def adjoint_gradient(torch, s, ns, fluid, target, steps, interval, subinterval=0):
     """(dJ/dn_s, dJ/dtau, timings) of the misfit through the discrete adjoint."""
     stream = torch.cuda.ExternalStream(s.stream())
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -338,7 +340,7 @@ def adjoint_gradient(torch, s, ns, fluid, target, steps, interval):
     s.initialize_uniform()
     s.wait()
     ev[0].record(stream)
-    s.adjoint_forward(steps, interval)
+    s.adjoint_forward(steps, interval, subinterval)
     ev[1].record(stream)
     f = s.compute_macroscopic()
     g = ((np.stack([f.ux, f.uy, f.uz]).astype(np.float64) - target) * fluid).astype(np.float32)
@@ -353,8 +355,12 @@ def adjoint_gradient(torch, s, ns, fluid, target, steps, interval):
     return grad.cpu().numpy(), gtau, ev[0].elapsed_time(ev[1]), e2.elapsed_time(ev[2])
 
 
-def adjoint_case(torch, cs, lattice, n, storage, steps, interval, device, seeds=(1, 2)):
-    """One differentiation workload: timings of forward, checkpointed forward and reverse sweep."""
+def adjoint_case(torch, cs, lattice, n, storage, steps, interval, device, seeds=(1, 2), subinterval=0):
+    """One differentiation workload: timings of forward, checkpointed forward and reverse sweep.
+
+    `subinterval` > 0 reverses each checkpoint segment in two levels of recompute (sub-checkpoints
+    every `subinterval` steps), which holds fewer frames for more recompute steps.
+    """
     from cfd_solvers_b200.cases import gray_field
 
     s, fluid = gray_solver(cs, lattice, n, storage, device)
@@ -368,13 +374,14 @@ def adjoint_case(torch, cs, lattice, n, storage, steps, interval, device, seeds=
         s.initialize_uniform()
         fwd_ms = time_steps(torch, s, steps)
         free0 = torch.cuda.mem_get_info()[0]
-        gns, gtau, afwd_ms, bwd_ms = adjoint_gradient(torch, s, ns, fluid, target, steps, interval)
+        gns, gtau, afwd_ms, bwd_ms = adjoint_gradient(torch, s, ns, fluid, target, steps, interval, subinterval)
         mem = s.adjoint_memory()
         s.adjoint_release()
     finally:
         s.close()
     return {
         "lattice": lattice, "n": n, "storage": storage, "steps": steps, "checkpoint_interval": interval,
+        "recompute_subinterval": subinterval,
         "forward_ms_per_step": fwd_ms / steps, "checkpointed_forward_ms_per_step": afwd_ms / steps,
         "adjoint_ms_per_step": bwd_ms / steps, "adjoint_over_forward": bwd_ms / fwd_ms,
         "forward_glups": cells * steps / (fwd_ms / 1e3) / 1e9,
@@ -434,7 +441,13 @@ def differentiation_variants(torch, cs, device, full=True):
     c4["fd_check"] = adjoint_fd_check(torch, cs, 32, 2000, 64, device)
     out["gray_d3q19_128_fp32"] = c4
     if full:
-        c5, _, _ = adjoint_case(torch, cs, "d3q27", 256, "fp16s", 4000, 64, device)
+        c5, g5, t5 = adjoint_case(torch, cs, "d3q27", 256, "fp16s", 4000, 64, device)
+        # The same run with two levels of recompute (sub-checkpoints every 8 steps): the ~57 GB of
+        # checkpoints plus 14 frames instead of 63, for about twice the recompute steps.
+        c5b, g5b, t5b = adjoint_case(torch, cs, "d3q27", 256, "fp16s", 4000, 64, device, subinterval=8)
+        c5["two_level_recompute"] = {k: c5b[k] for k in ("recompute_subinterval", "adjoint_ms_per_step",
+                                                         "adjoint_over_forward", "adjoint_buffers_gb")}
+        c5["two_level_recompute"]["gradients_bitwise_equal"] = bool(np.array_equal(g5, g5b) and t5 == t5b)
         # Gradient errors of FP16 storage against FP32 storage and the FP64 GPU adjoint (itself
         # pinned to the FP64 CPU adjoint) at 128^3: the FP32/FP64 checkpoints of the 256^3 run
         # would not fit in 180 GB with one level of checkpointing.
@@ -970,7 +983,7 @@ def main(argv=None):
             raise SystemExit("--case adjoint/precision run on one GPU")
         if args.case == "adjoint":
             out, _, _ = adjoint_case(torch, cs, args.lattice, args.n, args.storage, args.steps,
-                                     min(64, args.steps), local_rank)
+                                     min(64, args.steps), local_rank, subinterval=args.subinterval)
         else:
             out = precision_study(torch, cs, local_rank, shape=(args.n, args.n // 2, args.n // 2), steps=args.steps)
         print(json.dumps(out), flush=True)

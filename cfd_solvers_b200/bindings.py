@@ -160,6 +160,7 @@ SIGNATURES = {
     "cfdx_lbm_checkpoint_save": (_i, [_H, ctypes.c_char_p]),
     "cfdx_lbm_checkpoint_load": (_i, [_H, ctypes.c_char_p]),
     "cfdx_lbm_adjoint_forward": (_i, [_H, ctypes.c_uint64, ctypes.c_uint32]),
+    "cfdx_lbm_adjoint_set_subinterval": (_i, [_H, ctypes.c_uint32]),
     "cfdx_lbm_adjoint_backward": (_i, [_H, _vp, _vp, _vp, _vp, _i, _vp, _i, ctypes.POINTER(ctypes.c_double)]),
     "cfdx_lbm_adjoint_memory": (_i, [_H, ctypes.POINTER(_sz)]),
     "cfdx_lbm_adjoint_release": (_i, [_H]),

@@ -225,9 +225,11 @@ struct cfdx_lbm {
     // `interval` steps, recompute frames for one segment, the adjoint lattice
     // and the gradient accumulators.  Buffers are kept for reuse until
     // cfdx_lbm_adjoint_release or destroy.
+    std::uint32_t adjoint_sub = 0; // cfdx_lbm_adjoint_set_subinterval, for the next forward pass
     struct Adjoint {
         std::uint64_t t0 = 0, steps = 0, t_end = 0;
         std::uint32_t interval = 0;
+        std::uint32_t sub = 0;  // sub-checkpoint interval of the reverse sweep (0: one level)
         bool ready = false;     // a forward pass has run and nothing has changed since
         void* checkpoints = nullptr;
         std::size_t checkpoint_bytes = 0;
@@ -1720,12 +1722,25 @@ void adjoint_buffer(void** p, std::size_t* have, std::size_t bytes, const char* 
     *have = bytes;
 }
 
-void adjoint_reserve(cfdx_lbm* h, std::uint64_t steps, std::uint32_t interval) {
+// A segment of `len` steps is reversed with two levels of recompute when a
+// sub-checkpoint interval 2 <= sub < len is set.
+bool two_level(std::uint64_t sub, std::uint64_t len) { return sub >= 2U && sub < len; }
+
+// Recompute frames of the reverse sweep.  One level: interval - 1 frames,
+// the states inside a segment.  Two levels (sub-checkpoint interval m): the
+// ceil(interval / m) - 1 sub-checkpoints of a segment, then the m - 1 states
+// inside one sub-segment.  The forward pass, and the first recompute pass of
+// two levels, use two of the frames as ping-pong buffers.
+std::uint64_t adjoint_frames(std::uint64_t steps, std::uint32_t interval, std::uint32_t sub) {
+    const std::uint64_t len = std::min<std::uint64_t>(interval, steps);
+    if (!two_level(sub, len)) return std::max<std::uint64_t>(len - 1U, 2U);
+    return (len + sub - 1U) / sub - 1U + std::max<std::uint64_t>(sub - 1U, 2U);
+}
+
+void adjoint_reserve(cfdx_lbm* h, std::uint64_t steps, std::uint32_t interval, std::uint32_t sub) {
     auto& A = h->adj;
     const std::uint64_t segments = (steps + interval - 1U) / interval;
-    // interval - 1 recompute frames; the forward pass also uses two of them
-    // as its ping-pong buffers.
-    const std::uint64_t frames = std::max<std::uint64_t>(std::min<std::uint64_t>(interval, steps) - 1U, 2U);
+    const std::uint64_t frames = adjoint_frames(steps, interval, sub);
     const std::size_t lam_es = h->key.storage == kStoreF64 ? 8U : 4U;
     const dim3 g = h->grid();
     const std::size_t blocks = static_cast<std::size_t>(g.x) * g.y * g.z;
@@ -1747,13 +1762,31 @@ void adjoint_reserve(cfdx_lbm* h, std::uint64_t steps, std::uint32_t interval) {
     }
 }
 
+// One level: state k of segment `segment` (0: its checkpoint).
 void* adjoint_frame(cfdx_lbm* h, std::uint64_t segment, std::uint64_t k) {
     char* base = k == 0U ? static_cast<char*>(h->adj.checkpoints) + segment * h->f_bytes
                          : static_cast<char*>(h->adj.frames) + (k - 1U) * h->f_bytes;
     return base;
 }
+// Two levels: sub-checkpoint j >= 1 of the segment being reversed, and state
+// r >= 1 inside its sub-segment being reversed (`nsub` sub-checkpoints per
+// full segment, the checkpoint included).
+void* adjoint_subcheckpoint(cfdx_lbm* h, std::uint64_t j) {
+    return static_cast<char*>(h->adj.frames) + (j - 1U) * h->f_bytes;
+}
+void* adjoint_subframe(cfdx_lbm* h, std::uint64_t nsub, std::uint64_t r) {
+    return static_cast<char*>(h->adj.frames) + (nsub - 1U + r - 1U) * h->f_bytes;
+}
 
 } // namespace
+
+CFDX_API int cfdx_lbm_adjoint_set_subinterval(cfdx_lbm* h, std::uint32_t subinterval) {
+    return guarded([&] {
+        checked(h);
+        require(subinterval != 1U, "a sub-checkpoint interval is 0 (one level) or at least 2");
+        h->adjoint_sub = subinterval;
+    });
+}
 
 CFDX_API int cfdx_lbm_adjoint_forward(cfdx_lbm* h, std::uint64_t steps, std::uint32_t interval) {
     return guarded([&] {
@@ -1764,11 +1797,12 @@ CFDX_API int cfdx_lbm_adjoint_forward(cfdx_lbm* h, std::uint64_t steps, std::uin
         require(!h->moving_walls, "the adjoint does not cover moving walls");
         require(h->key.narrow, "the adjoint needs q * cells < 2^32");
         h->adj.ready = false;
-        adjoint_reserve(h, steps, interval);
+        adjoint_reserve(h, steps, interval, h->adjoint_sub);
         auto& A = h->adj;
         A.t0 = h->t;
         A.steps = steps;
         A.interval = interval;
+        A.sub = h->adjoint_sub;
         // The forward runs the out-of-place kernel the reverse sweep
         // recomputes with, so every recomputed frame equals the forward's
         // state bit for bit.  Checkpoints and frames all keep the layout of
@@ -1869,23 +1903,51 @@ CFDX_API int cfdx_lbm_adjoint_backward(cfdx_lbm* h, const float* g_rho, const fl
             const std::uint64_t ts = A.t0 + s * A.interval;
             const std::uint64_t len = std::min<std::uint64_t>(A.interval, A.t0 + A.steps - ts);
             const int P = static_cast<int>(A.t0 & 1U); // every checkpoint and frame keeps the layout of t0
+            // Recompute step from state `src` (time step ts + k - 1 of the forward) into `dst`.
+            const auto recompute = [&](void* src, void* dst, std::uint64_t k) -> cudaError_t {
+                LbmArgs a = h->args_at(src, es, P);
+                a.round_seed = h->round_seed(ts + k - 1U); // the forward's step at this time
+                return launch_step_oop(h->key, a, h->args_at(dst, es, P ^ 1), g, b, h->stream);
+            };
+            // Adjoint step k of the segment (reading its incoming state, the state k - 1).
+            const auto adjoint = [&](void* state) -> cudaError_t {
+                X.f = h->args_at(state, es, P);
+                X.l = h->args_at(A.lam, lam_es, static_cast<int>(parity & 1U));
+                ++parity;
+                return launch_adjoint_step(h->key, X, g, b, h->stream);
+            };
             // the segment's recompute and adjoint steps as one graph
             enqueue_captured(h, "adjoint segment kernels", [&]() -> cudaError_t {
-                for (std::uint64_t k = 1; k < len; ++k) {
-                    LbmArgs src = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
-                    src.round_seed = h->round_seed(ts + k - 1U); // the forward's step at this time
-                    const cudaError_t e =
-                        launch_step_oop(h->key, src, h->args_at(adjoint_frame(h, s, k), es, P ^ 1), g, b, h->stream);
-                    if (e != cudaSuccess) return e;
+                cudaError_t e = cudaSuccess;
+                if (!two_level(A.sub, len)) {
+                    for (std::uint64_t k = 1; k < len && e == cudaSuccess; ++k)
+                        e = recompute(adjoint_frame(h, s, k - 1U), adjoint_frame(h, s, k), k);
+                    for (std::uint64_t k = len; k >= 1U && e == cudaSuccess; --k) e = adjoint(adjoint_frame(h, s, k - 1U));
+                    return e;
                 }
-                for (std::uint64_t k = len; k >= 1U; --k) {
-                    X.f = h->args_at(adjoint_frame(h, s, k - 1U), es, P);
-                    X.l = h->args_at(A.lam, lam_es, static_cast<int>(parity & 1U));
-                    const cudaError_t e = launch_adjoint_step(h->key, X, g, b, h->stream);
-                    if (e != cudaSuccess) return e;
-                    ++parity;
+                // Two levels: first the sub-checkpoints (every m-th state, the
+                // others in two scratch frames), then each sub-segment from the
+                // last: its states from its sub-checkpoint, then its adjoint steps.
+                const std::uint64_t m = A.sub, nsub = (len + m - 1U) / m;
+                const std::uint64_t nsub_full = (std::min<std::uint64_t>(A.interval, A.steps) + m - 1U) / m;
+                const auto start = [&](std::uint64_t j) {
+                    return j == 0U ? adjoint_frame(h, s, 0) : adjoint_subcheckpoint(h, j);
+                };
+                void* cur = start(0);
+                for (std::uint64_t k = 1; k <= (nsub - 1U) * m && e == cudaSuccess; ++k) {
+                    void* dst = k % m == 0U ? adjoint_subcheckpoint(h, k / m) : adjoint_subframe(h, nsub_full, 1U + (k & 1U));
+                    e = recompute(cur, dst, k);
+                    cur = dst;
                 }
-                return cudaSuccess;
+                for (std::uint64_t j = nsub; j-- > 0U && e == cudaSuccess;) {
+                    const std::uint64_t k0 = j * m, kend = std::min<std::uint64_t>(k0 + m, len);
+                    const auto state = [&](std::uint64_t k) {
+                        return k == k0 ? start(j) : adjoint_subframe(h, nsub_full, k - k0);
+                    };
+                    for (std::uint64_t k = k0 + 1U; k < kend && e == cudaSuccess; ++k) e = recompute(state(k - 1U), state(k), k);
+                    for (std::uint64_t k = kend; k > k0 && e == cudaSuccess; --k) e = adjoint(state(k - 1U));
+                }
+                return e;
             });
         }
         check_cuda(launch_sum_partials(A.tau_partials, blocks, A.tau_out, h->stream), "adjoint tau reduction");

@@ -476,8 +476,15 @@ class EsotericPullCudaSolver:
         self._config = dataclasses.replace(self._config, tau=float(tau))
 
     # ------------------------------------------------------ discrete adjoint
-    def adjoint_forward(self, steps: int, interval: int = 64):
-        """Run `steps` steps keeping a checkpoint every `interval` steps for adjoint_backward."""
+    def adjoint_forward(self, steps: int, interval: int = 64, subinterval: int = 0):
+        """Run `steps` steps keeping a checkpoint every `interval` steps for adjoint_backward.
+
+        `subinterval` m (2 <= m < interval) makes the reverse sweep recompute
+        each segment in two levels, holding about interval/m + m lattice
+        frames instead of interval - 1, at about twice the recompute steps;
+        0 keeps one level.  The gradients are the same bit for bit.
+        """
+        self._call("cfdx_lbm_adjoint_set_subinterval", int(subinterval))
         self._call("cfdx_lbm_adjoint_forward", int(steps), int(interval))
 
     def adjoint_backward(self, g_ux, g_uy, g_uz, g_rho=None, grad_ns_out=None):

@@ -361,8 +361,11 @@ public:
     }
 
     // ------------------------------------------------ discrete adjoint (gray LBM)
-    // `steps` steps from the current state keeping a checkpoint every `interval` steps.
-    void adjoint_forward(std::uint64_t steps, std::uint32_t interval) {
+    // `steps` steps from the current state keeping a checkpoint every `interval` steps;
+    // `subinterval` 2 <= m < interval reverses each segment in two levels of recompute
+    // (fewer frames held, about twice the recompute steps), 0 in one.
+    void adjoint_forward(std::uint64_t steps, std::uint32_t interval, std::uint32_t subinterval = 0) {
+        cuda::check(cfdx_lbm_adjoint_set_subinterval(handle_, subinterval), "adjoint_forward");
         cuda::check(cfdx_lbm_adjoint_forward(handle_, steps, interval), "adjoint_forward");
     }
     struct AdjointGradient {

@@ -292,12 +292,22 @@ CFDX_API int cfdx_lbm_set_tau(cfdx_lbm* lbm, float tau);
  *
  * cfdx_lbm_adjoint_forward: runs `steps` steps from the current state like
  * cfdx_lbm_step, keeping a device copy of the lattice every `interval` steps
- * (ceil(steps/interval) copies, in the storage precision) plus
- * max(interval-1, 2) recompute frames.  It runs the out-of-place form of the
+ * (ceil(steps/interval) copies, in the storage precision) plus the reverse
+ * sweep's recompute frames (max(interval-1, 2) lattices with one level of
+ * recompute; see cfdx_lbm_adjoint_set_subinterval).  It runs the out-of-place form of the
  * step that the reverse sweep recomputes with, so the recomputed states equal
  * the forward's bit for bit; the final state equals cfdx_lbm_step(steps)'s to
  * within the last bit of the arithmetic type. */
 CFDX_API int cfdx_lbm_adjoint_forward(cfdx_lbm* lbm, uint64_t steps, uint32_t interval);
+
+/* Sub-checkpoint interval m of the reverse sweep for the following
+ * cfdx_lbm_adjoint_forward calls: 0 (the default) recomputes each segment once
+ * and holds its interval - 1 states; 2 <= m < interval recomputes it twice
+ * (first every m-th state, then each sub-segment of m steps from its
+ * sub-checkpoint) and holds ceil(interval/m) - 1 + max(m - 1, 2) frames
+ * instead, e.g. 14 instead of 63 for interval 64 and m = 8.  The gradients are
+ * bitwise the same.  1 is rejected (CFDX_ERR_INVALID). */
+CFDX_API int cfdx_lbm_adjoint_set_subinterval(cfdx_lbm* lbm, uint32_t subinterval);
 
 /* Reverse sweep for an objective J of the final state, given dJ/drho (N
  * floats, may be NULL) and dJ/du_x,y,z (N floats each) of the fields

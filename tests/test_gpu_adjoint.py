@@ -123,6 +123,36 @@ def test_adjoint_interval_invariance(engine, storage):
         assert gtau == out[0][1]
 
 
+@pytest.mark.parametrize("storage", ["fp32", "fp16s"])
+def test_adjoint_two_level_recompute_is_bitwise_equal(engine, storage):
+    """Sub-checkpoint intervals 2, 3, 5 and 7 under segments of 8 steps (the last one 7 steps: two
+    levels, and one level for m = 7) give the one-level gradients bit for bit, with fewer frames
+    (m = 7 holds 1 + 6, as many as one level)."""
+    steps, interval = 23, 8
+    kw, flags, ns, ustar = problem(19)
+    g = np.random.default_rng(5).normal(0, 1e-3, (3, NX * NY * NZ)).astype(np.float32)
+
+    def run(sub):
+        with solver(engine, 19, storage, kw, flags, ns) as s:
+            s.adjoint_forward(steps, interval, sub)
+            mem = s.adjoint_memory()
+            return s.adjoint_backward(g[0], g[1], g[2]), mem
+
+    (gns0, gtau0), mem0 = run(0)
+    for sub in (2, 3, 5, 7):
+        (gns, gtau), mem = run(sub)
+        assert np.array_equal(gns, gns0), sub
+        assert gtau == gtau0, sub
+        assert mem < mem0 if sub < 7 else mem == mem0, sub
+
+
+def test_adjoint_rejects_subinterval_one(engine):
+    kw, flags, ns, _ = problem(19)
+    with solver(engine, 19, "fp32", kw, flags, ns) as s:
+        with pytest.raises(ValueError):
+            s.adjoint_forward(4, 2, 1)
+
+
 def test_adjoint_keeps_forward_state_and_reuses_seed(engine):
     kw, flags, ns, _ = problem(19)
     g = np.random.default_rng(4).normal(0, 1e-3, (3, NX * NY * NZ)).astype(np.float32)
