@@ -175,6 +175,15 @@ struct cfdx_lbm {
     int reduce_blocks = 0;
     cudaStream_t stream = nullptr;
     std::uint64_t t = 0;
+    // Instantiated graph of kGraphSteps step launches, one per parity of its
+    // first step, with what it was captured from; replayed by later calls
+    // whose launches match it byte for byte (cfdx_lbm_step).
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        LbmArgs first{};
+        KernelKey key{};
+        dim3 grid, block;
+    } step_graph[2];
     float wall_u[kMaxWallIds][3]{};
     float scale[27]{};
     LaunchShape shape{};
@@ -262,7 +271,8 @@ struct cfdx_lbm {
     // Arguments for a lattice of this handle's shape at `lattice` (element
     // size `es` bytes), with the slot tables of parity `odd`.
     LbmArgs args_at(void* lattice, int elem_bytes, int odd) const {
-        LbmArgs a{};
+        LbmArgs a;
+        std::memset(&a, 0, sizeof a); // padding too: cached step graphs compare arguments byte for byte
         char* base = static_cast<char*>(lattice);
         const std::size_t es = static_cast<std::size_t>(elem_bytes);
         for (int d = 0; d < 27; ++d) a.fd[d] = d < key.q ? base + static_cast<std::size_t>(d) * N * es : nullptr;
@@ -502,6 +512,8 @@ void release(cfdx_lbm* h) {
     device_free(h->reduce_partials);
     device_free(h->reduce_out);
     release_adjoint(h);
+    for (auto& sg : h->step_graph)
+        if (sg.exec) cudaGraphExecDestroy(sg.exec);
     if (h->host_reduce) cudaFreeHost(h->host_reduce);
     if (h->event) cudaEventDestroy(h->event);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1080,16 +1092,21 @@ void exchange_cut(cfdx_lbm* lo, cfdx_lbm* up) {
 
 namespace {
 
-// Long step loops replay a CUDA graph of kGraphSteps step launches instead of
-// launching each step: on small lattices a step is shorter than its launch
-// (32^3: 5.3 us per launched step), and a graph also shortens the gaps between
-// kernels.  The graph is captured within the call from the same argument
-// blocks the loop would launch and replayed whole, so results are unchanged;
-// it is not kept across calls, since any call may change the arguments.
+// Step loops of kGraphSteps or more steps replay a CUDA graph of kGraphSteps
+// step launches instead of launching each step: on small lattices a step is
+// shorter than its launch (32^3: 5.3 us per launched step), and a graph also
+// shortens the gaps between kernels.  The graph is captured from the argument
+// blocks the loop would launch, so results are unchanged, and kept on the
+// handle (one per parity of the first step): a later call replays it when its
+// first step's arguments, kernel key and launch shape equal the captured ones
+// byte for byte, and captures a new one otherwise -- any call that changes a
+// parameter, a buffer or the kernel choice changes one of them.  The steps of
+// a graph differ only in parity (kGraphSteps is even) and in the FP16 rounding
+// seed, which FP32 and FP64 kernels do not read (it is zeroed here).
 // Excluded: slabs (an exchange follows every step), FP16 storage (its rounding
 // seed changes every step) and streams that are already being captured.
-constexpr std::uint64_t kGraphSteps = 32;
-constexpr std::uint64_t kGraphMinSteps = 2 * kGraphSteps;
+constexpr std::uint64_t kGraphSteps = 8;
+constexpr std::uint64_t kGraphMinSteps = kGraphSteps;
 
 bool graph_steps_eligible(const cfdx_lbm* h, std::uint64_t count) {
     if (count < kGraphMinSteps || h->slab.on || h->key.storage == kStoreF16S) return false;
@@ -1101,28 +1118,50 @@ bool graph_steps_eligible(const cfdx_lbm* h, std::uint64_t count) {
     return status == cudaStreamCaptureStatusNone;
 }
 
+// Arguments of the step at time step ts as a step graph holds them.
+LbmArgs graph_step_args(const cfdx_lbm* h, const LbmArgs& a, std::uint64_t ts) {
+    LbmArgs s = a;
+    h->set_step(s, ts);
+    s.round_seed = 0U;
+    return s;
+}
+
+bool same_dim(dim3 x, dim3 y) { return x.x == y.x && x.y == y.y && x.z == y.z; }
+
 // Runs whole replays of a kGraphSteps-step graph from time step h->t; returns the steps run.
-std::uint64_t step_graphs(cfdx_lbm* h, LbmArgs& a, dim3 g, dim3 b, std::uint64_t count) {
+std::uint64_t step_graphs(cfdx_lbm* h, const LbmArgs& a, dim3 g, dim3 b, std::uint64_t count) {
+    static_assert(kGraphSteps % 2U == 0U, "a replay must end on the parity it starts with");
     const std::uint64_t replays = count / kGraphSteps;
-    check_cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-    cudaError_t launched = cudaSuccess;
-    for (std::uint64_t i = 0; i < kGraphSteps && launched == cudaSuccess; ++i) {
-        h->set_step(a, h->t + i); // parity and (unused outside FP16) rounding seed of step t + i
-        launched = launch_step(h->key, a, g, b, h->stream);
+    auto& sg = h->step_graph[h->t & 1U];
+    const LbmArgs first = graph_step_args(h, a, h->t);
+    const bool cached = sg.exec != nullptr && std::memcmp(&sg.first, &first, sizeof first) == 0 &&
+                        std::memcmp(&sg.key, &h->key, sizeof h->key) == 0 && same_dim(sg.grid, g) &&
+                        same_dim(sg.block, b);
+    if (!cached) {
+        if (sg.exec) cudaGraphExecDestroy(sg.exec);
+        sg.exec = nullptr;
+        check_cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        cudaError_t launched = cudaSuccess;
+        for (std::uint64_t i = 0; i < kGraphSteps && launched == cudaSuccess; ++i)
+            launched = launch_step(h->key, graph_step_args(h, a, h->t + i), g, b, h->stream);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ended = cudaStreamEndCapture(h->stream, &graph);
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t made =
+            launched == cudaSuccess && ended == cudaSuccess ? cudaGraphInstantiate(&exec, graph, 0) : cudaSuccess;
+        if (graph) cudaGraphDestroy(graph);
+        check_cuda(launched, "step kernel (graph capture)");
+        check_cuda(ended, "cudaStreamEndCapture");
+        check_cuda(made, "cudaGraphInstantiate");
+        sg.exec = exec;
+        sg.first = first;
+        std::memcpy(&sg.key, &h->key, sizeof h->key);
+        sg.grid = g;
+        sg.block = b;
     }
-    cudaGraph_t graph = nullptr;
-    const cudaError_t ended = cudaStreamEndCapture(h->stream, &graph);
-    cudaGraphExec_t exec = nullptr;
-    const cudaError_t made =
-        launched == cudaSuccess && ended == cudaSuccess ? cudaGraphInstantiate(&exec, graph, 0) : cudaSuccess;
-    if (graph) cudaGraphDestroy(graph);
-    check_cuda(launched, "step kernel (graph capture)");
-    check_cuda(ended, "cudaStreamEndCapture");
-    check_cuda(made, "cudaGraphInstantiate");
     cudaError_t e = cudaSuccess;
     std::uint64_t run = 0;
-    for (; run < replays && e == cudaSuccess; ++run) e = cudaGraphLaunch(exec, h->stream);
-    cudaGraphExecDestroy(exec);
+    for (; run < replays && e == cudaSuccess; ++run) e = cudaGraphLaunch(sg.exec, h->stream);
     check_cuda(e, "cudaGraphLaunch");
     h->t += run * kGraphSteps;
     return run * kGraphSteps;
