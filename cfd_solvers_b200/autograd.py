@@ -44,13 +44,13 @@ class GrayLbm(torch.autograd.Function):
     """(ns, tau) -> (rho(T), u(T)) through the B200 gray-LBM step; backward = discrete adjoint."""
 
     @staticmethod
-    def forward(ctx, ns, tau, solver, steps, interval, init):
+    def forward(ctx, ns, tau, solver, steps, interval, init, subinterval=0):
         if not ns.is_cuda:
             raise ValueError("ns must be a CUDA tensor")
         solver.set_solid_fraction(ns.detach().to(torch.float32).contiguous())
         solver.set_tau(float(tau))
         init(solver)
-        solver.adjoint_forward(int(steps), int(interval))
+        solver.adjoint_forward(int(steps), int(interval), int(subinterval))
         rho, u = device_fields(solver, ns.device)
         ctx.solver = solver
         ctx.ns_dtype = ns.dtype
@@ -71,13 +71,18 @@ class GrayLbm(torch.autograd.Function):
         tau = ctx.tau_like
         gt = torch.tensor(gtau, dtype=tau.dtype if torch.is_tensor(tau) else torch.float64,
                           device=tau.device if torch.is_tensor(tau) else dev)
-        return grad.to(ctx.ns_dtype), gt, None, None, None, None
+        return grad.to(ctx.ns_dtype), gt, None, None, None, None, None
 
 
-def gray_lbm(ns: torch.Tensor, tau, solver: EsotericPullCudaSolver, steps: int, interval: int = 64, init=None):
-    """Functional form of :class:`GrayLbm`; ``init`` defaults to rest at rho = 1."""
+def gray_lbm(ns: torch.Tensor, tau, solver: EsotericPullCudaSolver, steps: int, interval: int = 64, init=None,
+             subinterval: int = 0):
+    """Functional form of :class:`GrayLbm`; ``init`` defaults to rest at rho = 1.
+
+    ``subinterval`` > 0 reverses each checkpoint segment in two levels of recompute
+    (see ``EsotericPullCudaSolver.adjoint_forward``); the gradients are the same.
+    """
     if init is None:
         init = lambda s: s.initialize_uniform()  # noqa: E731
     if not torch.is_tensor(tau):
         tau = torch.tensor(float(tau), dtype=torch.float64, device=ns.device)
-    return GrayLbm.apply(ns, tau, solver, steps, interval, init)
+    return GrayLbm.apply(ns, tau, solver, steps, interval, init, subinterval)

@@ -258,3 +258,20 @@ def test_autograd_matches_adjoint_and_finite_differences(engine):
         tp, tm = float(np.float32(0.63 + ht)), float(np.float32(0.63 - ht))
         fdt *= 2 * ht / (tp - tm)
         assert gt == pytest.approx(fdt, rel=1e-5)
+
+
+def test_autograd_two_level_recompute_same_gradients(engine):
+    torch = pytest.importorskip("torch")
+    from cfd_solvers_b200.autograd import gray_lbm
+
+    kw, flags, ns, ustar = problem(19)
+    dev = torch.device("cuda:0")
+    target = torch.tensor(ustar, dtype=torch.float32, device=dev)
+    grads = []
+    with solver(engine, 19, "fp32", kw, flags, ns) as s:
+        for sub in (0, 2):
+            ns_t = torch.tensor(ns, dtype=torch.float32, device=dev, requires_grad=True)
+            _, u = gray_lbm(ns_t, 0.63, s, 13, interval=6, subinterval=sub)
+            (0.5 * ((u - target) ** 2).sum()).backward()
+            grads.append(ns_t.grad.cpu().numpy())
+    assert np.array_equal(grads[0], grads[1])
