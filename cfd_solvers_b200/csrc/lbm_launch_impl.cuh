@@ -3,6 +3,8 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
+#include <cstdint>
 #include <type_traits>
 
 #include "lbm_adjoint.cuh"
@@ -69,15 +71,24 @@ cudaError_t step_paired(const LbmArgs& a, dim3 b, cudaStream_t s) {
 
 // Wall-aware z-marching pair kernel (FP16 storage): grid over pairs, rows and
 // chunks of a.planes planes; the pipelined form stages two planes of words
-// per thread in shared memory.  Its shared-memory carveout is set once so that
-// the blocks its register cap allows fit on an SM.
-template <class K> cudaError_t w2_carveout(K kernel, unsigned smem_bytes, int blocks) {
-    static cudaError_t done = [&] {
-        const unsigned need = (smem_bytes + 1024U) * static_cast<unsigned>(blocks); // + per-block reservation
-        const int pct = static_cast<int>(std::min(100U, (need * 100U + 228U * 1024U - 1U) / (228U * 1024U)));
-        return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
-    }();
-    return done;
+// per thread in shared memory.  Its dynamic shared-memory limit (above 48 KB a
+// kernel must opt in: D3Q27's stages) and its carveout (so that the blocks
+// its register cap allows fit on an SM) are set once per kernel and device:
+// function attributes belong to the device's context.
+template <class K>
+cudaError_t w2_attributes(K kernel, unsigned smem_bytes, int blocks, std::atomic<std::uint64_t>& devices_done) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    const std::uint64_t bit = device < 64 ? (1ULL << device) : 0ULL;
+    if (bit != 0ULL && (devices_done.load() & bit) != 0ULL) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes));
+    if (e != cudaSuccess) return e;
+    const unsigned need = (smem_bytes + 1024U) * static_cast<unsigned>(blocks); // + per-block reservation
+    const int pct = static_cast<int>(std::min(100U, (need * 100U + 228U * 1024U - 1U) / (228U * 1024U)));
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    if (e == cudaSuccess) devices_done.fetch_or(bit);
+    return e;
 }
 
 template <class L, class S, bool LES, bool FL, bool GR>
@@ -91,8 +102,9 @@ cudaError_t step_w2(const KernelKey& k, const LbmArgs& a, dim3 b, cudaStream_t s
         const unsigned span = a.z_end - a.z_first;
         dim3 g((pairs + b.x - 1U) / b.x, (a.ny + b.y - 1U) / b.y, (span + planes - 1U) / planes);
         if (k.w2_pipe) {
-            const cudaError_t e =
-                w2_carveout(k_step_w2<L, LES, FL, GR, true>, w2_smem_bytes<L>(), w2_min_blocks<L>());
+            static std::atomic<std::uint64_t> devices_done{0}; // one per kernel instantiation
+            const cudaError_t e = w2_attributes(k_step_w2<L, LES, FL, GR, true>, w2_smem_bytes<L>(),
+                                                w2_min_blocks<L>(), devices_done);
             if (e != cudaSuccess) return e;
             k_step_w2<L, LES, FL, GR, true><<<g, b, w2_smem_bytes<L>(), s>>>(a);
         } else {

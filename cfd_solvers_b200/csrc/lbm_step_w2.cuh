@@ -20,14 +20,23 @@
 //
 // Walls (half-way bounce-back in place, as the one-cell kernel's gather).  A
 // wall link only changes which slot a load takes: the source's other slot at
-// the same address.  The kernel loads the plain words for every pair and, for
-// the few cells with wall links (a nonzero wall-link mask), replaces the
-// bounced halves with 16-bit loads of the partner slots; a cell next to a
-// moving wall gets the one-cell kernel's correction lane by lane.  Stores are
-// the same slots with or without walls; a pair holding a wall cell stores its
-// fluid cell's halves alone (wall cells hold no populations of their own).
+// the same address (same element, the other table).  Stores are the same
+// slots with or without walls; a pair holding a wall cell stores its fluid
+// cell's halves alone (wall cells hold no populations of their own); a cell
+// next to a moving wall gets the one-cell kernel's correction lane by lane.
 // Warps without near-wall cells skip all of this on uniform branches, so
 // there is no near-wall cell list and no second launch.
+//   Pipelined form: the flags of a plane are read three planes ahead and the
+// wall-link masks of its near-wall pairs two planes ahead (into per-thread
+// shared-memory rings), so when the words of plane z + 1 are issued their
+// tables are known.  A warp holding a near-wall pair issues the near-wall
+// form for all its lanes: every aligned word (the pb word and the pa word of
+// a pair with c_x(j) = 0) once per cell, each from the table that cell's wall
+// link selects, and the shifted words (one per cell already) likewise.  The
+// relaxation then takes each cell's half from its own word (one byte permute
+// per aligned word) and never waits on a mask or a partner load.
+//   Unpipelined form: plain words for every pair; the cells with wall links
+// replace their bounced halves with 16-bit loads of the partner slots.
 //
 // Results equal the one-cell kernel's bit for bit: the same loads, the same
 // explicitly rounded collision (collide_scaled), the moving-wall correction
@@ -61,6 +70,23 @@ template <class L> struct W2Words {
         int p = 0;
         while (p + 1 < L::PAIRS && pa_slot(p + 1) <= k) ++p;
         return p;
+    }
+    // Word slot k (k >= 1) holds both cells' elements (an aligned pb or pa word);
+    // otherwise it is one of the two words of a shifted pa slot.
+    __host__ __device__ static constexpr bool aligned(int k) { return k <= L::PAIRS || !shifted(pa_pair(k)); }
+    // Cell whose source element a shifted word holds: the first word holds cell
+    // x0's (x0 + 1 or x0 - 1), the second cell x0 + 1's (x0 + 2 or x0).
+    __host__ __device__ static constexpr int cell_of(int k) { return k - pa_slot(pa_pair(k)); }
+    // Wall-link bit of slot k (k >= 1): a pb word carries direction j = 2p + 2
+    // (bit 2p + 1), a pa word direction i = 2p + 1 (bit 2p).
+    __host__ __device__ static constexpr u32 link_bit(int k) {
+        return k <= L::PAIRS ? (2U << (2 * (k - 1))) : (1U << (2 * pa_pair(k)));
+    }
+    // Wall-link bits of the aligned slots.
+    __host__ __device__ static constexpr u32 aligned_bits() {
+        u32 m = 0U;
+        for (int k = 1; k < count; ++k) m |= aligned(k) ? link_bit(k) : 0U;
+        return m;
     }
 };
 
@@ -105,6 +131,26 @@ template <class L, int D> __device__ __forceinline__ u32 w2_dyz(const W2Ctx& c) 
 // index per access: +10 % on the 512^3 FP16 cavity.
 __device__ __forceinline__ __half* w2_tab(const LbmArgs& a, u32 off) { return static_cast<__half*>(a.base) + off; }
 
+// Element index (within its table) of the first element of word slot K >= 1,
+// and the slot's table offset: plain, or (ALT) the table a wall link reads.
+template <class L, int K> __device__ __forceinline__ u32 w2_word_idx(const W2Ctx& c) {
+    if constexpr (K <= L::PAIRS) {
+        return c.n0;
+    } else {
+        constexpr int p = W2Words<L>::pa_pair(K);
+        constexpr int second = K - W2Words<L>::pa_slot(p);
+        constexpr int j = 2 * p + 2, s = L::cx(j);
+        const u32 dyz = w2_dyz<L, j>(c);
+        if constexpr (s == 0) return c.n0 + dyz;
+        else if constexpr (s > 0) return (second ? c.nr : c.n0) + dyz;
+        else return (second ? c.n0 : c.nl) + dyz;
+    }
+}
+template <class L, int K, bool ALT> __device__ __forceinline__ u32 w2_table(const LbmArgs& a) {
+    if constexpr (K <= L::PAIRS) return ALT ? a.pa_off[K - 1] : a.pb_off[K - 1];
+    else return ALT ? a.pb_off[W2Words<L>::pa_pair(K)] : a.pa_off[W2Words<L>::pa_pair(K)];
+}
+
 // Address of word slot K.
 template <class L, int K> __device__ __forceinline__ const __half* w2_word_ptr(const LbmArgs& a, const W2Ctx& c) {
     if constexpr (K == 0) {
@@ -131,6 +177,54 @@ template <class L, int K = 0, class F> __device__ __forceinline__ void w2_words(
     }
 }
 
+__device__ __forceinline__ u32 ld_u16(const __half* p) { return *reinterpret_cast<const unsigned short*>(p); }
+__device__ __forceinline__ u32 with_lo(u32 w, u32 h) { return (w & 0xffff0000U) | h; }
+__device__ __forceinline__ u32 with_hi(u32 w, u32 h) { return (w & 0x0000ffffU) | (h << 16); }
+
+// Near-wall form: calls f(std::integral_constant<int, k>, address) for every
+// word slot k with the table a wall link selects: for a shifted word the
+// link of the cell whose source it holds (masks m0, m1 of cells x0, x0 + 1),
+// for an aligned word (both cells' elements) the links in ma.
+template <class L, int K = 0, class F>
+__device__ __forceinline__ void w2_near_words(const LbmArgs& a, const W2Ctx& c, u32 m0, u32 m1, u32 ma, F&& f) {
+    using W = W2Words<L>;
+    if constexpr (K < W::count) {
+        if constexpr (K == 0) {
+            f(std::integral_constant<int, 0>{}, w2_word_ptr<L, 0>(a, c));
+        } else {
+            constexpr u32 bit = W::link_bit(K);
+            const u32 m = W::aligned(K) ? ma : (W::cell_of(K) ? m1 : m0);
+            const u32 t = (m & bit) ? w2_table<L, K, true>(a) : w2_table<L, K, false>(a);
+            f(std::integral_constant<int, K>{}, w2_tab(a, t) + w2_word_idx<L, K>(c));
+        }
+        w2_near_words<L, K + 1>(a, c, m0, m1, ma, f);
+    }
+}
+
+// Direction whose half-pair an aligned word slot K >= 1 holds: j of a pb word, i of a pa word.
+template <class L, int K> constexpr int w2_dir() {
+    return K <= L::PAIRS ? 2 * K : 2 * W2Words<L>::pa_pair(K) + 1;
+}
+
+// Cell x0 + 1's half of the aligned words whose table differs from cell x0's
+// (a pair whose two fluid cells disagree on such a link): reloaded from the
+// other table (bits in to_alt: the alternative table, in to_plain: the plain one).
+template <class L, int K = 1>
+__device__ __forceinline__ void w2_fix_second(const LbmArgs& a, const W2Ctx& c, u32 to_alt, u32 to_plain, u32* pw) {
+    using W = W2Words<L>;
+    if constexpr (K < W::count) {
+        if constexpr (W::aligned(K)) {
+            constexpr u32 bit = W::link_bit(K);
+            constexpr int d = w2_dir<L, K>();
+            if ((to_alt | to_plain) & bit) {
+                const u32 t = (to_alt & bit) ? w2_table<L, K, true>(a) : w2_table<L, K, false>(a);
+                pw[d] = with_hi(pw[d], ld_u16(w2_tab(a, t) + (w2_word_idx<L, K>(c) + 1U)));
+            }
+        }
+        w2_fix_second<L, K + 1>(a, c, to_alt, to_plain, pw);
+    }
+}
+
 // Pair words (low half: cell x0, high half: cell x0 + 1) of every direction
 // from the raw words, as if the pair had no walls.
 template <class L> __device__ __forceinline__ void w2_assemble(const u32* raw, u32* pw) {
@@ -147,9 +241,6 @@ template <class L> __device__ __forceinline__ void w2_assemble(const u32* raw, u
     });
 }
 
-__device__ __forceinline__ u32 ld_u16(const __half* p) { return *reinterpret_cast<const unsigned short*>(p); }
-__device__ __forceinline__ u32 with_lo(u32 w, u32 h) { return (w & 0xffff0000U) | h; }
-__device__ __forceinline__ u32 with_hi(u32 w, u32 h) { return (w & 0x0000ffffU) | (h << 16); }
 
 // Index, within the cell's own row plane, of the source element of cell
 // x0 + C for a direction with c_x = S (the halves of the shifted words of
@@ -203,36 +294,37 @@ __device__ __noinline__ void w2_moving_lane(const LbmArgs& a, const W2Ctx c, std
 // Stores: aligned words where the slot pair is aligned, two 16-bit stores
 // where the pa row is shifted (h2_stores' rule).
 // MERGE (a warp holding a pair with a wall cell): a wall cell is not stepped,
-// and its slots must keep their bits.  Its half of each aligned word is the
-// word's loaded value (raw(k), word slot k; byte selector sel: 0x3210 keeps
-// the stepped word, 0x3254 takes the low half, 0x7610 the high half from
-// raw), and its shifted halves are not stored (live0 / live1).  Writing the
-// loaded bits back is exact: no cell writes a wall cell's slots within a step
-// and the cells that read them (bounce-back) read the same bits either way.
-template <class L, bool MERGE, class Raw>
-__device__ __forceinline__ void w2_stores(const LbmArgs& a, const W2Ctx& c, const float2* f, u32 h0, u32 h1, u32 sel,
-                                          bool live0, bool live1, Raw&& raw) {
-    const auto merged = [&](u32 w, auto K) {
-        if constexpr (MERGE)
-            return __byte_perm(w, raw(K), sel);
-        else
-            return w;
+// and its slots must keep their bits, so a pair with one live cell (live0 /
+// live1) stores that cell's halves alone, as 16-bit stores.  No cell writes a
+// wall cell's slots within a step, so its slots keep their bits.
+template <class L, bool MERGE>
+__device__ __forceinline__ void w2_stores(const LbmArgs& a, const W2Ctx& c, const float2* f, u32 h0, u32 h1,
+                                          bool live0, bool live1) {
+    const auto store_aligned = [&](__half* ptr, u32 w) {
+        if constexpr (MERGE) {
+            if (live0 && live1) {
+                st_word(ptr, w);
+            } else if (live0) {
+                st_half(ptr, w);
+            } else if (live1) {
+                st_half(ptr + 1, w >> 16);
+            }
+        } else {
+            st_word(ptr, w);
+        }
     };
-    st_word(w2_tab(a, a.rest_off) + c.n0,
-            merged(f16x2_rs(f[0].y, f[0].x, lo_halves(round_bits(a, h0, 0), round_bits(a, h1, 0))),
-                   std::integral_constant<int, 0>{}));
+    store_aligned(w2_tab(a, a.rest_off) + c.n0,
+                  f16x2_rs(f[0].y, f[0].x, lo_halves(round_bits(a, h0, 0), round_bits(a, h1, 0))));
     static_for_pairs<L>([&](auto PP) {
         constexpr int p = decltype(PP)::value;
         constexpr int i = 2 * p + 1, j = i + 1, s = L::cx(j);
-        constexpr int k = W2Words<L>::pa_slot(p);
         const u32 k0 = round_bits(a, h0, p + 1), k1 = round_bits(a, h1, p + 1);
-        st_word(w2_tab(a, a.pb_off[p]) + c.n0,
-                merged(f16x2_rs(f[i].y, f[i].x, lo_halves(k0, k1)), std::integral_constant<int, 1 + p>{}));
+        store_aligned(w2_tab(a, a.pb_off[p]) + c.n0, f16x2_rs(f[i].y, f[i].x, lo_halves(k0, k1)));
         const u32 wj = f16x2_rs(f[j].y, f[j].x, hi_halves(k0, k1));
         __half* t = w2_tab(a, a.pa_off[p]);
         const u32 dyz = w2_dyz<L, j>(c);
         if constexpr (s == 0) {
-            st_word(t + (c.n0 + dyz), merged(wj, std::integral_constant<int, k>{}));
+            store_aligned(t + (c.n0 + dyz), wj);
         } else if constexpr (MERGE) {
             if (live0) st_half(t + (w2_src<s, 0>(c) + dyz), wj);
             if (live1) st_half(t + (w2_src<s, 1>(c) + dyz), wj >> 16);
@@ -243,8 +335,10 @@ __device__ __forceinline__ void w2_stores(const LbmArgs& a, const W2Ctx& c, cons
     });
 }
 
-// One pair of cells from its raw words.  fl2: the two internal flag bytes
-// (cell x0 in the low byte).  raw(k): word slot k as loaded (for MERGE stores).
+// One pair of cells from its pair words pw (low half cell x0).  fl2: the two
+// internal flag bytes (cell x0 in the low byte).  BOUNCE: pw holds the plain
+// words and the cells with wall links reload their bounced halves here (the
+// unpipelined form; the pipelined one assembles them from the near-wall form).
 // The moving-wall correction is a call, not inlined code: inlined, its
 // per-lane arrays raised the register demand of the whole kernel and the
 // interior path spilled.  It gets a copy of the populations (tmp), since an
@@ -252,15 +346,12 @@ __device__ __forceinline__ void w2_stores(const LbmArgs& a, const W2Ctx& c, cons
 // The bounce-back loads stay inline: they run in every warp that holds a
 // near-wall pair (on a cavity, the first and last warp of each row), and a
 // call there saved and restored the live registers through local memory.
-template <class L, bool LES, bool FLAGS, bool GRAY, class Raw>
-__device__ __forceinline__ void w2_cell_pair(const LbmArgs& a, const W2Ctx& c, const u32* raw_words, unsigned fl2,
-                                             Raw&& raw) {
-    u32 pw[L::Q];
-    w2_assemble<L>(raw_words, pw);
+template <class L, bool LES, bool FLAGS, bool GRAY, bool BOUNCE>
+__device__ __forceinline__ void w2_cell_pair(const LbmArgs& a, const W2Ctx& c, u32* pw, unsigned fl2) {
     constexpr unsigned kNearWall2 = kFlagNearWall * 0x0101U;
     constexpr unsigned kNearMoving2 = kFlagNearMoving * 0x0101U;
     constexpr unsigned kType2 = kFlagTypeMask * 0x0101U;
-    if constexpr (FLAGS) {
+    if constexpr (FLAGS && BOUNCE) {
         if (fl2 & kNearWall2) {
             // wall cells have empty masks; a fluid cell's mask is loaded only when it has links
             const u32 m0 = (fl2 & kFlagNearWall) ? a.wall_mask[c.n0] : 0U;
@@ -291,17 +382,19 @@ __device__ __forceinline__ void w2_cell_pair(const LbmArgs& a, const W2Ctx& c, c
         const bool wall0 = (fl2 & kFlagTypeMask) != 0U, wall1 = (fl2 & (kFlagTypeMask << 8)) != 0U;
         // warp-uniform choice: the merging stores cost every thread of the warp the same
         if (__any_sync(__activemask(), (fl2 & kType2) != 0U)) {
-            const u32 sel = wall0 ? 0x3254U : (wall1 ? 0x7610U : 0x3210U);
-            w2_stores<L, true>(a, c, f, h0, h1, sel, !wall0, !wall1, raw);
+            w2_stores<L, true>(a, c, f, h0, h1, !wall0, !wall1);
             return;
         }
     }
-    w2_stores<L, false>(a, c, f, h0, h1, 0x3210U, true, true, raw);
+    w2_stores<L, false>(a, c, f, h0, h1, true, true);
 }
 
 // ---------------------------------------------------------------- cp.async
 template <int OFF> __device__ __forceinline__ void cp_async4(u32 smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0+%2], [%1], 4;\n" ::"r"(smem), "l"(gmem), "n"(OFF) : "memory");
+}
+__device__ __forceinline__ void cp_async8(u32 smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
@@ -323,17 +416,32 @@ template <class L> constexpr int w2_min_blocks() { return L::Q == 27 ? CFDX_W2_M
 // form are laid out for it, so their offsets are immediates).
 constexpr unsigned kW2Threads = 128;
 
-// Shared memory of the pipelined form: two stages of the word slots per
-// thread, in groups of four words so that one 16-byte load reads four.
-template <class L> constexpr unsigned w2_groups() { return (static_cast<unsigned>(W2Words<L>::count) + 3U) / 4U; }
-template <class L> constexpr unsigned w2_smem_bytes() { return 2U * w2_groups<L>() * kW2Threads * 16U; }
+// Shared memory of the pipelined form, per thread, in groups of four words
+// (one 16-byte load reads four): two stages, each with the count word slots,
+// two words of second-cell fixes (w2_fix_second's bits, written when the
+// plane's words are issued) and two words holding the wall-link masks of the
+// plane three ahead of the one the stage holds (same parity); then a ring of
+// four planes' pair flags.  D3Q19: 7 groups per stage, 30 KB per block.
+// Measured and replaced (512^3 cavity, FP16): a near-wall form with a word
+// per cell for every aligned slot (42 KB per block: the L1 left beside five
+// blocks' shared memory cost the interior 5 %); one stage read into
+// registers before the next plane's copies (24 KB; the pair words live
+// through the issue spilled).
+template <class L> constexpr unsigned w2_groups() { return (static_cast<unsigned>(W2Words<L>::count) + 4U + 3U) / 4U; }
+template <class L> constexpr unsigned w2_fix_slot() { return static_cast<unsigned>(W2Words<L>::count); }
+template <class L> constexpr unsigned w2_mask_slot() { return 4U * w2_groups<L>() - 2U; } // 8-byte aligned
+constexpr unsigned kW2FlagRing = 4;
+template <class L> constexpr unsigned w2_smem_bytes() {
+    return 2U * w2_groups<L>() * kW2Threads * 16U + kW2FlagRing * kW2Threads * 4U;
+}
 
 // Grid: x over pairs (blockDim.x threads, nx/2 pairs), y over rows
 // (blockDim.x * blockDim.y == kW2Threads), z over chunks of a.planes planes
 // of [a.z_first, a.z_end).
 template <class L, bool LES, bool FLAGS, bool GRAY, bool PIPE>
 __global__ void __launch_bounds__(kW2Threads, w2_min_blocks<L>()) k_step_w2(const __grid_constant__ LbmArgs a) {
-    constexpr int W = W2Words<L>::count;
+    using Wd = W2Words<L>;
+    constexpr int W = Wd::count;
     const u32 x0 = 2U * (blockIdx.x * blockDim.x + threadIdx.x);
     const u32 y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x0 >= a.nx || y >= a.ny) return;
@@ -341,9 +449,11 @@ __global__ void __launch_bounds__(kW2Threads, w2_min_blocks<L>()) k_step_w2(cons
     const u32 ze = min(a.z_end, zb + a.planes);
     W2Ctx c;
     w2_thread(a, x0, y, c);
-    const auto flags_of = [&](const W2Ctx& cc) -> unsigned {
+    constexpr unsigned kNear2 = kFlagNearWall * 0x0101U;
+    // pair flags (cell x0 in the low byte) of plane z
+    const auto flags_at = [&](u32 z) -> unsigned {
         if constexpr (FLAGS)
-            return *reinterpret_cast<const unsigned short*>(a.flags + cc.n0);
+            return *reinterpret_cast<const unsigned short*>(a.flags + ((z * a.ny + y) * a.nx + x0));
         else
             return 0U;
     };
@@ -354,58 +464,133 @@ __global__ void __launch_bounds__(kW2Threads, w2_min_blocks<L>()) k_step_w2(cons
     if constexpr (!PIPE) {
         for (u32 z = zb; z < ze; ++z) {
             w2_plane(a, z, c);
-            const unsigned fl2 = flags_of(c);
+            const unsigned fl2 = flags_at(z);
             if (both_walls(fl2)) continue;
             u32 raw[W];
             w2_words<L>(a, c, [&](auto K, const __half* p) { raw[decltype(K)::value] = ld_word(p); });
-            // merging stores reload a wall cell's words (no other cell writes them in this step)
-            w2_cell_pair<L, LES, FLAGS, GRAY>(a, c, raw, fl2, [&](auto K) {
-                return ld_word(w2_word_ptr<L, decltype(K)::value>(a, c));
-            });
+            u32 pw[L::Q];
+            w2_assemble<L>(raw, pw);
+            w2_cell_pair<L, LES, FLAGS, GRAY, true>(a, c, pw, fl2);
         }
     } else {
-        // word k of stage st: component k % 4 of w2_stage[(st * G + k / 4) * kW2Threads + tid]
+        // Word k of stage st: component k % 4 of w2_stage[(st * G + k / 4) * kW2Threads + tid]; the
+        // masks of a plane at word w2_mask_slot of the stage of its parity.  After the stages, ring
+        // slot r of the flags: the pair flags of a plane, bit 16 set when its words were issued in
+        // the near-wall form.  Plane z uses stage (z - zb) % 2 and flag slot (z - zb) % 4.
+        // Iteration z issues the words of z + 1 and the masks of z + 3, then waits for everything
+        // but that (so the masks of z + 1, fetched two iterations earlier, have arrived).
         constexpr u32 G = w2_groups<L>();
+        constexpr u32 GW = (static_cast<u32>(W) + 3U) / 4U; // groups holding words
+        constexpr u32 kStageBytes = G * kW2Threads * 16U;
+        constexpr u32 kMask = w2_mask_slot<L>(), kFix = w2_fix_slot<L>();
+        static_assert(kFix + 2U <= kMask, "second-cell fixes between the words and the masks");
         extern __shared__ uint4 w2_stage[];
         const u32 tid = threadIdx.y * blockDim.x + threadIdx.x;
         const uint4* mine = w2_stage + tid;
         const u32 sbase = static_cast<u32>(__cvta_generic_to_shared(mine));
-        constexpr u32 kStageBytes = G * kW2Threads * 16U;
-        const auto issue = [&](u32 z, u32 st) -> unsigned {
+        u32* const fring = reinterpret_cast<u32*>(w2_stage + 2U * G * kW2Threads) + tid;
+        const auto slot_at = [&](u32 st, u32 k) { // byte offset of word slot k of stage st from sbase
+            return st * kStageBytes + (k / 4U) * kW2Threads * 16U + (k % 4U) * 4U;
+        };
+        const auto slot_ptr = [&](u32 st, u32 k) {
+            return reinterpret_cast<u32*>(reinterpret_cast<char*>(w2_stage + tid) + slot_at(st, k));
+        };
+        // wall-link masks of plane z into the stage of its parity (n0 even: 8-byte aligned)
+        const auto fetch_masks = [&](u32 z) {
+            cp_async8(sbase + slot_at((z - zb) & 1U, kMask), a.wall_mask + ((z * a.ny + y) * a.nx + x0));
+        };
+        // Copies the words of plane z into stage st, with the tables its wall links select when a
+        // lane of the warp has links (the warp's vote: the form costs every lane the same); returns
+        // the ring word.  A wall cell's halves are never stored, so an aligned word takes the
+        // table of its pair's fluid cell; when both cells are fluid and disagree on a link, cell
+        // x0's choice is taken and the second cell's half is fixed after the words arrive.
+        const auto issue = [&](u32 z, u32 st, unsigned fl2, uint2 m) -> unsigned {
             W2Ctx cn = c;
             w2_plane(a, z, cn);
             const u32 s0 = sbase + st * kStageBytes;
-            w2_words<L>(a, cn, [&](auto K, const __half* p) {
+            bool near = false;
+            if constexpr (FLAGS) near = __any_sync(__activemask(), (fl2 & kNear2) != 0U);
+            const auto copy = [&](auto K, const __half* p) {
                 constexpr int k = decltype(K)::value;
                 cp_async4<(k / 4) * kW2Threads * 16 + (k % 4) * 4>(s0, p);
-            });
-            return flags_of(cn);
+            };
+            if (!both_walls(fl2)) {
+                if (near) {
+                    // wall cells have empty masks; a fluid cell's mask was fetched only when it has links
+                    const u32 m0 = (fl2 & kFlagNearWall) ? m.x : 0U;
+                    const u32 m1 = (fl2 & (kFlagNearWall << 8)) ? m.y : 0U;
+                    const u32 m0e = (fl2 & kFlagTypeMask) != 0U ? m1 : m0;
+                    const u32 m1e = (fl2 & (kFlagTypeMask << 8)) != 0U ? m0 : m1;
+                    const u32 mixed = (m0e ^ m1e) & Wd::aligned_bits();
+                    w2_near_words<L>(a, cn, m0, m1, m0e, copy);
+                    u32* fix = slot_ptr(st, kFix);
+                    fix[0] = mixed & m1e;  // the second cell reads the alternative table
+                    fix[1] = mixed & ~m1e; // the second cell reads the plain table
+                } else {
+                    w2_words<L>(a, cn, copy);
+                }
+            }
+            return fl2 | (near ? 0x10000U : 0U);
         };
-        unsigned fl_next = issue(zb, 0U);
+        // prologue: flags of the first four planes, masks of the first three, words of the first
+        const unsigned f0 = flags_at(zb);
+        const unsigned f1 = zb + 1U < ze ? flags_at(zb + 1U) : 0U;
+        const unsigned f2 = zb + 2U < ze ? flags_at(zb + 2U) : 0U;
+        unsigned ahead = zb + 3U < ze ? flags_at(zb + 3U) : 0U; // flags of plane z + 3 in iteration z
+        fring[kW2Threads] = f1;
+        fring[2U * kW2Threads] = f2;
+        uint2 m0v = make_uint2(0U, 0U);
+        if constexpr (FLAGS) {
+            if (zb + 1U < ze && (f1 & kNear2)) fetch_masks(zb + 1U);
+            if (zb + 2U < ze && (f2 & kNear2)) fetch_masks(zb + 2U);
+        }
         cp_async_commit();
+        if constexpr (FLAGS) {
+            if (f0 & kNear2) m0v = *reinterpret_cast<const uint2*>(a.wall_mask + ((zb * a.ny + y) * a.nx + x0));
+        }
+        fring[0] = issue(zb, 0U, f0, m0v);
+        cp_async_commit();
+        cp_async_wait<1>(); // the masks of planes zb + 1, zb + 2
         for (u32 z = zb; z < ze; ++z) {
-            const unsigned fl2 = fl_next;
-            const u32 st = (z - zb) & 1U;
-            if (z + 1U < ze) fl_next = issue(z + 1U, st ^ 1U);
+            const u32 r = z - zb;
+            const unsigned f3 = ahead;
+            if (z + 3U < ze) fring[((r + 3U) & 3U) * kW2Threads] = f3;
+            ahead = z + 4U < ze ? flags_at(z + 4U) : 0U;
+            if (z + 1U < ze) {
+                u32* const slot = fring + ((r + 1U) & 3U) * kW2Threads;
+                const unsigned fn = *slot;
+                uint2 mn = make_uint2(0U, 0U);
+                if (FLAGS && (fn & kNear2)) mn = *reinterpret_cast<const uint2*>(slot_ptr((r + 1U) & 1U, kMask));
+                *slot = issue(z + 1U, (r + 1U) & 1U, fn, mn);
+            }
+            if constexpr (FLAGS) {
+                // after the read above: the masks of z + 3 go where those of z + 1 were
+                if (z + 3U < ze && (f3 & kNear2)) fetch_masks(z + 3U);
+            }
             cp_async_commit();
-            cp_async_wait<1>();
+            cp_async_wait<1>(); // all but this iteration's copies: the words of z
+            const unsigned ring = fring[(r & 3U) * kW2Threads];
+            const unsigned fl2 = ring & 0xffffU;
             if (both_walls(fl2)) continue;
-            const uint4* groups = mine + st * (G * kW2Threads);
-            u32 raw[4 * G];
+            const uint4* groups = mine + (r & 1U) * (G * kW2Threads);
+            u32 raw[4 * GW];
 #pragma unroll
-            for (u32 g = 0; g < G; ++g) {
+            for (u32 g = 0; g < GW; ++g) {
                 const uint4 v = groups[g * kW2Threads];
                 raw[4 * g] = v.x;
                 raw[4 * g + 1] = v.y;
                 raw[4 * g + 2] = v.z;
                 raw[4 * g + 3] = v.w;
             }
+            u32 pw[L::Q];
+            w2_assemble<L>(raw, pw);
             w2_plane(a, z, c);
-            // merging stores re-read the words from the stage, intact until the next issue
-            w2_cell_pair<L, LES, FLAGS, GRAY>(a, c, raw, fl2, [&](auto K) {
-                constexpr int k = decltype(K)::value;
-                return reinterpret_cast<const u32*>(groups + (k / 4) * kW2Threads)[k % 4];
-            });
+            if (FLAGS && (ring & 0x10000U) != 0U) {
+                const u32* fix = slot_ptr(r & 1U, kFix);
+                const u32 to_alt = fix[0], to_plain = fix[1];
+                if ((to_alt | to_plain) != 0U) w2_fix_second<L>(a, c, to_alt, to_plain, pw);
+            }
+            w2_cell_pair<L, LES, FLAGS, GRAY, false>(a, c, pw, fl2);
         }
         cp_async_wait_all();
     }

@@ -68,7 +68,9 @@ def test_paired_variant_requires_even_nx(engine):
 
 # The wall-aware FP16 pair kernel (variants 3 and 4) marches along z; plane
 # counts that do not divide nz leave a short last chunk, and rows of 256 cells
-# span more than one warp.
+# span more than one warp.  The pipelined form (variant 3) reads flags three
+# and wall-link masks two planes ahead: runs of 1, 2 and 3 planes per thread
+# end its look-ahead at every depth.
 W2_SHAPES = SHAPES + [(256, 5, 9)]
 
 
@@ -77,7 +79,7 @@ W2_SHAPES = SHAPES + [(256, 5, 9)]
 @pytest.mark.parametrize("shape", W2_SHAPES, ids=[f"{a}x{b}x{c}" for a, b, c in W2_SHAPES])
 @pytest.mark.parametrize("flags_kind, gray", [(None, False), ("random", False), ("random", True),
                                               ("cavity", False), ("cavity", True)])
-@pytest.mark.parametrize("variant, planes", [(3, 0), (3, 3), (4, 1), (4, 5)])
+@pytest.mark.parametrize("variant, planes", [(3, 0), (3, 1), (3, 2), (3, 3), (4, 1), (4, 5)])
 def test_wall_aware_pairs_match_single_bitwise(engine, q, storage, shape, flags_kind, gray, variant, planes):
     steps = 5
     a_log, a_red = run(engine, 1, q, shape, storage, flags_kind, gray, steps)
