@@ -205,13 +205,15 @@ struct cfdx_lbm {
         return storage == kStoreF16S && q == 19 && !flags;
     }
     // The wall-aware z-marching pair kernel (k_step_w2, cp.async pipeline, 4
-    // planes per thread) against the one-cell kernel, B200, FP16, GLUPS:
-    // D3Q19 TRT + Smagorinsky cavity 512^3 50.6 vs 48.6; without Smagorinsky
-    // 51.9 vs 52.0; D3Q27 Smagorinsky cavity 29.6 vs 34.1; gray channels (D3Q27
-    // 256^3, D3Q19 128^3) 15.7 vs 30.7 and 29.2 vs 36.4; 512x256x256 sphere pack
-    // 40.8 vs 45.6.  Automatic choice: where it wins.
-    static bool w2_default(int storage, int q, bool flags, bool les, bool gray) {
-        return storage == kStoreF16S && q == 19 && flags && les && !gray;
+    // planes per thread, wall links resolved three planes ahead) against the
+    // one-cell kernel, B200, FP16, GLUPS: D3Q19 TRT + Smagorinsky cavity 512^3
+    // 52.2 vs 47.8; without Smagorinsky 53.3 vs 51.4; 512x256x256 sphere pack
+    // 46.2 vs 45.6; D3Q27 Smagorinsky cavity 384^3 28.1 vs 34.7; gray channels
+    // (D3Q19 128^3, D3Q27 256^3) 23.8 vs 37.5 and 12.8 vs 30.3 (the gray and
+    // D3Q27 forms spill); periodic BGK 57.1 vs 63.7 for the flag-free paired
+    // kernel.  Automatic choice: where it wins.
+    static bool w2_default(int storage, int q, bool flags, bool gray) {
+        return storage == kStoreF16S && q == 19 && flags && !gray;
     }
     double les_k = 0.0;
     std::uint64_t h2d = 0, d2h = 0, syncs = 0;
@@ -368,7 +370,7 @@ struct cfdx_lbm {
     void choose_variant() {
         key.narrow = offsets_fit();
         key.w2 = (variant == 3 || variant == 4 ||
-                  (variant == 0 && w2_default(key.storage, key.q, key.flags, key.les, key.gray))) &&
+                  (variant == 0 && w2_default(key.storage, key.q, key.flags, key.gray))) &&
                  w2_eligible();
         key.w2_pipe = variant != 4;
         key.paired = !key.w2 && (variant == 2 || (variant == 0 && paired_eligible() &&

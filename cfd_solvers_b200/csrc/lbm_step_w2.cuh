@@ -426,7 +426,11 @@ constexpr unsigned kW2Threads = 128;
 // per cell for every aligned slot (42 KB per block: the L1 left beside five
 // blocks' shared memory cost the interior 5 %); one stage read into
 // registers before the next plane's copies (24 KB; the pair words live
-// through the issue spilled).
+// through the issue spilled); staging the second cell's fix words too (up to
+// eight per pair, 38 KB per block): 49.1 instead of 52.2 GLUPS on the cavity
+// and 38.8 instead of 46.2 on the 512x256x256 sphere pack, whose mixed pairs
+// paid more for the issue than the fix loads cost.  A stage stride of a
+// power of two groups (8) made ptxas spill.
 template <class L> constexpr unsigned w2_groups() { return (static_cast<unsigned>(W2Words<L>::count) + 4U + 3U) / 4U; }
 template <class L> constexpr unsigned w2_fix_slot() { return static_cast<unsigned>(W2Words<L>::count); }
 template <class L> constexpr unsigned w2_mask_slot() { return 4U * w2_groups<L>() - 2U; } // 8-byte aligned
