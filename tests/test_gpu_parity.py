@@ -264,6 +264,51 @@ def test_fp16_storage_matches_fp16_oracle(engine, oracle_mod, q, wide):
         assert fields_err(s.compute_macroscopic(), L.macroscopic()) < 5e-5
 
 
+FP16_WALL_CASES = [("sphere", (96, 40, 36)), ("sphere", (256, 24, 20)), ("cavity", (96, 96, 96))]
+
+
+@pytest.mark.parametrize("case, shape", FP16_WALL_CASES, ids=[f"{c}-{a}x{b}x{d}" for c, (a, b, d) in FP16_WALL_CASES])
+@pytest.mark.parametrize("variant, planes", [(0, 0), (3, 3)], ids=["automatic", "pairs-3-planes"])
+def test_fp16_walled_lattices_match_fp16_oracle(engine, oracle_mod, case, shape, variant, planes):
+    """The shapes of the precision configuration (a D3Q19 TRT channel, periodic in x with no-slip
+    y/z walls, a seeded sphere pack, a body force) and of the plain method at scale (a lid-driven
+    cavity, TRT + Smagorinsky Cs 0.1, tau 0.51, lid (0.1, 0, 0)) in FP16 shifted storage, on lattices
+    the oracle runs in seconds (nearest rounding, the oracle's codec).  With flags and an even nx the
+    automatic step is the wall-aware pair kernel, so its near-wall pairs are checked against the
+    oracle directly: wall cells beside fluid cells in one pair (every x-wall of the cavity), fluid
+    pairs that disagree on a wall link (sphere surfaces), shifted words that wrap around x beside a
+    sphere, and the rows next to the moving lid.  9 and 10 steps."""
+    from cfd_solvers_b200.cases import sphere_pack
+
+    nx, ny, nz = shape
+    wall_u = None
+    if case == "sphere":
+        kw = dict(tau=0.55, storage="fp16s", collision="trt", acceleration_x=1e-5, fp16_rounding="nearest")
+        flags = sphere_pack(nx, ny, nz, fraction=0.10, rmin=2.0, rmax=5.0, seed=3)
+    else:
+        kw = dict(tau=0.51, storage="fp16s", collision="trt", trt_magic=3.0 / 16.0, smagorinsky_les=True,
+                  smagorinsky_cs=0.1, fp16_rounding="nearest")
+        flags, wall_u, _, _ = case_inputs("cavity", False, False, nx, ny, nz)
+    scale = np.array([2.0 ** round(np.log2(1 / w)) for w in oracle_weights(19)], np.float32)
+    L = oracle_mod.OracleLattice(**oracle_config(oracle_mod, 19, nx, ny, nz, kw), storage="f16s", flags=flags,
+                                 scale=scale, wall_u=wall_u)
+    with make(engine, 19, nx, ny, nz, **kw) as s:
+        s.set_launch_shape(0, 0, variant)
+        s.set_step_planes(planes)
+        s.set_flags(flags)
+        if wall_u is not None:
+            s.set_wall_velocity(2, *wall_u[2])
+            s.initialize_uniform()
+            L.init_uniform()
+        else:
+            s.initialize_taylor_green(0.04)
+            L.init_taylor_green(0.04)
+        for steps in (9, 1):
+            s.step(steps)
+            L.step(steps)
+            assert fields_err(s.compute_macroscopic(), L.macroscopic()) < 5e-5, L.t
+
+
 @pytest.mark.parametrize("q", [19, 27])
 @pytest.mark.parametrize("storage", ["fp32", "fp16s", "fp64"])
 def test_wide_slot_pointers_equal_offsets_bitwise(engine, q, storage):
