@@ -239,8 +239,8 @@ CFDX_API int cfdx_lbm_raw_populations(cfdx_lbm* lbm, void** device_ptr, size_t* 
  * kernel that marches along z, with / without its shared-memory prefetch of
  * the next plane (FP16 storage, even nx).  All variants give bitwise equal
  * results.  Automatic: two cells for D3Q19 FP16 on lattices without flags,
- * the wall-aware pair kernel (3) for D3Q19 FP16 with flags and Smagorinsky
- * and without gray cells, one cell otherwise.  Zeros restore the defaults.
+ * the wall-aware pair kernel (3) for D3Q19 FP16 with flags and without gray
+ * cells, one cell otherwise.  Zeros restore the defaults.
  * Reference: no counterpart (the OpenMP loop of step_once,
  * esoteric_pull.hpp:494-515, has no launch shape). */
 CFDX_API int cfdx_lbm_set_launch_shape(cfdx_lbm* lbm, int block_x, int block_y, int variant);
