@@ -21,20 +21,22 @@
 // Walls (half-way bounce-back in place, as the one-cell kernel's gather).  A
 // wall link only changes which slot a load takes: the source's other slot at
 // the same address (same element, the other table).  Stores are the same
-// slots with or without walls; a pair holding a wall cell stores its fluid
-// cell's halves alone (wall cells hold no populations of their own); a cell
-// next to a moving wall gets the one-cell kernel's correction lane by lane.
-// Warps without near-wall cells skip all of this on uniform branches, so
-// there is no near-wall cell list and no second launch.
-//   Pipelined form: the flags of a plane are read three planes ahead and the
-// wall-link masks of its near-wall pairs two planes ahead (into per-thread
-// shared-memory rings), so when the words of plane z + 1 are issued their
-// tables are known.  A warp holding a near-wall pair issues the near-wall
-// form for all its lanes: every aligned word (the pb word and the pa word of
-// a pair with c_x(j) = 0) once per cell, each from the table that cell's wall
-// link selects, and the shifted words (one per cell already) likewise.  The
-// relaxation then takes each cell's half from its own word (one byte permute
-// per aligned word) and never waits on a mask or a partner load.
+// slots with or without walls.  A pair holding a wall cell stores its fluid
+// cell's halves alone: the wall cell is not stepped, and its slots hold what
+// fluid neighbours wrote in the previous step and read back in this one.  A
+// cell next to a moving wall gets the one-cell kernel's correction lane by
+// lane.  Warps without near-wall cells skip all of this on uniform branches,
+// so there is no near-wall cell list and no second launch.
+//   Pipelined form: the flags of a plane are read three planes ahead (a ring
+// in shared memory) and the wall-link masks of its near-wall pairs two
+// planes ahead of the issue (two spare words of the stage), so when the words
+// of plane z + 1 are issued their tables are known.  A warp holding a
+// near-wall pair copies every word from the table a wall link selects: a
+// shifted word (one cell's element) by its cell's link, an aligned word (both
+// cells' elements) by the link of the pair's fluid cell, or of cell x0 when
+// both are fluid.  Where two fluid cells disagree on an aligned link, the
+// second cell's half is fixed with one 16-bit load once the words arrive (the
+// fix bits are written beside the words).  The relaxation waits on no mask.
 //   Unpipelined form: plain words for every pair; the cells with wall links
 // replace their bounced halves with 16-bit loads of the partner slots.
 //
